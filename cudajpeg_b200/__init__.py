@@ -1,0 +1,280 @@
+"""cudajpeg_b200 -- B200-native baseline-JPEG decoder.
+
+The decoder is ``libcudajpeg.so`` (C ABI in ``include/*.h``, CUDA kernels for
+sm_100a in ``csrc/``); this package builds it in-tree and binds it with
+ctypes.  There is no CPU decode path: without the library or a GPU every
+call fails with an exception.
+
+    import cudajpeg_b200 as cj
+    with cj.Reader() as r:
+        r.open("image.jpg")          # openJPG
+        rgb = r.pixels()             # H x W x 3 uint8 (H x W for grey)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcudajpeg.so")
+
+# format.h error codes
+NO_ERROR = 0
+SYNTAX_ERROR = 1
+UNSUPPORTED_ERROR = 2
+OOM_ERROR = 3
+CUDA_MEM_ERROR = 4
+FILE_ERROR = 5
+CUDA_KERNEL_LAUNCH_ERROR = 6
+PROGRAMMER_ERROR = -1
+ERROR_NAMES = {0: "NO_ERROR", 1: "SYNTAX_ERROR", 2: "UNSUPPORTED_ERROR", 3: "OOM_ERROR",
+               4: "CUDA_MEM_ERROR", 5: "FILE_ERROR", 6: "CUDA_KERNEL_LAUNCH_ERROR",
+               -1: "PROGRAMMER_ERROR"}
+
+READER_HOST_COEFFICIENTS = 1
+
+# Every symbol the C headers in include/ declare (checked by the CPU tests).
+EXPORTED = [
+    "read16", "delJPGReader", "newJPGReader", "openJPG", "openJPGMem", "writeJPG",
+    "printError", "skipBlock", "decodeSOF", "decodeDHT", "decodeDQT", "decodeDRI",
+    "decodeScanGPU", "iDCT_resample_colourTransform", "cjIDCTPlane", "cjIDCTBlocksRaw",
+    "cjReaderInfo", "cjReaderPixels", "cjReaderSetFlags", "cjReaderSetSubsequenceBits",
+    "cjReaderStageTimes", "cjReaderDeviceCoefficients", "cjReaderDeviceQuantTable",
+    "cjReaderStream", "cjDebugHuffDecode", "cjReaderRedecodeDevice", "cjReaderSync",
+    "cjReaderDevicePixels", "cjReaderSetProfile", "cjReaderKernelTimes", "cjReaderLaunchCount",
+]
+
+KERNEL_NAMES = ["k_destuff_count", "k_scan_tiles", "k_destuff_scatter", "k_build_segments",
+                "k_sync_intra", "k_sync_inter", "k_scan_warps", "k_decode_write", "k_pixel"]
+
+
+class DecodeError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        super().__init__(f"{ERROR_NAMES.get(code, code)}{': ' + what if what else ''}")
+
+
+_lib = None
+
+
+def load(build_if_missing: bool = True):
+    """Load libcudajpeg.so (building it with nvcc if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if not build_if_missing:
+            raise OSError(f"{LIB_PATH} is not built (python -m cudajpeg_b200.build)")
+        from . import build as _build
+        _build.build()
+    lib = C.CDLL(LIB_PATH)
+    vp, i64p = C.c_void_p, C.POINTER(C.c_int64)
+    lib.newJPGReader.restype = vp
+    lib.delJPGReader.argtypes = [vp]
+    lib.openJPG.argtypes = [vp, C.c_char_p]
+    lib.openJPGMem.argtypes = [vp, vp, C.c_size_t]
+    lib.writeJPG.argtypes = [vp, C.c_char_p]
+    lib.printError.argtypes = [vp]
+    lib.read16.restype = C.c_ushort
+    lib.read16.argtypes = [vp]
+    lib.cjReaderInfo.argtypes = [vp, i64p]
+    lib.cjReaderPixels.restype = vp
+    lib.cjReaderPixels.argtypes = [vp]
+    lib.cjReaderSetFlags.argtypes = [vp, C.c_int]
+    lib.cjReaderSetSubsequenceBits.argtypes = [vp, C.c_int]
+    lib.cjReaderStageTimes.argtypes = [vp, C.POINTER(C.c_float)]
+    lib.cjReaderDeviceCoefficients.restype = vp
+    lib.cjReaderDeviceCoefficients.argtypes = [vp, i64p]
+    lib.cjReaderDeviceQuantTable.restype = vp
+    lib.cjReaderDeviceQuantTable.argtypes = [vp, C.c_int]
+    lib.cjReaderStream.restype = vp
+    lib.cjReaderStream.argtypes = [vp]
+    lib.cjIDCTPlane.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp,
+                                C.c_int, C.c_int, vp]
+    lib.cjIDCTBlocksRaw.argtypes = [vp, C.c_longlong, vp, vp, C.c_int, vp]
+    lib.cjDebugHuffDecode.argtypes = [vp, vp, C.c_uint]
+    lib.cjReaderRedecodeDevice.argtypes = [vp]
+    lib.cjReaderSync.argtypes = [vp]
+    lib.cjReaderDevicePixels.restype = vp
+    lib.cjReaderDevicePixels.argtypes = [vp]
+    lib.cjReaderSetProfile.argtypes = [vp, C.c_int]
+    lib.cjReaderKernelTimes.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int]
+    lib.cjReaderLaunchCount.restype = C.c_longlong
+    lib.cjReaderLaunchCount.argtypes = [vp]
+    _lib = lib
+    return lib
+
+
+class Reader:
+    """A JPGReader (format.h): one decoder with its own CUDA stream and
+    grow-only device / pinned buffers, reused across images."""
+
+    def __init__(self, sub_bits: int = 0, host_coefficients: bool = False):
+        self.lib = load()
+        self.ptr = self.lib.newJPGReader()
+        if not self.ptr:
+            raise MemoryError("newJPGReader failed")
+        if sub_bits:
+            self.set_subsequence_bits(sub_bits)
+        if host_coefficients:
+            self.lib.cjReaderSetFlags(self.ptr, READER_HOST_COEFFICIENTS)
+        self._pinned_src = None
+
+    def close(self):
+        if self.ptr:
+            self.lib.delJPGReader(self.ptr)
+            self.ptr = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_subsequence_bits(self, bits: int):
+        if self.lib.cjReaderSetSubsequenceBits(self.ptr, bits):
+            raise ValueError(f"bad subsequence size {bits}")
+
+    # ---- decode
+    def open(self, path: str, check: bool = True) -> int:
+        err = self.lib.openJPG(self.ptr, os.fsencode(path))
+        if check and err:
+            raise DecodeError(err, path)
+        return err
+
+    def open_bytes(self, data, check: bool = True) -> int:
+        """Decode JPEG bytes (bytes, bytearray, uint8 ndarray, or a pinned
+        torch tensor's data_ptr given as (ptr, size))."""
+        if isinstance(data, tuple):
+            ptr, size = data
+        else:
+            arr = np.frombuffer(data, np.uint8) if not isinstance(data, np.ndarray) else data
+            arr = np.ascontiguousarray(arr)
+            self._pinned_src = arr  # keep alive during the call
+            ptr, size = arr.ctypes.data, arr.nbytes
+        err = self.lib.openJPGMem(self.ptr, C.c_void_p(ptr), size)
+        if check and err:
+            raise DecodeError(err)
+        return err
+
+    # ---- results
+    def info(self) -> dict:
+        a = (C.c_int64 * 12)()
+        self.lib.cjReaderInfo(self.ptr, a)
+        keys = ["width", "height", "channels", "mcux", "mcuy", "restart_interval", "bpm",
+                "subsequences", "destuffed", "markers", "scan_bytes", "param_bytes"]
+        return dict(zip(keys, [int(v) for v in a]))
+
+    def pixels(self, copy: bool = True) -> np.ndarray:
+        inf = self.info()
+        h, w, ch = inf["height"], inf["width"], inf["channels"]
+        n = w * h * (3 if ch == 3 else 1)
+        p = self.lib.cjReaderPixels(self.ptr)
+        if not p:
+            raise DecodeError(PROGRAMMER_ERROR, "no decoded image")
+        buf = (C.c_uint8 * n).from_address(p)
+        arr = np.frombuffer(buf, np.uint8).reshape((h, w, 3) if ch == 3 else (h, w))
+        return arr.copy() if copy else arr
+
+    def stage_times(self) -> tuple:
+        a = (C.c_float * 2)()
+        self.lib.cjReaderStageTimes(self.ptr, a)
+        return float(a[0]), float(a[1])
+
+    def coefficients(self) -> list:
+        """int32 dequantised coefficients per channel, [nblocks, 64] natural
+        order, the reference's working_space layout.  Needs
+        host_coefficients=True at construction."""
+        out = []
+        hdr = _reader_fields(self.ptr)
+        for c in range(hdr["channels"]):
+            mem, size = _working_space(self.ptr, c)
+            if not mem:
+                raise DecodeError(PROGRAMMER_ERROR, "coefficients were not exported")
+            buf = (C.c_int32 * size).from_address(mem)
+            out.append(np.frombuffer(buf, np.int32).copy().reshape(-1, 64))
+        return out
+
+    # ---- device-resident decode and instrumentation (benchmarks)
+    def redecode_device(self):
+        err = self.lib.cjReaderRedecodeDevice(self.ptr)
+        if err:
+            raise DecodeError(err, "redecode")
+
+    def sync(self) -> int:
+        return self.lib.cjReaderSync(self.ptr)
+
+    def stream(self) -> int:
+        return self.lib.cjReaderStream(self.ptr)
+
+    def set_profile(self, on: bool):
+        self.lib.cjReaderSetProfile(self.ptr, 1 if on else 0)
+
+    def kernel_times(self) -> list:
+        ids = (C.c_int * 32)()
+        ms = (C.c_float * 32)()
+        n = self.lib.cjReaderKernelTimes(self.ptr, ids, ms, 32)
+        return [(KERNEL_NAMES[ids[k]], float(ms[k])) for k in range(n)]
+
+    def launch_count(self) -> int:
+        return int(self.lib.cjReaderLaunchCount(self.ptr))
+
+    def device_coefficients(self):
+        n = C.c_int64(0)
+        p = self.lib.cjReaderDeviceCoefficients(self.ptr, C.byref(n))
+        return p, n.value
+
+
+# ---- JPGReader field access for the few fields ctypes needs (layout of
+# include/format.h on LP64)
+class _Managed(C.Structure):
+    _fields_ = [("mem", C.c_void_p), ("size", C.c_uint), ("max_size", C.c_uint)]
+
+
+class _Channel(C.Structure):
+    _fields_ = [("id", C.c_int), ("dq_id", C.c_int), ("ac_id", C.c_int), ("dc_id", C.c_int),
+                ("width", C.c_int), ("height", C.c_int), ("samples_x", C.c_int),
+                ("samples_y", C.c_int), ("stride", C.c_int), ("block_stride", C.c_int),
+                ("num_blocks", C.c_int), ("dc_cumulative_val", C.c_int),
+                ("working_space", _Managed), ("pixels", _Managed)]
+
+
+class _Reader(C.Structure):
+    _fields_ = [("buf", C.c_void_p), ("pos", C.c_void_p), ("end", C.c_void_p),
+                ("width", C.c_ushort), ("height", C.c_ushort),
+                ("num_blocks_x", C.c_ushort), ("num_blocks_y", C.c_ushort),
+                ("block_size_x", C.c_ushort), ("block_size_y", C.c_ushort),
+                ("num_channels", C.c_ubyte), ("restart_interval", C.c_int),
+                ("channels", _Channel * 3), ("pixels", C.c_void_p), ("max_pixels_size", C.c_int),
+                ("dq_tables", (C.c_ubyte * 64) * 4), ("file_buf", _Managed),
+                ("time", C.c_long), ("error", C.c_int), ("error_line", C.c_int),
+                ("error_file", C.c_char_p), ("error_func", C.c_char_p),
+                ("flags", C.c_int), ("scan_seen", C.c_int), ("huff_defined", C.c_int),
+                ("dev", C.c_void_p)]
+
+
+def _reader_fields(ptr) -> dict:
+    r = _Reader.from_address(ptr)
+    return {"channels": r.num_channels, "error": r.error, "time": r.time,
+            "error_func": r.error_func}
+
+
+def _working_space(ptr, c):
+    r = _Reader.from_address(ptr)
+    ws = r.channels[c].working_space
+    return ws.mem, ws.size
+
+
+def decode(data, sub_bits: int = 0) -> np.ndarray:
+    """Decode one JPEG (bytes) to an RGB / grey ndarray."""
+    with Reader(sub_bits=sub_bits) as r:
+        r.open_bytes(data)
+        return r.pixels()

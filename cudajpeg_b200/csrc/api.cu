@@ -1,0 +1,113 @@
+// api.cu -- plain-C accessors and tuning knobs of libcudajpeg (cudajpeg.h).
+#include <stddef.h>
+
+#include "../../include/cudajpeg.h"
+#include "cj_internal.h"
+#include "cj_tables.h"
+
+extern "C" {
+
+void cjReaderInfo(const JPGReader* r, int64_t* info) {
+  const CJReaderDevice* d = r->dev;
+  const CJStatus* st = (d && d->h_status.p) ? (const CJStatus*)d->h_status.p : nullptr;
+  const CJScanParams* hp = (d && d->h_params.p) ? (const CJScanParams*)d->h_params.p : nullptr;
+  info[0] = r->width;
+  info[1] = r->height;
+  info[2] = r->num_channels;
+  info[3] = r->num_blocks_x;
+  info[4] = r->num_blocks_y;
+  info[5] = r->restart_interval;
+  info[6] = hp ? hp->bpm : 0;
+  info[7] = st ? st->nsub : 0;
+  info[8] = st ? st->destuffed : 0;
+  info[9] = st ? st->nmarkers : 0;
+  info[10] = d ? (int64_t)d->raw_len : 0;
+  info[11] = (int64_t)sizeof(CJScanParams);
+}
+
+const unsigned char* cjReaderPixels(const JPGReader* r) { return r->pixels; }
+
+void cjReaderSetFlags(JPGReader* r, int flags) { r->flags = flags; }
+
+int cjReaderSetSubsequenceBits(JPGReader* r, int bits) {
+  if (bits == 0) bits = CJ_SUB_BITS_DEFAULT;
+  if (bits < 128 || bits > 65536 || (bits & 31)) return PROGRAMMER_ERROR;
+  r->dev->sub_bits = bits;
+  return 0;
+}
+
+void cjReaderStageTimes(const JPGReader* r, float* ms) {
+  const CJReaderDevice* d = r->dev;
+  ms[0] = ms[1] = 0.f;
+  if (!d->gpu_ready) return;
+  cudaEventElapsedTime(&ms[0], d->ev_begin, d->ev_scan);
+  cudaEventElapsedTime(&ms[1], d->ev_scan, d->ev_end);
+}
+
+const short* cjReaderDeviceCoefficients(const JPGReader* r, int64_t* nblocks) {
+  *nblocks = r->dev->total_blocks;
+  return (const short*)r->dev->coef.p;
+}
+
+const short* cjReaderDeviceQuantTable(const JPGReader* r, int t) {
+  if (!r->dev->params.p || t < 0 || t > 3) return nullptr;
+  return ((const CJScanParams*)r->dev->params.p)->qnat[t];
+}
+
+void* cjReaderStream(const JPGReader* r) { return (void*)r->dev->stream; }
+
+int cjReaderRedecodeDevice(JPGReader* r) {
+  CJReaderDevice* d = r->dev;
+  if (!d->gpu_ready || !d->raw.p || !d->total_blocks) return PROGRAMMER_ERROR;
+  int err = cj_scan_device(r);
+  if (!err) err = cj_pixel_launch(r, false);
+  return err;
+}
+
+int cjReaderSync(JPGReader* r) {
+  CJReaderDevice* d = r->dev;
+  if (!d->gpu_ready) return PROGRAMMER_ERROR;
+  CJ_CUDA_TRY(cudaMemcpyAsync(d->h_status.p, d->status.p, sizeof(CJStatus), cudaMemcpyDeviceToHost,
+                              d->stream),
+              CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaStreamSynchronize(d->stream), CUDA_KERNEL_LAUNCH_ERROR);
+  const CJStatus* st = (const CJStatus*)d->h_status.p;
+  if (st->unstable) {
+    int err = cj_scan_resync(r);
+    if (!err) err = cj_pixel_launch(r, false);
+    if (err) return err;
+    CJ_CUDA_TRY(cudaMemcpyAsync(d->h_status.p, d->status.p, sizeof(CJStatus),
+                                cudaMemcpyDeviceToHost, d->stream),
+                CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaStreamSynchronize(d->stream), CUDA_KERNEL_LAUNCH_ERROR);
+  }
+  return cj_status_error(st);
+}
+
+const unsigned char* cjReaderDevicePixels(const JPGReader* r) {
+  return (const unsigned char*)r->dev->pix.p;
+}
+
+void cjReaderSetProfile(JPGReader* r, int on) { r->dev->profile = on != 0; }
+
+int cjReaderKernelTimes(const JPGReader* r, int* ids, float* ms, int max) {
+  const CJReaderDevice* d = r->dev;
+  int n = d->nkev < max ? d->nkev : max;
+  for (int k = 0; k < n; k++) {
+    ids[k] = d->kslot[k];
+    ms[k] = 0.f;
+    cudaEventElapsedTime(&ms[k], d->kev[k], d->kev[k + 1]);
+  }
+  return n;
+}
+
+long long cjReaderLaunchCount(const JPGReader* r) { return r->dev->launches; }
+
+int cjDebugHuffDecode(const unsigned char counts[16], const unsigned char* symbols,
+                      unsigned int win16) {
+  CJHuff t;
+  cj_build_huff(counts, symbols, &t);
+  return (int)cj_huff_decode(t, win16 & 0xFFFF);
+}
+
+}  // extern "C"

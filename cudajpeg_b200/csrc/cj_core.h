@@ -1,0 +1,202 @@
+// cj_core.h -- data layouts and the per-lane Huffman block decoder shared by
+// the entropy kernels.  Everything here is plain C++ marked __host__
+// __device__ so the same code is compiled for sm_100a kernels and for host
+// unit checks of the table builder.
+#pragma once
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define CJ_HD __host__ __device__ __forceinline__
+#else
+#define CJ_HD inline
+#endif
+
+// ---------------------------------------------------------------- limits
+#define CJ_FAST_BITS 10          // first-level Huffman lookup width
+#define CJ_MAX_BPM 32            // blocks per MCU (the standard allows 10)
+#define CJ_SUB_BITS_DEFAULT 1024 // bits per speculative subsequence
+
+// Device error codes (the reader maps them to the format.h codes)
+#define CJ_DEV_OK 0
+#define CJ_DEV_BAD_CODE 1        // Huffman prefix with no code (SYNTAX_ERROR)
+#define CJ_DEV_BAD_AC 2          // zero-size AC symbol that is not EOB/ZRL, or run past 63
+#define CJ_DEV_OVERRUN 3         // restart interval needs bits past its marker
+#define CJ_DEV_TRAILING 4        // restart interval has whole bytes after its last MCU
+#define CJ_DEV_MARKER 5          // bad / missing / misplaced RSTn, or other marker in scan
+#define CJ_DEV_DC_RANGE 6        // DC predictor outside int16 (UNSUPPORTED_ERROR)
+#define CJ_DEV_EXTRA 7           // more entropy data than MCUs
+#define CJ_DEV_CAPACITY 8        // more markers / subsequences than buffers allow
+
+// One Huffman table in canonical form.
+//   fast[w >> (16 - CJ_FAST_BITS)] = (len << 8) | symbol for codes of length
+//   <= CJ_FAST_BITS, else 0; longer codes are found through maxcode/valoff
+//   exactly as in ITU T.81 Annex F.2.2.3 (DECODE procedure).
+struct CJHuff {
+  uint16_t fast[1 << CJ_FAST_BITS];
+  int32_t maxcode[18];  // [l], l = 1..16: largest code of length l, -1 if none
+  int32_t valoff[18];   // symbol index of code c of length l = valoff[l] + c
+  uint8_t vals[256];
+};
+
+// Per-scan parameters, built on the host after SOS and copied once.
+struct alignas(16) CJScanParams {
+  CJHuff huff[4];                 // DC0, DC1, AC0, AC1
+  int16_t qnat[4][64];            // quantisation tables, natural order
+  uint8_t phase_comp[CJ_MAX_BPM]; // component of the k-th block of an MCU
+  uint8_t phase_blk[CJ_MAX_BPM];  // index of that block inside its component's MCU part
+  uint8_t comp_dc[3], comp_ac[3], comp_q[3];
+  uint8_t comp_sx[3], comp_sy[3];
+  uint8_t pad0;
+  uint8_t zz[64];                 // natural-order index of zig-zag position k
+  int32_t nch, bpm, mcux, mcuy;
+  int32_t width, height;
+  int32_t hmax, vmax, xshift, yshift; // chroma upsample shifts
+  int32_t restart_interval;          // MCUs, 0 = none
+  int32_t nseg_expected;             // restart intervals in the scan
+  int64_t total_blocks;              // mcux*mcuy*bpm
+  int32_t comp_stride[3];            // plane strides (bytes) for plane outputs
+  int32_t comp_rows[3];
+};
+
+// A restart interval (or the whole scan) in the destuffed buffer.
+struct CJSegment {
+  uint64_t bit_begin, bit_end;   // bits in the destuffed buffer
+  int64_t first_block;           // global block index of its first block
+  int64_t nblocks;               // blocks it must contain
+  int32_t first_sub, nsub;       // its subsequences
+  int32_t marker_follows;        // an RSTn ends it: its data must end on that
+                                 // byte; otherwise reads past the end give 1-bits
+  int32_t pad;
+};
+
+// Decoder state at a block boundary: bit position and MCU phase.
+CJ_HD uint64_t cj_state(uint64_t bit, uint32_t phase) { return (bit << 8) | phase; }
+CJ_HD uint64_t cj_state_bit(uint64_t s) { return s >> 8; }
+CJ_HD uint32_t cj_state_phase(uint64_t s) { return (uint32_t)(s & 0xFF); }
+
+// One speculative subsequence: where its decode started, where it left off,
+// how many blocks it began and the sum of its DC differences per component.
+struct CJSubRec {
+  uint64_t start;
+  uint64_t exit;
+  int32_t nblocks;
+  int32_t dc[3];
+};
+
+// Per-warp aggregate used by the segmented block/DC scan.
+struct CJWarpAgg {
+  int32_t has_head;  // a segment starts inside this warp
+  int32_t nblocks;   // sums over the lanes after the last segment head
+  int32_t dc[3];
+  int32_t pad[3];
+};
+
+// Status words the host reads back after a decode.
+struct CJStatus {
+  unsigned long long err_key; // min over errors of (block << 8 | CJ_DEV_*); ~0 = none
+  int32_t unstable;           // warps whose last exit changed in the last fix-up pass
+  int32_t nmarkers;           // RSTn markers found by the destuffer
+  int32_t nsub;               // subsequences in use
+  int32_t nseg;               // restart intervals in use
+  int64_t destuffed;          // bytes after destuffing
+};
+#define CJ_NO_ERROR_KEY 0xFFFFFFFFFFFFFFFFull
+
+// ---------------------------------------------------------------- bit access
+CJ_HD uint32_t cj_bswap(uint32_t v) {
+#ifdef __CUDA_ARCH__
+  return __byte_perm(v, 0, 0x0123);
+#else
+  return __builtin_bswap32(v);
+#endif
+}
+
+// 32-bit big-endian word `w` of the destuffed buffer; bytes at or past
+// `end_byte` read as 0xFF (the padding the reference's bit reader supplies).
+CJ_HD uint32_t cj_word(const uint32_t* words, uint64_t w, uint64_t end_byte) {
+  uint64_t first = w * 4;
+  if (first >= end_byte) return 0xFFFFFFFFu;
+  uint32_t v = cj_bswap(words[w]);
+  uint64_t last = first + 4;
+  if (last > end_byte) v |= (1u << (8 * (uint32_t)(last - end_byte))) - 1u;
+  return v;
+}
+
+// 32 bits starting at bit `p` (MSB first).
+CJ_HD uint32_t cj_peek32(const uint32_t* words, uint64_t p, uint64_t end_byte) {
+  uint64_t w = p >> 5;
+  uint32_t s = (uint32_t)(p & 31);
+  uint32_t hi = cj_word(words, w, end_byte);
+  if (!s) return hi;
+  uint32_t lo = cj_word(words, w + 1, end_byte);
+  return (hi << s) | (lo >> (32 - s));
+}
+
+// Decode one Huffman code from a left-aligned 16-bit window.  Returns
+// (len << 8) | symbol, or 0 when no code of length 1..16 matches.
+CJ_HD uint32_t cj_huff_decode(const CJHuff& t, uint32_t win16) {
+  uint32_t e = t.fast[win16 >> (16 - CJ_FAST_BITS)];
+  if (e) return e;
+  for (int l = CJ_FAST_BITS + 1; l <= 16; l++) {
+    int32_t code = (int32_t)(win16 >> (16 - l));
+    if (code <= t.maxcode[l]) return ((uint32_t)l << 8) | t.vals[(t.valoff[l] + code) & 255];
+  }
+  return 0;
+}
+
+// Sign extension of a `size`-bit magnitude category value (T.81 F.2.2.1).
+CJ_HD int32_t cj_extend(uint32_t bits, uint32_t size) {
+  return (bits < (1u << (size - 1))) ? (int32_t)bits - (int32_t)(1u << size) + 1 : (int32_t)bits;
+}
+
+// Natural-order index of zig-zag position k (T.81 figure A.6).
+#define CJ_ZIGZAG_INIT                                                                  \
+  {0,  1,  8,  16, 9,  2,  3,  10, 17, 24, 32, 25, 18, 11, 4,  5,  12, 19, 26, 33, 40, 48, \
+   41, 34, 27, 20, 13, 6,  7,  14, 21, 28, 35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, \
+   30, 37, 44, 51, 58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63}
+
+// Decode one block starting at bit `p` with the given tables.
+//   Sink receives (natural index, value) for every coefficient written,
+//   including the DC difference at index 0 (before prediction).
+//   Returns the bit position after the block; *err = CJ_DEV_* (0 ok).
+//   On an error the block is cut short at the failing symbol, consuming at
+//   least one bit, so a speculative decode keeps moving.
+//   *last_sym receives the start bit of the block's final symbol.
+template <class Sink>
+CJ_HD uint64_t cj_decode_block(const uint32_t* words, uint64_t end_byte, uint64_t p,
+                               const CJHuff& dc, const CJHuff& ac, const uint8_t* zz,
+                               int32_t* dc_diff, int* err, Sink& sink, uint64_t* last_sym) {
+  *err = 0;
+  *last_sym = p;
+  uint32_t v = cj_peek32(words, p, end_byte);
+  uint32_t e = cj_huff_decode(dc, v >> 16);
+  if (!e) { *err = CJ_DEV_BAD_CODE; *dc_diff = 0; return p + 1; }
+  uint32_t len = e >> 8, size = e & 15;
+  int32_t diff = 0;
+  if (size) diff = cj_extend((v << len) >> (32 - size), size);
+  *dc_diff = diff;
+  sink(0, diff);
+  p += len + size;
+  int k = 0;
+  for (;;) {
+    *last_sym = p;
+    v = cj_peek32(words, p, end_byte);
+    e = cj_huff_decode(ac, v >> 16);
+    if (!e) { *err = CJ_DEV_BAD_CODE; return p + 1; }
+    len = e >> 8;
+    uint32_t sym = e & 255;
+    if (sym == 0) { p += len; break; }       // EOB
+    size = sym & 15;
+    if (!size && sym != 0xF0) { *err = CJ_DEV_BAD_AC; return p + len; }
+    k += (int)(sym >> 4) + 1;
+    if (k > 63) { *err = CJ_DEV_BAD_AC; return p + len; }
+    if (size) sink(zz[k], cj_extend((v << len) >> (32 - size), size));
+    p += len + size;
+    if (k >= 63) break;
+  }
+  return p;
+}
+
+struct CJNullSink {
+  CJ_HD void operator()(int, int32_t) const {}
+};

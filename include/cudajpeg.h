@@ -1,0 +1,87 @@
+/*
+ * cudajpeg.h -- libcudajpeg additions that have no counterpart in the
+ * reference: plain-C accessors for FFI callers that cannot read the
+ * JPGReader struct directly, and decoder tuning knobs.
+ */
+#ifndef CUDAJPEG_H
+#define CUDAJPEG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "format.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* info[0..11]: width, height, channels, MCUs across, MCUs down, restart
+ * interval, blocks per MCU, subsequences of the last scan, destuffed scan
+ * bytes, markers found, entropy-coded bytes copied to the device, parameter
+ * bytes copied to the device (Huffman / quantisation tables, geometry). */
+void cjReaderInfo(const JPGReader *r, int64_t *info);
+
+/* The decoded image of the last successful openJPG / openJPGMem: RGB
+ * (width*height*3) or grey (width*height), in the reader's pinned buffer. */
+const unsigned char *cjReaderPixels(const JPGReader *r);
+
+/* Reader flags (CJ_READER_* in format.h). */
+void cjReaderSetFlags(JPGReader *r, int flags);
+
+/* Bits per speculative subsequence of the parallel Huffman decode
+ * (multiple of 32, 128..65536); 0 restores the default. */
+int cjReaderSetSubsequenceBits(JPGReader *r, int bits);
+
+/* Device time of the last decode split by stage, in milliseconds:
+ * [0] entropy stages (destuff .. coefficient write), [1] pixel kernel. */
+void cjReaderStageTimes(const JPGReader *r, float *ms);
+
+/* Device pointer to the quantised int16 coefficient blocks of the last scan
+ * (natural order, MCU scan order, 64 per block) and their count. */
+const short *cjReaderDeviceCoefficients(const JPGReader *r, int64_t *nblocks);
+
+/* Device pointer to the natural-order int16 quantisation table `t` (0..3)
+ * of the last scan. */
+const short *cjReaderDeviceQuantTable(const JPGReader *r, int t);
+
+/* The reader's CUDA stream (cudaStream_t). */
+void *cjReaderStream(const JPGReader *r);
+
+/* Re-run the whole device decode of the last successfully decoded file from
+ * its compressed bytes already resident on the GPU (destuff .. pixel
+ * kernel), leaving the image in device memory and skipping every host<->
+ * device copy.  Asynchronous on the reader's stream; check the result with
+ * cjReaderSync.  Returns 0 or a format.h error code. */
+int cjReaderRedecodeDevice(JPGReader *r);
+
+/* Wait for the reader's stream and return the device decode status of the
+ * last decode (0 or a format.h error code). */
+int cjReaderSync(JPGReader *r);
+
+/* Device pointer to the decoded image of the last decode. */
+const unsigned char *cjReaderDevicePixels(const JPGReader *r);
+
+/* Per-kernel timing: when on, every kernel launch is followed by a CUDA event
+ * on the reader's stream; cjReaderKernelTimes then returns, for the last
+ * decode, up to `max` (kernel id, milliseconds) pairs in launch order and
+ * their count.  Kernel ids: 0 destuff-count, 1 tile-scan, 2 destuff-scatter,
+ * 3 segments, 4 sync-intra, 5 sync-inter, 6 warp-scan, 7 decode-write,
+ * 8 pixel. */
+void cjReaderSetProfile(JPGReader *r, int on);
+int cjReaderKernelTimes(const JPGReader *r, int *ids, float *ms, int max);
+
+/* Kernels launched by this reader since it was created. */
+long long cjReaderLaunchCount(const JPGReader *r);
+
+/* Host check of the Huffman table builder: decode the left-aligned 16-bit
+ * window `win16` with the table built from a DHT segment's 16 code-length
+ * counts and symbols.  Returns (code length << 8) | symbol, or 0 when no
+ * code matches -- the {num_bits, tuple} entry of the reference's 64K table
+ * (src/format.cu:357-391) for the same window. */
+int cjDebugHuffDecode(const unsigned char counts[16], const unsigned char *symbols,
+                      unsigned int win16);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUDAJPEG_H */

@@ -1,0 +1,230 @@
+"""ctypes front end of the CPU checker.  TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may
+import this module; the decoder in ``cudajpeg_b200`` never does.
+
+Three libraries sit behind it (all built by ``oracle/Makefile``):
+
+* ``liboracle.so`` -- our C restatement of the reference path
+  (``jpeg_oracle.c``; see its header for the reference file:line map);
+* ``_ref/libref_cpuonly.so`` -- the reference's own CPUonly decoder compiled
+  from its sources: the pixel oracle and the timed CPU baseline;
+* ``_ref/libref_gputree.so`` -- the reference's ``src/format.cu`` +
+  ``src/decodeScanCPU.cu`` built as host C++: the coefficient oracle, which
+  also decodes restart-marker files.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+ERROR_NAMES = {0: "NO_ERROR", 1: "SYNTAX_ERROR", 2: "UNSUPPORTED_ERROR", 3: "OOM_ERROR",
+               4: "CUDA_MEM_ERROR", 5: "FILE_ERROR", 6: "CUDA_KERNEL_LAUNCH_ERROR",
+               -1: "PROGRAMMER_ERROR"}
+
+_lib = None
+_ref_cpu = None
+_ref_gpu = None
+
+
+def build() -> None:
+    """Compile liboracle.so (and oracle/_ref when the reference sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        lib = C.CDLL(path)
+        lib.oracle_decode.restype = C.c_void_p
+        lib.oracle_decode.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_int)]
+        lib.oracle_free.argtypes = [C.c_void_p]
+        lib.oracle_info.argtypes = [C.c_void_p, C.c_void_p]
+        lib.oracle_coefs.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        lib.oracle_plane.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        lib.oracle_pixels.argtypes = [C.c_void_p, C.c_void_p]
+        lib.oracle_dq.argtypes = [C.c_void_p, C.c_void_p]
+        lib.oracle_idct_blocks.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        lib.oracle_idct_f64.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        _lib = lib
+    return _lib
+
+
+@dataclass
+class Component:
+    samples_x: int
+    samples_y: int
+    width: int
+    height: int
+    stride: int
+    rows: int
+    nblocks: int
+    dq_id: int
+
+
+@dataclass
+class Decoded:
+    error: int
+    width: int = 0
+    height: int = 0
+    nch: int = 0
+    mcux: int = 0
+    mcuy: int = 0
+    restart_interval: int = 0
+    comps: list = field(default_factory=list)
+    coefs: list = field(default_factory=list)   # int32 [nblocks, 64] per component
+    planes: list = field(default_factory=list)  # uint8 [rows, stride] per component
+    pixels: np.ndarray | None = None            # uint8 [H, W, 3] or [H, W]
+    dq: np.ndarray | None = None                # uint8 [4, 64] zig-zag order
+
+
+def decode(data: bytes) -> Decoded:
+    """Decode a JPEG held in memory with the C restatement."""
+    lib = _load()
+    err = C.c_int(0)
+    h = lib.oracle_decode(data, len(data), C.byref(err))
+    try:
+        out = Decoded(error=err.value)
+        if err.value != 0 or not h:
+            return out
+        info = np.zeros(6 + 8 * 3, np.int32)
+        lib.oracle_info(h, info.ctypes.data)
+        out.width, out.height, out.nch, out.mcux, out.mcuy, out.restart_interval = map(int, info[:6])
+        for c in range(out.nch):
+            comp = Component(*map(int, info[6 + 8 * c: 14 + 8 * c]))
+            out.comps.append(comp)
+            coef = np.empty((comp.nblocks, 64), np.int32)
+            lib.oracle_coefs(h, c, coef.ctypes.data)
+            plane = np.empty((comp.rows, comp.stride), np.uint8)
+            lib.oracle_plane(h, c, plane.ctypes.data)
+            out.coefs.append(coef)
+            out.planes.append(plane)
+        shape = (out.height, out.width, 3) if out.nch == 3 else (out.height, out.width)
+        out.pixels = np.empty(shape, np.uint8)
+        lib.oracle_pixels(h, out.pixels.ctypes.data)
+        out.dq = np.empty((4, 64), np.uint8)
+        lib.oracle_dq(h, out.dq.ctypes.data)
+        return out
+    finally:
+        if h:
+            lib.oracle_free(h)
+
+
+def idct_int(coefs: np.ndarray) -> np.ndarray:
+    """Reference integer iDCT of int32 natural-order blocks -> uint8 [n, 64]."""
+    lib = _load()
+    c = np.ascontiguousarray(coefs, np.int32).reshape(-1, 64)
+    out = np.empty(c.shape, np.uint8)
+    lib.oracle_idct_blocks(c.ctypes.data, c.shape[0], out.ctypes.data)
+    return out
+
+
+def idct_f64(coefs: np.ndarray) -> np.ndarray:
+    """Exact FP64 iDCT (before +128, rounding and clip) -> float64 [n, 64]."""
+    lib = _load()
+    c = np.ascontiguousarray(coefs, np.int32).reshape(-1, 64)
+    out = np.empty(c.shape, np.float64)
+    lib.oracle_idct_f64(c.ctypes.data, c.shape[0], out.ctypes.data)
+    return out
+
+
+def quantised(d: Decoded) -> list:
+    """Per-component quantised coefficients (dequantised // Q), int32 [n, 64]."""
+    zz = np.array([0, 1, 8, 16, 9, 2, 3, 10, 17, 24, 32, 25, 18, 11, 4, 5, 12, 19, 26, 33, 40, 48,
+                   41, 34, 27, 20, 13, 6, 7, 14, 21, 28, 35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15,
+                   23, 30, 37, 44, 51, 58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63])
+    out = []
+    for comp, coef in zip(d.comps, d.coefs):
+        q = np.zeros(64, np.int64)
+        q[zz] = d.dq[comp.dq_id]
+        q[q == 0] = 1
+        out.append((coef // q).astype(np.int32))
+    return out
+
+
+# ---------------------------------------------------------------- reference builds
+
+def ref_available() -> bool:
+    return (os.path.exists(os.path.join(REF_DIR, "libref_cpuonly.so"))
+            and os.path.exists(os.path.join(REF_DIR, "libref_gputree.so")))
+
+
+def _load_ref():
+    global _ref_cpu, _ref_gpu
+    if _ref_cpu is None:
+        cpu = C.CDLL(os.path.join(REF_DIR, "libref_cpuonly.so"))
+        cpu.refcpu_open.restype = C.c_void_p
+        cpu.refcpu_open.argtypes = [C.c_char_p]
+        cpu.refcpu_info.argtypes = [C.c_void_p, C.c_void_p]
+        cpu.refcpu_pixels.argtypes = [C.c_void_p, C.c_void_p]
+        cpu.refcpu_close.argtypes = [C.c_void_p]
+        cpu.refcpu_bench.restype = C.c_double
+        cpu.refcpu_bench.argtypes = [C.POINTER(C.c_char_p), C.c_int, C.c_int, C.c_int,
+                                     C.POINTER(C.c_longlong), C.POINTER(C.c_int)]
+        gpu = C.CDLL(os.path.join(REF_DIR, "libref_gputree.so"))
+        gpu.refgpu_new.restype = C.c_void_p
+        gpu.refgpu_del.argtypes = [C.c_void_p]
+        gpu.refgpu_open.argtypes = [C.c_void_p, C.c_char_p]
+        gpu.refgpu_info.argtypes = [C.c_void_p, C.c_void_p]
+        gpu.refgpu_coefs.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        _ref_cpu, _ref_gpu = cpu, gpu
+    return _ref_cpu, _ref_gpu
+
+
+def ref_cpu_pixels(path: str):
+    """Reference CPUonly decode of a file -> pixels array, or None on failure."""
+    cpu, _ = _load_ref()
+    h = cpu.refcpu_open(path.encode())
+    if not h:
+        return None
+    try:
+        info = np.zeros(4, np.int32)
+        cpu.refcpu_info(h, info.ctypes.data)
+        w, hgt, nch = map(int, info[:3])
+        shape = (hgt, w, 3) if nch == 3 else (hgt, w)
+        px = np.empty(shape, np.uint8)
+        cpu.refcpu_pixels(h, px.ctypes.data)
+        return px
+    finally:
+        cpu.refcpu_close(h)
+
+
+def ref_gpu_coefs(path: str):
+    """Reference GPU-tree host decode -> (error, [int32 [n,64] per component])."""
+    _, gpu = _load_ref()
+    r = gpu.refgpu_new()
+    try:
+        err = gpu.refgpu_open(r, path.encode())
+        if err:
+            return err, []
+        info = np.zeros(18, np.int32)
+        gpu.refgpu_info(r, info.ctypes.data)
+        out = []
+        for c in range(int(info[2])):
+            n = int(info[8 + 4 * c])
+            a = np.empty(n, np.int32)
+            gpu.refgpu_coefs(r, c, a.ctypes.data)
+            out.append(a.reshape(-1, 64))
+        return 0, out
+    finally:
+        gpu.refgpu_del(r)
+
+
+def ref_cpu_bench(paths, iters: int, threads: int):
+    """Time the reference CPUonly decoder: (seconds, pixels, failures)."""
+    cpu, _ = _load_ref()
+    arr = (C.c_char_p * len(paths))(*[p.encode() for p in paths])
+    px = C.c_longlong(0)
+    fails = C.c_int(0)
+    secs = cpu.refcpu_bench(arr, len(paths), iters, threads, C.byref(px), C.byref(fails))
+    return secs, px.value, fails.value
