@@ -44,6 +44,9 @@ EXPORTED = [
     "cjReaderStageTimes", "cjReaderDeviceCoefficients", "cjReaderDeviceQuantTable",
     "cjReaderStream", "cjDebugHuffDecode", "cjReaderRedecodeDevice", "cjReaderSync",
     "cjReaderDevicePixels", "cjReaderSetProfile", "cjReaderKernelTimes", "cjReaderLaunchCount",
+    "cjBatchCreate", "cjBatchDestroy", "cjBatchSetSubsequenceBits", "cjBatchStage", "cjBatchRun",
+    "cjBatchFetch", "cjBatchWait", "cjBatchDecode", "cjBatchImage", "cjBatchDeviceImage",
+    "cjBatchStream", "cjBatchStats", "cjBatchKernelMs",
 ]
 
 KERNEL_NAMES = ["k_destuff_count", "k_scan_tiles", "k_destuff_scatter", "k_build_segments",
@@ -103,6 +106,24 @@ def load(build_if_missing: bool = True):
     lib.cjReaderKernelTimes.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int]
     lib.cjReaderLaunchCount.restype = C.c_longlong
     lib.cjReaderLaunchCount.argtypes = [vp]
+    lib.cjBatchCreate.restype = vp
+    lib.cjBatchDestroy.argtypes = [vp]
+    lib.cjBatchSetSubsequenceBits.argtypes = [vp, C.c_int]
+    lib.cjBatchStage.argtypes = [vp, C.c_int, vp, vp, vp]
+    lib.cjBatchRun.argtypes = [vp]
+    lib.cjBatchFetch.argtypes = [vp]
+    lib.cjBatchWait.argtypes = [vp, vp]
+    lib.cjBatchDecode.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+    lib.cjBatchImage.restype = vp
+    lib.cjBatchImage.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                 C.POINTER(C.c_int)]
+    lib.cjBatchDeviceImage.restype = vp
+    lib.cjBatchDeviceImage.argtypes = [vp, C.c_int]
+    lib.cjBatchStream.restype = vp
+    lib.cjBatchStream.argtypes = [vp]
+    lib.cjBatchStats.argtypes = [vp, i64p]
+    lib.cjBatchKernelMs.restype = C.c_float
+    lib.cjBatchKernelMs.argtypes = [vp]
     _lib = lib
     return lib
 
@@ -231,6 +252,109 @@ class Reader:
         n = C.c_int64(0)
         p = self.lib.cjReaderDeviceCoefficients(self.ptr, C.byref(n))
         return p, n.value
+
+
+class Batch:
+    """The batched decoder (cudajpeg.h cjBatch*): one persistent kernel per
+    batch of JPEGs of any size / subsampling / restart structure."""
+
+    STAT_KEYS = ["submitted", "on_device", "grid", "warp_items", "destuff_tiles", "pixel_tiles",
+                 "passes", "input_bytes", "output_bytes", "smem", "launches"]
+
+    def __init__(self, sub_bits: int = 0):
+        self.lib = load()
+        self.ptr = self.lib.cjBatchCreate()
+        if not self.ptr:
+            raise MemoryError("cjBatchCreate failed")
+        if sub_bits and self.lib.cjBatchSetSubsequenceBits(self.ptr, sub_bits):
+            raise ValueError(f"bad subsequence size {sub_bits}")
+        self.n = 0
+        self._keep = None
+
+    def close(self):
+        if self.ptr:
+            self.lib.cjBatchDestroy(self.ptr)
+            self.ptr = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def pack(files) -> tuple:
+        """Concatenate JPEG byte strings -> (blob uint8 array, offsets, sizes)."""
+        sizes = np.array([len(f) for f in files], np.int64)
+        offsets = np.zeros(len(files), np.int64)
+        if len(files):
+            offsets[1:] = np.cumsum(sizes)[:-1]
+        blob = np.frombuffer(b"".join(files), np.uint8) if files else np.zeros(1, np.uint8)
+        return blob, offsets, sizes
+
+    def stage(self, blob_ptr: int, offsets: np.ndarray, sizes: np.ndarray):
+        offsets = np.ascontiguousarray(offsets, np.int64)
+        sizes = np.ascontiguousarray(sizes, np.int64)
+        self._keep = (offsets, sizes)
+        self.n = len(sizes)
+        err = self.lib.cjBatchStage(self.ptr, self.n, C.c_void_p(blob_ptr), offsets.ctypes.data,
+                                    sizes.ctypes.data)
+        if err:
+            raise DecodeError(err, "cjBatchStage")
+
+    def run(self):
+        err = self.lib.cjBatchRun(self.ptr)
+        if err:
+            raise DecodeError(err, "cjBatchRun")
+
+    def fetch(self):
+        err = self.lib.cjBatchFetch(self.ptr)
+        if err:
+            raise DecodeError(err, "cjBatchFetch")
+
+    def wait(self) -> list:
+        errs = np.zeros(max(self.n, 1), np.int32)
+        err = self.lib.cjBatchWait(self.ptr, errs.ctypes.data)
+        if err:
+            raise DecodeError(err, "cjBatchWait")
+        return [int(e) for e in errs[: self.n]]
+
+    def image(self, i: int, copy: bool = True):
+        w, h, c = C.c_int(0), C.c_int(0), C.c_int(0)
+        p = self.lib.cjBatchImage(self.ptr, i, C.byref(w), C.byref(h), C.byref(c))
+        if not p:
+            return None
+        n = w.value * h.value * c.value
+        arr = np.frombuffer((C.c_uint8 * n).from_address(p), np.uint8)
+        arr = arr.reshape((h.value, w.value, 3) if c.value == 3 else (h.value, w.value))
+        return arr.copy() if copy else arr
+
+    def decode(self, files) -> tuple:
+        """Decode a list of JPEG byte strings -> (list of arrays or None, errors)."""
+        blob, offsets, sizes = self.pack(files)
+        self._blob = blob
+        self.stage(blob.ctypes.data, offsets, sizes)
+        self.run()
+        self.fetch()
+        errs = self.wait()
+        return [self.image(i) if not e else None for i, e in enumerate(errs)], errs
+
+    def stats(self) -> dict:
+        a = (C.c_int64 * 11)()
+        self.lib.cjBatchStats(self.ptr, a)
+        return dict(zip(self.STAT_KEYS, [int(v) for v in a]))
+
+    def kernel_ms(self) -> float:
+        return float(self.lib.cjBatchKernelMs(self.ptr))
+
+    def stream(self) -> int:
+        return self.lib.cjBatchStream(self.ptr)
 
 
 # ---- JPGReader field access for the few fields ctypes needs (layout of

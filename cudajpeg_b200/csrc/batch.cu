@@ -1,0 +1,933 @@
+// batch.cu -- persistent, cooperative batch decoder: many JPEGs of uneven
+// size, subsampling and restart structure decoded by ONE kernel launch.
+//
+// The whole decode path of scan.cu + pixel.cu runs as phases of a single
+// cooperative kernel (every CTA co-resident), separated by a grid barrier:
+//
+//   0 tables     build each image's canonical Huffman tables and geometry on
+//                the device from its raw DHT/DQT bytes
+//   1-3 destuff  count / per-image scan / scatter of every 4 KiB tile
+//   4 segments   restart intervals -> segments -> speculative subsequences
+//   5 sync       speculative decode + warp settle (every warp item)
+//   6 fix-up     passes between warps until no warp's exit moves; the loop is
+//                driven on the device, no host round trip
+//   7 scan       segmented block / DC prefix over warps
+//   8 write      coefficient write-out
+//   9 pixel      TMA-staged integer iDCT + upsample + colour per MCU tile
+//
+// Work items are grid-strided, so a warp item is always handled by the same
+// persistent warp in phases 5, 6 and 8.  Data one CTA writes and another
+// reads inside the kernel is read with L2-coherent loads (__ldcg).  Errors
+// are kept per image: a corrupt image fails alone.
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <thread>
+#include <vector>
+
+#include "../../include/cudajpeg.h"
+#include "cj_entropy.cuh"
+#include "cj_idct.cuh"
+#include "cj_internal.h"
+#include "cj_pixel.cuh"
+#include "cj_scan_util.cuh"
+#include "cj_tables.h"
+
+#define BT_THREADS 256
+#define BT_WARPS (BT_THREADS / 32)
+#define BT_TILE_BYTES 4096  // destuff tile: 256 threads x 16 bytes
+
+// ---------------------------------------------------------------- layouts
+
+// What the host parse of one image hands the device.
+struct CJImageHeader {
+  uint8_t counts[4][16];    // DHT BITS per table slot
+  uint8_t symbols[4][256];  // DHT HUFFVAL per table slot
+  uint8_t dq[4][64];        // DQT, zig-zag order
+  uint8_t comp_dc[3], comp_ac[3], comp_q[3], comp_sx[3], comp_sy[3];
+  uint8_t nch, huff_mask, xshift, yshift, pad[4];
+  int32_t mcux, mcuy, width, height, hmax, vmax, restart_interval, nseg_expected;
+  int64_t total_blocks;
+};
+
+// Where one image's data lives in the batch buffers (host-planned).
+struct CJImageDesc {
+  int64_t src_off, raw_len;  // entropy-coded bytes in the input blob
+  int64_t data_off;          // destuffed bytes (16-byte aligned)
+  int32_t tile0, ntiles;     // destuff tiles
+  int32_t mark0, mark_cap;   // RSTn positions
+  int32_t seg0, seg_cap;     // segments
+  int32_t sub0, sub_cap;     // subsequences (multiples of 32)
+  int32_t ptile0, nptiles;   // pixel tiles
+  int32_t T, sub_bits;       // MCUs per pixel tile; bits per subsequence
+  int64_t coef0;             // first block in the coefficient buffer
+  int64_t out_off;           // output byte offset
+};
+
+struct CJBatchCtl {
+  unsigned bar_count, bar_gen;
+  int unstable[3];
+  int timeout;
+  int passes;
+  int pad;
+};
+
+struct CJBatchArgs {
+  const CJImageHeader* hdr;
+  const CJImageDesc* desc;
+  CJScanParams* prm;
+  CJStatus* st;
+  const uint8_t* blob;
+  uint8_t* data;
+  int32_t* tile_keep;
+  int32_t* tile_mark;
+  uint32_t* mpos;
+  uint8_t* mcode;
+  CJSegment* segs;
+  CJSubRec* recs;
+  uint64_t* snap0;
+  uint64_t* snap1;
+  CJWarpAgg* wagg;
+  CJWarpAgg* carry;
+  int16_t* coef;
+  uint8_t* out;
+  CJBatchCtl* ctl;
+  int n, ntiles, nwarps, nptiles, max_passes;
+};
+
+// ---------------------------------------------------------------- device helpers
+
+__device__ __forceinline__ void bt_raise(CJStatus* st, int64_t block, int code) {
+  atomicMax(&st->err_key, ~(((unsigned long long)block << 8) | (unsigned)code));
+}
+__device__ __forceinline__ void bt_raise_dec(CJStatus* st, int64_t block, int code) {
+  atomicMax(&st->dec_err_key, ~(((unsigned long long)block << 8) | (unsigned)code));
+}
+
+// Grid barrier for a cooperative launch (all CTAs co-resident).  The wait is
+// bounded: on timeout the batch is flagged and the CTA carries on, so the
+// kernel always terminates.
+__device__ __forceinline__ void bt_grid_sync(CJBatchCtl* ctl, unsigned& gen) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned g = gen;
+    if (atomicAdd(&ctl->bar_count, 1) == gridDim.x - 1) {
+      atomicExch(&ctl->bar_count, 0);
+      __threadfence();
+      atomicAdd(&ctl->bar_gen, 1);
+    } else {
+      unsigned it = 0;
+      while (atomicAdd(&ctl->bar_gen, 0) == g) {
+        if (++it > (1u << 24)) {
+          atomicExch(&ctl->timeout, 1);
+          break;
+        }
+        __nanosleep(128);
+      }
+    }
+    __threadfence();
+    gen = g + 1;
+  }
+  __syncthreads();
+}
+
+// Largest i with key(i) <= v over a sorted int32 field of the descriptors.
+template <class F>
+__device__ __forceinline__ int bt_find(int n, int v, F key) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (key(mid) <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Phase 0: one CTA builds one image's CJScanParams (the device twin of
+// cj_build_huff + cj_fill_params).
+__device__ void bt_build_params(const CJImageHeader& h, CJScanParams& p) {
+  for (int e = threadIdx.x; e < 4 * (1 << CJ_FAST_BITS); e += blockDim.x) {
+    int slot = e >> CJ_FAST_BITS, f = e & ((1 << CJ_FAST_BITS) - 1);
+    uint16_t out = 0;
+    if (h.huff_mask & (1 << slot)) {
+      int code = 0, k = 0;
+      for (int l = 1; l <= CJ_FAST_BITS; l++) {
+        int n = h.counts[slot][l - 1];
+        int c = f >> (CJ_FAST_BITS - l);
+        if (c >= code && c < code + n) {
+          out = (uint16_t)((l << 8) | h.symbols[slot][k + c - code]);
+          break;
+        }
+        k += n;
+        code = (code + n) << 1;
+      }
+    }
+    p.huff[slot].fast[f] = out;
+  }
+  for (int e = threadIdx.x; e < 4 * 256; e += blockDim.x) p.huff[e >> 8].vals[e & 255] = h.symbols[e >> 8][e & 255];
+  if (threadIdx.x < 4) {
+    int slot = threadIdx.x;
+    int code = 0, k = 0;
+    p.huff[slot].maxcode[0] = -1;
+    p.huff[slot].valoff[0] = 0;
+    for (int l = 1; l <= 16; l++) {
+      int n = h.counts[slot][l - 1];
+      p.huff[slot].valoff[l] = k - code;
+      code += n;
+      k += n;
+      p.huff[slot].maxcode[l] = n ? code - 1 : -1;
+      code <<= 1;
+    }
+    p.huff[slot].maxcode[17] = -1;
+    p.huff[slot].valoff[17] = 0;
+  }
+  const uint8_t zz[64] = CJ_ZIGZAG_INIT;
+  for (int e = threadIdx.x; e < 4 * 64; e += blockDim.x) p.qnat[e >> 6][zz[e & 63]] = h.dq[e >> 6][e & 63];
+  if (threadIdx.x < 64) p.zz[threadIdx.x] = zz[threadIdx.x];
+  if (threadIdx.x == 0) {
+    int k = 0;
+    for (int c = 0; c < h.nch; c++)
+      for (int j = 0; j < h.comp_sx[c] * h.comp_sy[c]; j++, k++) {
+        p.phase_comp[k] = (uint8_t)c;
+        p.phase_blk[k] = (uint8_t)j;
+      }
+    for (int c = 0; c < 3; c++) {
+      p.comp_dc[c] = h.comp_dc[c];
+      p.comp_ac[c] = h.comp_ac[c];
+      p.comp_q[c] = h.comp_q[c];
+      p.comp_sx[c] = h.comp_sx[c];
+      p.comp_sy[c] = h.comp_sy[c];
+      p.comp_stride[c] = h.mcux * h.comp_sx[c] * 8;
+      p.comp_rows[c] = h.mcuy * h.comp_sy[c] * 8;
+    }
+    p.nch = h.nch;
+    p.bpm = k;
+    p.mcux = h.mcux;
+    p.mcuy = h.mcuy;
+    p.width = h.width;
+    p.height = h.height;
+    p.hmax = h.hmax;
+    p.vmax = h.vmax;
+    p.xshift = h.xshift;
+    p.yshift = h.yshift;
+    p.restart_interval = h.restart_interval;
+    p.nseg_expected = h.nseg_expected;
+    p.total_blocks = h.total_blocks;
+  }
+}
+
+// ---------------------------------------------------------------- the kernel
+
+__device__ __forceinline__ uint32_t bt_smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ uint64_t bar;
+  __shared__ int2 sm2[33];
+  __shared__ CJPixSmemParams P;
+  unsigned gen = 0;
+  if (threadIdx.x == 0) {
+    gen = atomicAdd(&a.ctl->bar_gen, 0);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bt_smem_addr(&bar)), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  const int lane = threadIdx.x & 31;
+  const int gwarp0 = blockIdx.x * BT_WARPS + (threadIdx.x >> 5);
+  const int gwarps = gridDim.x * BT_WARPS;
+
+  // ---- phase 0: tables + status
+  for (int i = blockIdx.x; i < a.n; i += gridDim.x) {
+    bt_build_params(a.hdr[i], a.prm[i]);
+    if (threadIdx.x == 0) {
+      CJStatus z;
+      memset(&z, 0, sizeof(z));
+      a.st[i] = z;
+    }
+  }
+  bt_grid_sync(a.ctl, gen);
+
+  // ---- phase 1: destuff count
+  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    int i = bt_find(a.n, t, [&](int k) { return a.desc[k].tile0; });
+    const CJImageDesc& d = a.desc[i];
+    int64_t base = (int64_t)(t - d.tile0) * BT_TILE_BYTES + threadIdx.x * 16;
+    CJChunk c = cj_classify(a.blob + d.src_off, d.raw_len, base);
+    int2 tot;
+    cj_block_exclusive(make_int2(__popc(c.keep), __popc(c.mark)), sm2, &tot);
+    if (threadIdx.x == 0) {
+      a.tile_keep[t] = tot.x;
+      a.tile_mark[t] = tot.y;
+    }
+    if (c.bad) bt_raise(&a.st[i], 0, CJ_DEV_MARKER);
+  }
+  bt_grid_sync(a.ctl, gen);
+
+  // ---- phase 2: per-image tile offsets
+  for (int i = blockIdx.x; i < a.n; i += gridDim.x) {
+    const CJImageDesc& d = a.desc[i];
+    int2 run = make_int2(0, 0);
+    for (int t0 = 0; t0 < d.ntiles; t0 += blockDim.x) {
+      int t = t0 + threadIdx.x;
+      int2 v = make_int2(0, 0);
+      if (t < d.ntiles) v = make_int2(__ldcg(&a.tile_keep[d.tile0 + t]), __ldcg(&a.tile_mark[d.tile0 + t]));
+      int2 tot;
+      int2 ex = cj_block_exclusive(v, sm2, &tot);
+      if (t < d.ntiles) {
+        a.tile_keep[d.tile0 + t] = run.x + ex.x;
+        a.tile_mark[d.tile0 + t] = run.y + ex.y;
+      }
+      run.x += tot.x;
+      run.y += tot.y;
+    }
+    if (threadIdx.x == 0) {
+      a.st[i].destuffed = run.x;
+      a.st[i].nmarkers = run.y;
+    }
+  }
+  bt_grid_sync(a.ctl, gen);
+
+  // ---- phase 3: destuff scatter
+  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    int i = bt_find(a.n, t, [&](int k) { return a.desc[k].tile0; });
+    const CJImageDesc& d = a.desc[i];
+    int64_t base = (int64_t)(t - d.tile0) * BT_TILE_BYTES + threadIdx.x * 16;
+    CJChunk c = cj_classify(a.blob + d.src_off, d.raw_len, base);
+    int2 tot;
+    int2 ex = cj_block_exclusive(make_int2(__popc(c.keep), __popc(c.mark)), sm2, &tot);
+    int64_t o = (int64_t)__ldcg(&a.tile_keep[t]) + ex.x;
+    int r = __ldcg(&a.tile_mark[t]) + ex.y;
+    uint8_t* out = a.data + d.data_off;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      if (c.keep & (1u << j)) out[o++] = (uint8_t)cj_byte(c, j);
+      if (c.mark & (1u << j)) {
+        if (r < d.mark_cap) {
+          a.mpos[d.mark0 + r] = (uint32_t)o;
+          a.mcode[d.mark0 + r] = (uint8_t)(j < 15 ? cj_byte(c, j + 1) : c.next);
+        }
+        r++;
+      }
+    }
+  }
+  bt_grid_sync(a.ctl, gen);
+
+  // ---- phase 4: segments and subsequences, one CTA per image
+  for (int i = blockIdx.x; i < a.n; i += gridDim.x) {
+    const CJImageDesc& d = a.desc[i];
+    const CJScanParams& p = a.prm[i];
+    CJStatus* st = &a.st[i];
+    const int M = __ldcg(&st->nmarkers);
+    const int64_t L = __ldcg(&st->destuffed);
+    const int RI = __ldcg(&p.restart_interval);
+    const int E = RI ? __ldcg(&p.nseg_expected) : 1;
+    const int64_t total = __ldcg(&p.total_blocks);
+    const int64_t per_seg = RI ? (int64_t)RI * __ldcg(&p.bpm) : total;
+    const uint32_t* mpos = a.mpos + d.mark0;
+    const uint8_t* mcode = a.mcode + d.mark0;
+    bool ok;
+    if (RI == 0) ok = (M == 0);
+    else if (M == E - 1) ok = true;
+    else if (M == E && M <= d.mark_cap && __ldcg(&mpos[M - 1]) == (uint32_t)L) ok = true;
+    else ok = false;
+    if (M > d.mark_cap || E > d.seg_cap) ok = false;
+    if (!ok) {
+      if (threadIdx.x == 0) {
+        bt_raise(st, 0, CJ_DEV_MARKER);
+        st->nsub = 0;
+        st->nseg = 0;
+      }
+      continue;
+    }
+    int running = 0;
+    for (int k0 = 0; k0 < E; k0 += blockDim.x) {
+      int k = k0 + threadIdx.x;
+      int64_t begin = 0, end = 0;
+      int nsub = 0;
+      if (k < E) {
+        begin = k ? __ldcg(&mpos[k - 1]) : 0;
+        end = k < M ? (int64_t)__ldcg(&mpos[k]) : L;
+        if (k < M && __ldcg(&mcode[k]) != 0xD0 + (k & 7)) bt_raise(st, (int64_t)k * per_seg, CJ_DEV_MARKER);
+        nsub = (int)(((end - begin) * 8 + d.sub_bits - 1) / d.sub_bits);
+        if (nsub < 1) nsub = 1;
+      }
+      int2 tot;
+      int2 ex = cj_block_exclusive(make_int2(nsub, 0), sm2, &tot);
+      if (k < E) {
+        CJSegment s;
+        s.bit_begin = (uint64_t)begin * 8;
+        s.bit_end = (uint64_t)end * 8;
+        s.first_block = (int64_t)k * per_seg;
+        s.nblocks = min(per_seg, total - s.first_block);
+        s.first_sub = running + ex.x;
+        s.nsub = nsub;
+        s.marker_follows = k < M;
+        s.pad = 0;
+        a.segs[d.seg0 + k] = s;
+      }
+      running += tot.x;
+    }
+    if (threadIdx.x == 0) {
+      st->nseg = E;
+      if (running > d.sub_cap) {
+        bt_raise(st, 0, CJ_DEV_CAPACITY);
+        running = 0;
+      }
+      st->nsub = running;
+    }
+  }
+  bt_grid_sync(a.ctl, gen);
+
+  // ---- phase 5: speculative decode + warp settle
+  for (int w = gwarp0; w < a.nwarps; w += gwarps) {
+    int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
+    const CJImageDesc& d = a.desc[i];
+    const int nsub = __ldcg(&a.st[i].nsub), nseg = __ldcg(&a.st[i].nseg);
+    const int j0 = w * 32 - d.sub0;
+    if (j0 >= nsub) continue;  // warp-uniform
+    const CJScanParams& sp = a.prm[i];
+    const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
+    CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
+    CJSubRec r;
+    r.start = cj_state(ln.begin, 0);
+    r.exit = r.start;
+    r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
+    if (ln.active) r = cj_spec_decode(sp, words, ln, r.start);
+    cj_warp_settle(sp, words, ln, r, r.start);
+    if (ln.active) a.recs[d.sub0 + j0 + lane] = r;
+    unsigned act = __ballot_sync(CJ_FULL, ln.active);
+    if (lane == 31 - __clz(act)) a.snap0[w] = r.exit;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.ctl->unstable[0] = 0;
+    a.ctl->unstable[1] = 0;
+  }
+  bt_grid_sync(a.ctl, gen);
+
+  // ---- phase 6: fix-up passes until no warp's last exit moves
+  int pass = 0;
+  for (; pass < a.max_passes; pass++) {
+    const uint64_t* snap_in = (pass & 1) ? a.snap1 : a.snap0;
+    uint64_t* snap_out = (pass & 1) ? a.snap0 : a.snap1;
+    int* unstable = &a.ctl->unstable[pass % 3];
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->unstable[(pass + 1) % 3] = 0;
+    for (int w = gwarp0; w < a.nwarps; w += gwarps) {
+      int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
+      const CJImageDesc& d = a.desc[i];
+      const int nsub = __ldcg(&a.st[i].nsub), nseg = __ldcg(&a.st[i].nseg);
+      const int j0 = w * 32 - d.sub0;
+      if (j0 >= nsub) {
+        if (lane == 0) {
+          CJWarpAgg z;
+          memset(&z, 0, sizeof(z));
+          a.wagg[w] = z;
+        }
+        continue;
+      }
+      const CJScanParams& sp = a.prm[i];
+      const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
+      CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
+      CJSubRec r;
+      if (ln.active) r = a.recs[d.sub0 + j0 + lane];
+      else {
+        r.start = r.exit = 0;
+        r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
+      }
+      uint64_t in0 = (j0 > 0 && lane == 0) ? __ldcg(&snap_in[w - 1]) : r.start;
+      if (cj_warp_settle(sp, words, ln, r, in0) && ln.active) a.recs[d.sub0 + j0 + lane] = r;
+      unsigned act = __ballot_sync(CJ_FULL, ln.active);
+      if (lane == 31 - __clz(act)) {
+        if (r.exit != __ldcg(&snap_in[w])) atomicAdd(unstable, 1);
+        snap_out[w] = r.exit;
+      }
+      unsigned heads = __ballot_sync(CJ_FULL, ln.active && ln.head);
+      int h = heads ? 31 - __clz(heads) : 0;
+      bool use = ln.active && lane >= h;
+      int v0 = use ? r.nblocks : 0, v1 = use ? r.dc[0] : 0, v2 = use ? r.dc[1] : 0,
+          v3 = use ? r.dc[2] : 0;
+#pragma unroll
+      for (int dd = 16; dd; dd >>= 1) {
+        v0 += __shfl_xor_sync(CJ_FULL, v0, dd);
+        v1 += __shfl_xor_sync(CJ_FULL, v1, dd);
+        v2 += __shfl_xor_sync(CJ_FULL, v2, dd);
+        v3 += __shfl_xor_sync(CJ_FULL, v3, dd);
+      }
+      if (lane == 0) {
+        CJWarpAgg g;
+        g.has_head = heads != 0;
+        g.nblocks = v0;
+        g.dc[0] = v1;
+        g.dc[1] = v2;
+        g.dc[2] = v3;
+        g.pad[0] = g.pad[1] = g.pad[2] = 0;
+        a.wagg[w] = g;
+      }
+    }
+    bt_grid_sync(a.ctl, gen);
+    if (atomicAdd(unstable, 0) == 0) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->passes = pass + 1;
+  // the last pass wrote its exits into the other snapshot; nothing reads them
+
+  // ---- phase 7: segmented scan of the warp aggregates (CTA 0)
+  if (blockIdx.x == 0) {
+    CJAgg5* sm = reinterpret_cast<CJAgg5*>(smem);  // BT_THREADS entries
+    const int nw = a.nwarps;
+    int per = (nw + blockDim.x - 1) / blockDim.x;
+    int lo = threadIdx.x * per, hi = min(nw, lo + per);
+    CJAgg5 acc = {0, 0, 0, 0, 0};
+    for (int w = lo; w < hi; w++) {
+      CJWarpAgg g = a.wagg[w];
+      acc = cj_op(acc, CJAgg5{g.has_head, g.nblocks, g.dc[0], g.dc[1], g.dc[2]});
+    }
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    for (int dd = 1; dd < (int)blockDim.x; dd <<= 1) {
+      CJAgg5 x = sm[threadIdx.x];
+      CJAgg5 y = threadIdx.x >= (unsigned)dd ? sm[threadIdx.x - dd] : CJAgg5{0, 0, 0, 0, 0};
+      __syncthreads();
+      if (threadIdx.x >= (unsigned)dd) sm[threadIdx.x] = cj_op(y, x);
+      __syncthreads();
+    }
+    CJAgg5 run = threadIdx.x ? sm[threadIdx.x - 1] : CJAgg5{0, 0, 0, 0, 0};
+    for (int w = lo; w < hi; w++) {
+      CJWarpAgg o;
+      o.has_head = run.f;
+      o.nblocks = run.n;
+      o.dc[0] = run.a;
+      o.dc[1] = run.b;
+      o.dc[2] = run.c;
+      o.pad[0] = o.pad[1] = o.pad[2] = 0;
+      a.carry[w] = o;
+      CJWarpAgg g = a.wagg[w];
+      run = cj_op(run, CJAgg5{g.has_head, g.nblocks, g.dc[0], g.dc[1], g.dc[2]});
+    }
+  }
+  bt_grid_sync(a.ctl, gen);
+
+  // ---- phase 8: coefficient write-out
+  for (int w = gwarp0; w < a.nwarps; w += gwarps) {
+    int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
+    const CJImageDesc& d = a.desc[i];
+    CJStatus* st = &a.st[i];
+    const int nsub = __ldcg(&st->nsub), nseg = __ldcg(&st->nseg);
+    const int j0 = w * 32 - d.sub0;
+    if (j0 >= nsub) continue;
+    const CJScanParams& sp = a.prm[i];
+    const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
+    CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
+    CJSubRec r;
+    if (ln.active) r = a.recs[d.sub0 + j0 + lane];
+    else {
+      r.start = r.exit = 0;
+      r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
+    }
+    int64_t b;
+    int dc0, dc1, dc2;
+    cj_warp_prefix(r, ln, __ldcg(&a.carry[w].nblocks), __ldcg(&a.carry[w].dc[0]),
+                   __ldcg(&a.carry[w].dc[1]), __ldcg(&a.carry[w].dc[2]), &b, &dc0, &dc1, &dc2);
+    if (!ln.active) continue;
+    const CJSegment seg = a.segs[d.seg0 + ln.seg];
+    cj_write_lane(sp, words, ln, seg, r, b + seg.first_block, dc0, dc1, dc2,
+                  a.coef + d.coef0 * 64, st);
+  }
+  bt_grid_sync(a.ctl, gen);
+
+  // ---- phase 9: pixel tiles
+  uint32_t parity = 0;
+  for (int t = blockIdx.x; t < a.nptiles; t += gridDim.x) {
+    int i = bt_find(a.n, t, [&](int k) { return a.desc[k].ptile0; });
+    const CJImageDesc& d = a.desc[i];
+    const CJScanParams& prm = a.prm[i];
+    CJPixGeom g;
+    g.nch = prm.nch;
+    g.bpm = prm.bpm;
+    g.mcux = prm.mcux;
+    g.mcuy = prm.mcuy;
+    g.width = prm.width;
+    g.height = prm.height;
+    g.hmax = prm.hmax;
+    g.vmax = prm.vmax;
+    g.xs = prm.xshift;
+    g.ys = prm.yshift;
+    g.T = d.T;
+    cj_pix_layout(&g, prm.comp_sx[1], prm.comp_sy[1]);
+    const int gx = (g.mcux + g.T - 1) / g.T;
+    const int local = t - d.ptile0;
+    if (!cj_pixel_tile(prm, a.coef + d.coef0 * 64, a.out + d.out_off, &a.st[i], g, local / gx,
+                       (local % gx) * g.T, smem, &bar, parity, &P))
+      break;
+    parity ^= 1;
+  }
+}
+
+// ---------------------------------------------------------------- host side
+
+struct CJBatch {
+  bool ready = false;
+  int device = 0, sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int sub_bits = CJ_SUB_BITS_DEFAULT;
+  JPGReader* parser = nullptr;  // host marker parse, one image at a time
+  // device buffers (grow-only)
+  CJDevBuf hdr, desc, prm, st, blob, data, tile_keep, tile_mark, mpos, mcode, segs, recs, snap,
+      wagg, carry, coef, out, ctl;
+  // pinned host staging
+  CJHostBuf h_hdr, h_desc, h_out, h_st, h_ctl;
+  // plan of the staged batch
+  int n_in = 0, n_dev = 0;
+  std::vector<int> dev_of;     // device slot of each submitted image, -1 if rejected
+  std::vector<int> host_err;   // host-side (parse) error of each submitted image
+  std::vector<int> dims;       // width, height, channels per device slot
+  std::vector<int64_t> outoff; // output offset per device slot
+  int ntiles = 0, nwarps = 0, nptiles = 0;
+  int64_t blob_bytes = 0, out_total = 0;
+  size_t smem = 0;
+  int grid = 0;
+  long long launches = 0;
+};
+
+static int bt_init(CJBatch* b) {
+  if (b->ready) return 0;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    fprintf(stderr, "libcudajpeg: no CUDA device available; the decoder has no CPU path\n");
+    return CUDA_MEM_ERROR;
+  }
+  CJ_CUDA_TRY(cudaGetDevice(&b->device), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, b->device),
+              CUDA_MEM_ERROR);
+  int coop = 0;
+  CJ_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->device), CUDA_MEM_ERROR);
+  if (!coop) return UNSUPPORTED_ERROR;
+  CJ_CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaEventCreate(&b->ev0), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaEventCreate(&b->ev1), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaFuncSetAttribute(k_decode_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
+              CUDA_MEM_ERROR);
+  b->parser = newJPGReader();
+  if (!b->parser) return OOM_ERROR;
+  b->ready = true;
+  return 0;
+}
+
+// Host parse of one file up to its scan; fills the device header.
+static int bt_parse(CJBatch* b, const unsigned char* data, size_t size, CJImageHeader* h,
+                    int64_t* scan_off, int64_t* scan_len) {
+  JPGReader* r = b->parser;
+  r->huff_defined = 0;  // images of a batch are independent
+  int e = cj_parse_to_scan(r, data, size);
+  if (e) return e;
+  memset(h, 0, sizeof(*h));
+  for (int s = 0; s < 4; s++) {
+    memcpy(h->counts[s], r->dev->huff[s].counts, 16);
+    memcpy(h->symbols[s], r->dev->huff[s].symbols, 256);
+  }
+  h->huff_mask = (uint8_t)r->huff_defined;
+  memcpy(h->dq, r->dq_tables, sizeof(h->dq));
+  h->nch = r->num_channels;
+  for (int c = 0; c < r->num_channels; c++) {
+    h->comp_dc[c] = (uint8_t)r->channels[c].dc_id;
+    h->comp_ac[c] = (uint8_t)r->channels[c].ac_id;
+    h->comp_q[c] = (uint8_t)r->channels[c].dq_id;
+    h->comp_sx[c] = (uint8_t)r->channels[c].samples_x;
+    h->comp_sy[c] = (uint8_t)r->channels[c].samples_y;
+  }
+  h->mcux = r->num_blocks_x;
+  h->mcuy = r->num_blocks_y;
+  h->width = r->width;
+  h->height = r->height;
+  h->hmax = r->block_size_x >> 3;
+  h->vmax = r->block_size_y >> 3;
+  int xs = 0, ys = 0;
+  if (r->num_channels == 3) {
+    while ((r->channels[1].width << xs) < r->width) xs++;
+    while ((r->channels[1].height << ys) < r->height) ys++;
+  }
+  h->xshift = (uint8_t)xs;
+  h->yshift = (uint8_t)ys;
+  h->restart_interval = r->restart_interval;
+  int64_t mcus = (int64_t)h->mcux * h->mcuy;
+  h->nseg_expected = r->restart_interval ? (int)((mcus + r->restart_interval - 1) / r->restart_interval) : 1;
+  int bpm = 0;
+  for (int c = 0; c < h->nch; c++) bpm += h->comp_sx[c] * h->comp_sy[c];
+  h->total_blocks = mcus * bpm;
+  // the pixel tile layout's geometry condition (cj_pix_check)
+  if (h->comp_sx[0] != h->hmax || h->comp_sy[0] != h->vmax) return UNSUPPORTED_ERROR;
+  if (h->nch == 3 && ((h->comp_sx[1] << xs) != h->hmax || (h->comp_sy[1] << ys) != h->vmax))
+    return UNSUPPORTED_ERROR;
+  *scan_off = (int64_t)(r->pos - data);
+  *scan_len = (int64_t)(r->end - r->pos);
+  return 0;
+}
+
+extern "C" {
+
+CJBatch* cjBatchCreate(void) { return new (std::nothrow) CJBatch(); }
+
+void cjBatchDestroy(CJBatch* b) {
+  if (!b) return;
+  if (b->ready) {
+    cudaStreamSynchronize(b->stream);
+    CJDevBuf* bufs[] = {&b->hdr,  &b->desc, &b->prm,   &b->st,   &b->blob,  &b->data,
+                        &b->tile_keep, &b->tile_mark, &b->mpos, &b->mcode, &b->segs,
+                        &b->recs, &b->snap, &b->wagg, &b->carry, &b->coef, &b->out, &b->ctl};
+    for (CJDevBuf* d : bufs)
+      if (d->p) cudaFree(d->p);
+    CJHostBuf* hb[] = {&b->h_hdr, &b->h_desc, &b->h_out, &b->h_st, &b->h_ctl};
+    for (CJHostBuf* h : hb)
+      if (h->p) cudaFreeHost(h->p);
+    cudaEventDestroy(b->ev0);
+    cudaEventDestroy(b->ev1);
+    cudaStreamDestroy(b->stream);
+    delJPGReader(b->parser);
+  }
+  delete b;
+}
+
+int cjBatchSetSubsequenceBits(CJBatch* b, int bits) {
+  if (bits == 0) bits = CJ_SUB_BITS_DEFAULT;
+  if (bits < 128 || bits > 65536 || (bits & 31)) return PROGRAMMER_ERROR;
+  b->sub_bits = bits;
+  return 0;
+}
+
+int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* offsets,
+                 const int64_t* sizes) {
+  int err = bt_init(b);
+  if (err) return err;
+  if (n < 0) return PROGRAMMER_ERROR;
+  b->n_in = n;
+  b->dev_of.assign(n, -1);
+  b->host_err.assign(n, 0);
+  b->dims.clear();
+  b->outoff.clear();
+  int64_t blob_bytes = 0;
+  for (int i = 0; i < n; i++) blob_bytes = std::max(blob_bytes, offsets[i] + sizes[i]);
+  if (cj_host_ensure(b->h_hdr, (size_t)std::max(n, 1) * sizeof(CJImageHeader)) ||
+      cj_host_ensure(b->h_desc, (size_t)std::max(n, 1) * sizeof(CJImageDesc)))
+    return OOM_ERROR;
+  CJImageHeader* hh = (CJImageHeader*)b->h_hdr.p;
+  CJImageDesc* dd = (CJImageDesc*)b->h_desc.p;
+  int nd = 0, ntiles = 0, nsubw = 0, nptiles = 0, nmark = 0, nseg = 0;
+  int64_t data_bytes = 0, blocks = 0, out_total = 0;
+  size_t smem = 8192;
+  for (int i = 0; i < n; i++) {
+    int64_t so = 0, sl = 0;
+    int e = bt_parse(b, blob + offsets[i], (size_t)sizes[i], &hh[nd], &so, &sl);
+    if (!e && (uint64_t)sl > CJ_MAX_SCAN_BYTES) e = UNSUPPORTED_ERROR;
+    if (e) {
+      b->host_err[i] = e;
+      continue;
+    }
+    const CJImageHeader& h = hh[nd];
+    CJImageDesc& d = dd[nd];
+    memset(&d, 0, sizeof(d));
+    d.src_off = offsets[i] + so;
+    d.raw_len = sl;
+    d.data_off = data_bytes;
+    data_bytes += (sl + 16 + 15) & ~(int64_t)15;
+    d.tile0 = ntiles;
+    d.ntiles = (int)((sl + BT_TILE_BYTES - 1) / BT_TILE_BYTES);
+    if (d.ntiles < 1) d.ntiles = 1;
+    ntiles += d.ntiles;
+    d.mark0 = nmark;
+    d.mark_cap = h.nseg_expected + 1;
+    nmark += d.mark_cap;
+    d.seg0 = nseg;
+    d.seg_cap = h.nseg_expected;
+    nseg += d.seg_cap;
+    d.sub_bits = b->sub_bits;
+    int sub_cap = (int)((sl * 8 + b->sub_bits - 1) / b->sub_bits) + h.nseg_expected + 1;
+    sub_cap = (sub_cap + 31) & ~31;
+    d.sub0 = nsubw * 32;
+    d.sub_cap = sub_cap;
+    nsubw += sub_cap / 32;
+    int bpm = (int)(h.total_blocks / ((int64_t)h.mcux * h.mcuy));
+    d.T = cj_pix_tile_mcus(h.hmax, bpm);
+    d.ptile0 = nptiles;
+    d.nptiles = h.mcuy * ((h.mcux + d.T - 1) / d.T);
+    nptiles += d.nptiles;
+    d.coef0 = blocks;
+    blocks += h.total_blocks;
+    d.out_off = out_total;
+    int ch = h.nch == 3 ? 3 : 1;
+    out_total += (int64_t)h.width * h.height * ch;
+    CJPixGeom g;
+    g.nch = h.nch;
+    g.bpm = bpm;
+    g.hmax = h.hmax;
+    g.vmax = h.vmax;
+    g.T = d.T;
+    smem = std::max(smem, cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1]));
+    b->dev_of[i] = nd;
+    b->dims.push_back(h.width);
+    b->dims.push_back(h.height);
+    b->dims.push_back(ch);
+    b->outoff.push_back(d.out_off);
+    nd++;
+  }
+  b->n_dev = nd;
+  b->ntiles = ntiles;
+  b->nwarps = nsubw;
+  b->nptiles = nptiles;
+  b->blob_bytes = blob_bytes;
+  b->out_total = out_total;
+  b->smem = std::max(smem, (size_t)BT_THREADS * sizeof(CJAgg5));
+  if (!nd) return 0;
+  size_t nd_ = (size_t)nd;
+  if (cj_dev_ensure(b->hdr, nd_ * sizeof(CJImageHeader)) || cj_dev_ensure(b->desc, nd_ * sizeof(CJImageDesc)) ||
+      cj_dev_ensure(b->prm, nd_ * sizeof(CJScanParams)) || cj_dev_ensure(b->st, nd_ * sizeof(CJStatus)) ||
+      cj_dev_ensure(b->blob, (size_t)blob_bytes + 64) || cj_dev_ensure(b->data, (size_t)data_bytes + 64) ||
+      cj_dev_ensure(b->tile_keep, (size_t)ntiles * 4) || cj_dev_ensure(b->tile_mark, (size_t)ntiles * 4) ||
+      cj_dev_ensure(b->mpos, (size_t)nmark * 4) || cj_dev_ensure(b->mcode, (size_t)nmark) ||
+      cj_dev_ensure(b->segs, (size_t)nseg * sizeof(CJSegment)) ||
+      cj_dev_ensure(b->recs, (size_t)nsubw * 32 * sizeof(CJSubRec)) ||
+      cj_dev_ensure(b->snap, (size_t)2 * nsubw * sizeof(uint64_t)) ||
+      cj_dev_ensure(b->wagg, (size_t)nsubw * sizeof(CJWarpAgg)) ||
+      cj_dev_ensure(b->carry, (size_t)nsubw * sizeof(CJWarpAgg)) ||
+      cj_dev_ensure(b->coef, (size_t)blocks * 128 + 128) || cj_dev_ensure(b->out, (size_t)out_total + 64) ||
+      cj_dev_ensure(b->ctl, sizeof(CJBatchCtl)))
+    return CUDA_MEM_ERROR;
+  if (cj_host_ensure(b->h_st, nd_ * sizeof(CJStatus)) || cj_host_ensure(b->h_ctl, sizeof(CJBatchCtl)))
+    return OOM_ERROR;
+  cudaStream_t s = b->stream;
+  CJ_CUDA_TRY(cudaMemcpyAsync(b->hdr.p, hh, nd_ * sizeof(CJImageHeader), cudaMemcpyHostToDevice, s),
+              CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaMemcpyAsync(b->desc.p, dd, nd_ * sizeof(CJImageDesc), cudaMemcpyHostToDevice, s),
+              CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaMemcpyAsync(b->blob.p, blob, (size_t)blob_bytes, cudaMemcpyHostToDevice, s),
+              CUDA_MEM_ERROR);
+  int per_sm = 0;
+  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_decode_batch, BT_THREADS, b->smem),
+              CUDA_KERNEL_LAUNCH_ERROR);
+  if (per_sm < 1) return UNSUPPORTED_ERROR;
+  b->grid = per_sm * b->sm_count;
+  return 0;
+}
+
+int cjBatchRun(CJBatch* b) {
+  if (!b->ready) return PROGRAMMER_ERROR;
+  if (!b->n_dev) return 0;
+  CJBatchArgs a;
+  a.hdr = (const CJImageHeader*)b->hdr.p;
+  a.desc = (const CJImageDesc*)b->desc.p;
+  a.prm = (CJScanParams*)b->prm.p;
+  a.st = (CJStatus*)b->st.p;
+  a.blob = (const uint8_t*)b->blob.p;
+  a.data = (uint8_t*)b->data.p;
+  a.tile_keep = (int32_t*)b->tile_keep.p;
+  a.tile_mark = (int32_t*)b->tile_mark.p;
+  a.mpos = (uint32_t*)b->mpos.p;
+  a.mcode = (uint8_t*)b->mcode.p;
+  a.segs = (CJSegment*)b->segs.p;
+  a.recs = (CJSubRec*)b->recs.p;
+  a.snap0 = (uint64_t*)b->snap.p;
+  a.snap1 = a.snap0 + b->nwarps;
+  a.wagg = (CJWarpAgg*)b->wagg.p;
+  a.carry = (CJWarpAgg*)b->carry.p;
+  a.coef = (int16_t*)b->coef.p;
+  a.out = (uint8_t*)b->out.p;
+  a.ctl = (CJBatchCtl*)b->ctl.p;
+  a.n = b->n_dev;
+  a.ntiles = b->ntiles;
+  a.nwarps = b->nwarps;
+  a.nptiles = b->nptiles;
+  a.max_passes = b->nwarps + 2;
+  cudaStream_t s = b->stream;
+  CJ_CUDA_TRY(cudaMemsetAsync(b->ctl.p, 0, sizeof(CJBatchCtl), s), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaEventRecord(b->ev0, s), CUDA_KERNEL_LAUNCH_ERROR);
+  void* args[] = {&a};
+  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_decode_batch, dim3(b->grid), dim3(BT_THREADS), args,
+                                          b->smem, s),
+              CUDA_KERNEL_LAUNCH_ERROR);
+  b->launches++;
+  CJ_CUDA_TRY(cudaEventRecord(b->ev1, s), CUDA_KERNEL_LAUNCH_ERROR);
+  return 0;
+}
+
+int cjBatchFetch(CJBatch* b) {
+  if (!b->ready) return PROGRAMMER_ERROR;
+  if (!b->n_dev) return 0;
+  if (cj_host_ensure(b->h_out, (size_t)b->out_total + 64)) return OOM_ERROR;
+  cudaStream_t s = b->stream;
+  CJ_CUDA_TRY(cudaMemcpyAsync(b->h_out.p, b->out.p, (size_t)b->out_total, cudaMemcpyDeviceToHost, s),
+              CUDA_MEM_ERROR);
+  return 0;
+}
+
+int cjBatchWait(CJBatch* b, int* errors) {
+  if (!b->ready) return PROGRAMMER_ERROR;
+  cudaStream_t s = b->stream;
+  if (b->n_dev) {
+    CJ_CUDA_TRY(cudaMemcpyAsync(b->h_st.p, b->st.p, (size_t)b->n_dev * sizeof(CJStatus),
+                                cudaMemcpyDeviceToHost, s),
+                CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaMemcpyAsync(b->h_ctl.p, b->ctl.p, sizeof(CJBatchCtl), cudaMemcpyDeviceToHost, s),
+                CUDA_MEM_ERROR);
+  }
+  CJ_CUDA_TRY(cudaStreamSynchronize(s), CUDA_KERNEL_LAUNCH_ERROR);
+  const CJBatchCtl* ctl = (const CJBatchCtl*)b->h_ctl.p;
+  int batch_err = 0;
+  if (b->n_dev && (ctl->timeout || ctl->passes > b->nwarps + 2)) batch_err = PROGRAMMER_ERROR;
+  const CJStatus* st = (const CJStatus*)b->h_st.p;
+  if (errors)
+    for (int i = 0; i < b->n_in; i++) {
+      int k = b->dev_of[i];
+      errors[i] = k < 0 ? b->host_err[i] : (batch_err ? batch_err : cj_status_error(&st[k]));
+    }
+  return batch_err;
+}
+
+int cjBatchDecode(CJBatch* b, int n, const unsigned char* blob, const int64_t* offsets,
+                  const int64_t* sizes, int* errors) {
+  int e = cjBatchStage(b, n, blob, offsets, sizes);
+  if (!e) e = cjBatchRun(b);
+  if (!e) e = cjBatchFetch(b);
+  int w = cjBatchWait(b, errors);
+  return e ? e : w;
+}
+
+const unsigned char* cjBatchImage(const CJBatch* b, int i, int* w, int* h, int* c) {
+  if (i < 0 || i >= b->n_in || b->dev_of[i] < 0 || !b->h_out.p) return NULL;
+  int k = b->dev_of[i];
+  if (w) *w = b->dims[3 * k];
+  if (h) *h = b->dims[3 * k + 1];
+  if (c) *c = b->dims[3 * k + 2];
+  return (const unsigned char*)b->h_out.p + b->outoff[k];
+}
+
+const unsigned char* cjBatchDeviceImage(const CJBatch* b, int i) {
+  if (i < 0 || i >= b->n_in || b->dev_of[i] < 0) return NULL;
+  return (const unsigned char*)b->out.p + b->outoff[b->dev_of[i]];
+}
+
+void* cjBatchStream(const CJBatch* b) { return (void*)b->stream; }
+
+void cjBatchStats(const CJBatch* b, int64_t* s) {
+  const CJBatchCtl* ctl = (const CJBatchCtl*)b->h_ctl.p;
+  s[0] = b->n_in;
+  s[1] = b->n_dev;
+  s[2] = b->grid;
+  s[3] = b->nwarps;
+  s[4] = b->ntiles;
+  s[5] = b->nptiles;
+  s[6] = ctl ? ctl->passes : 0;
+  s[7] = b->blob_bytes;
+  s[8] = b->out_total;
+  s[9] = (int64_t)b->smem;
+  s[10] = b->launches;
+}
+
+float cjBatchKernelMs(const CJBatch* b) {
+  float ms = 0.f;
+  if (b->ready) cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+  return ms;
+}
+
+}  // extern "C"

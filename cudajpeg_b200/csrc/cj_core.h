@@ -15,6 +15,7 @@
 #define CJ_FAST_BITS 10          // first-level Huffman lookup width
 #define CJ_MAX_BPM 32            // blocks per MCU (the standard allows 10)
 #define CJ_SUB_BITS_DEFAULT 1024 // bits per speculative subsequence
+#define CJ_MAX_SCAN_BYTES (256u << 20) // block / bit counters are 32-bit
 
 // Device error codes (the reader maps them to the format.h codes)
 #define CJ_DEV_OK 0
@@ -93,7 +94,11 @@ struct CJWarpAgg {
 
 // Status words the host reads back after a decode.
 struct CJStatus {
-  unsigned long long err_key; // min over errors of (block << 8 | CJ_DEV_*); ~0 = none
+  unsigned long long err_key;     // destuff / segment errors: complemented
+                                  // min of (block << 8 | CJ_DEV_*), 0 = none
+  unsigned long long dec_err_key; // errors of the coefficient write-out and
+                                  // pixel passes (same encoding); cleared when
+                                  // those passes are re-run
   int32_t unstable;           // warps whose last exit changed in the last fix-up pass
   int32_t nmarkers;           // RSTn markers found by the destuffer
   int32_t nsub;               // subsequences in use
@@ -155,46 +160,108 @@ CJ_HD int32_t cj_extend(uint32_t bits, uint32_t size) {
    41, 34, 27, 20, 13, 6,  7,  14, 21, 28, 35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, \
    30, 37, 44, 51, 58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63}
 
-// Decode one block starting at bit `p` with the given tables.
-//   Sink receives (natural index, value) for every coefficient written,
-//   including the DC difference at index 0 (before prediction).
-//   Returns the bit position after the block; *err = CJ_DEV_* (0 ok).
-//   On an error the block is cut short at the failing symbol, consuming at
-//   least one bit, so a speculative decode keeps moving.
-//   *last_sym receives the start bit of the block's final symbol.
+// MSB-first bit reader over the destuffed buffer with a 64-bit register
+// window and one word of prefetch, so the load feeding the next refill is in
+// flight while the current symbols decode.  Bytes at or past `end_byte` read
+// as 0xFF (the padding the reference's bit reader supplies).
+struct CJBits {
+  const uint32_t* words;
+  uint64_t end_byte;
+  uint64_t buf;   // unread bits, MSB-aligned
+  uint64_t pos;   // absolute bit position of buf's MSB
+  uint64_t w;     // next word to append
+  uint32_t nxt;   // that word, already loaded
+  int n;          // valid bits in buf (32..63 after a refill)
+
+  CJ_HD void init(const uint32_t* wd, uint64_t eb, uint64_t p) {
+    words = wd;
+    end_byte = eb;
+    pos = p;
+    w = p >> 5;
+    uint32_t first = cj_word(words, w, end_byte);
+    uint32_t s = (uint32_t)(p & 31);
+    buf = ((uint64_t)first << 32) << s;
+    n = 32 - (int)s;
+    w++;
+    nxt = cj_word(words, w, end_byte);
+    refill();
+  }
+  CJ_HD void refill() {
+    if (n < 32) {
+      buf |= (uint64_t)nxt << (32 - n);
+      n += 32;
+      w++;
+      nxt = cj_word(words, w, end_byte);
+    }
+  }
+  CJ_HD uint32_t peek32() const { return (uint32_t)(buf >> 32); }
+  CJ_HD void skip(uint32_t k) {
+    buf <<= k;
+    n -= (int)k;
+    pos += k;
+    refill();
+  }
+};
+
+// Decode one block at the reader's position with the given tables.
+//   Sink receives (natural index, value) for every nonzero AC coefficient.
+//   *dc_diff gets the DC difference.  Returns CJ_DEV_* (0 ok).  On an error
+//   the block is cut short at the failing symbol, consuming at least one bit,
+//   so a speculative decode keeps moving.
+template <class Sink>
+CJ_HD int cj_block(CJBits& br, const CJHuff& dc, const CJHuff& ac, const uint8_t* zz,
+                   int32_t* dc_diff, Sink& sink) {
+  uint32_t v = br.peek32();
+  uint32_t e = cj_huff_decode(dc, v >> 16);
+  if (!e) {
+    *dc_diff = 0;
+    br.skip(1);
+    return CJ_DEV_BAD_CODE;
+  }
+  uint32_t len = e >> 8, size = e & 15;
+  *dc_diff = size ? cj_extend((v << len) >> (32 - size), size) : 0;
+  br.skip(len + size);
+  int k = 0;
+  for (;;) {
+    v = br.peek32();
+    e = cj_huff_decode(ac, v >> 16);
+    if (!e) {
+      br.skip(1);
+      return CJ_DEV_BAD_CODE;
+    }
+    len = e >> 8;
+    uint32_t sym = e & 255;
+    size = sym & 15;
+    if (!size) {
+      br.skip(len);
+      if (sym == 0) return 0;             // EOB
+      if (sym != 0xF0) return CJ_DEV_BAD_AC;
+      k += 16;                            // ZRL
+      if (k > 63) return CJ_DEV_BAD_AC;
+      if (k == 63) return 0;
+      continue;
+    }
+    k += (int)(sym >> 4) + 1;
+    if (k > 63) {
+      br.skip(len);
+      return CJ_DEV_BAD_AC;
+    }
+    sink(zz[k], cj_extend((v << len) >> (32 - size), size));
+    br.skip(len + size);
+    if (k == 63) return 0;
+  }
+}
+
+// Reference-style wrapper used by host tools: decode the block at bit `p`.
 template <class Sink>
 CJ_HD uint64_t cj_decode_block(const uint32_t* words, uint64_t end_byte, uint64_t p,
                                const CJHuff& dc, const CJHuff& ac, const uint8_t* zz,
                                int32_t* dc_diff, int* err, Sink& sink, uint64_t* last_sym) {
-  *err = 0;
+  CJBits br;
+  br.init(words, end_byte, p);
+  *err = cj_block(br, dc, ac, zz, dc_diff, sink);
   *last_sym = p;
-  uint32_t v = cj_peek32(words, p, end_byte);
-  uint32_t e = cj_huff_decode(dc, v >> 16);
-  if (!e) { *err = CJ_DEV_BAD_CODE; *dc_diff = 0; return p + 1; }
-  uint32_t len = e >> 8, size = e & 15;
-  int32_t diff = 0;
-  if (size) diff = cj_extend((v << len) >> (32 - size), size);
-  *dc_diff = diff;
-  sink(0, diff);
-  p += len + size;
-  int k = 0;
-  for (;;) {
-    *last_sym = p;
-    v = cj_peek32(words, p, end_byte);
-    e = cj_huff_decode(ac, v >> 16);
-    if (!e) { *err = CJ_DEV_BAD_CODE; return p + 1; }
-    len = e >> 8;
-    uint32_t sym = e & 255;
-    if (sym == 0) { p += len; break; }       // EOB
-    size = sym & 15;
-    if (!size && sym != 0xF0) { *err = CJ_DEV_BAD_AC; return p + len; }
-    k += (int)(sym >> 4) + 1;
-    if (k > 63) { *err = CJ_DEV_BAD_AC; return p + len; }
-    if (size) sink(zz[k], cj_extend((v << len) >> (32 - size), size));
-    p += len + size;
-    if (k >= 63) break;
-  }
-  return p;
+  return br.pos;
 }
 
 struct CJNullSink {

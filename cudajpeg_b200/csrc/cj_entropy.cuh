@@ -1,0 +1,275 @@
+// cj_entropy.cuh -- device building blocks of the entropy decode shared by
+// the per-image kernels (scan.cu) and the persistent batch kernel
+// (batch.cu): destuff classification, subsequence lanes, speculative block
+// decode and the warp settle loop.
+#pragma once
+#include <stdint.h>
+
+#include "cj_core.h"
+#include "cj_scan_util.cuh"
+
+// 16 stuffed bytes starting at `base`, their neighbours, and what to keep.
+struct CJChunk {
+  uint32_t w[4];    // the 16 bytes, little-endian words
+  uint32_t keep;    // bit j: byte j is entropy data
+  uint32_t mark;    // bit j: byte j is the FF of an RSTn marker
+  uint32_t next;    // byte after the chunk (marker code of bit 15)
+  bool bad;         // an FF followed by anything but 00 / D0-D7
+};
+
+__device__ __forceinline__ uint32_t cj_byte(const CJChunk& c, int j) {
+  return (c.w[j >> 2] >> (8 * (j & 3))) & 0xFF;
+}
+
+__device__ __forceinline__ CJChunk cj_classify(const uint8_t* raw, int64_t n, int64_t base) {
+  CJChunk c;
+  c.keep = c.mark = 0;
+  c.bad = false;
+  if (base + 16 <= n && (((uintptr_t)(raw + base)) & 15) == 0) {
+    uint4 v = *reinterpret_cast<const uint4*>(raw + base);
+    c.w[0] = v.x; c.w[1] = v.y; c.w[2] = v.z; c.w[3] = v.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t x = 0;
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        int64_t q = base + 4 * k + b;
+        if (q < n) x |= (uint32_t)raw[q] << (8 * b);
+      }
+      c.w[k] = x;
+    }
+  }
+  c.next = (base + 16 < n) ? raw[base + 16] : 0;
+  uint32_t prev = (base > 0 && base - 1 < n) ? raw[base - 1] : 0;
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    if (base + j >= n) break;
+    uint32_t b = cj_byte(c, j);
+    uint32_t nx = (j < 15) ? cj_byte(c, j + 1) : c.next;
+    bool has_next = base + j + 1 < n;
+    if (prev == 0xFF && (base + j) > 0) {
+      // second byte of an FF pair: stuffing or the RSTn code, never data
+      if (b != 0x00 && (b & 0xF8) != 0xD0) c.bad = true;
+    } else if (b == 0xFF) {
+      if (has_next && nx == 0x00) c.keep |= 1u << j;
+      else if (has_next && (nx & 0xF8) == 0xD0) c.mark |= 1u << j;
+      else c.bad = true;
+    } else {
+      c.keep |= 1u << j;
+    }
+    prev = b;
+  }
+  return c;
+}
+
+struct CJLane {
+  uint64_t begin, end;   // this subsequence's bits
+  uint64_t end_byte;     // its segment's end (bytes)
+  int seg;
+  bool head, last, active;
+};
+
+__device__ __forceinline__ CJLane cj_lane(const CJSegment* segs, int nseg, int nsub, int i,
+                                          int sub_bits) {
+  CJLane l;
+  l.active = i < nsub;
+  l.begin = l.end = l.end_byte = 0;
+  l.seg = 0;
+  l.head = l.last = false;
+  if (!l.active) return l;
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (segs[mid].first_sub <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  const CJSegment& s = segs[lo];
+  int j = i - s.first_sub;
+  l.seg = lo;
+  l.begin = s.bit_begin + (uint64_t)j * sub_bits;
+  l.end = min(s.bit_end, l.begin + (uint64_t)sub_bits);
+  if (l.begin > s.bit_end) l.begin = s.bit_end;
+  l.end_byte = s.bit_end >> 3;
+  l.head = (j == 0);
+  l.last = (j == s.nsub - 1);
+  return l;
+}
+
+// Speculative decode of one subsequence from `start`: blocks beginning
+// before the subsequence's end, their DC sums, and the state after them.
+__device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const uint32_t* words,
+                                                   const CJLane& ln, uint64_t start) {
+  CJBits br;
+  br.init(words, ln.end_byte, cj_state_bit(start));
+  uint32_t m = cj_state_phase(start);
+  int nb = 0, d0 = 0, d1 = 0, d2 = 0;
+  CJNullSink ns;
+  while (br.pos < ln.end) {
+    int c = sp.phase_comp[m];
+    int32_t dd;
+    cj_block(br, sp.huff[sp.comp_dc[c]], sp.huff[sp.comp_ac[c]], sp.zz, &dd, ns);
+    d0 += (c == 0) ? dd : 0;
+    d1 += (c == 1) ? dd : 0;
+    d2 += (c == 2) ? dd : 0;
+    nb++;
+    m = (m + 1 == (uint32_t)sp.bpm) ? 0 : m + 1;
+  }
+  CJSubRec r;
+  r.start = start;
+  r.exit = cj_state(br.pos, m);
+  r.nblocks = nb;
+  r.dc[0] = d0;
+  r.dc[1] = d1;
+  r.dc[2] = d2;
+  return r;
+}
+
+// Re-decode lanes whose input state (lane 0: `lane0_in`; others: the exit of
+// the previous lane) differs from the state they last decoded from, until no
+// lane changes.  Lane l settles after at most l+1 re-decodes.
+__device__ __forceinline__ bool cj_warp_settle(const CJScanParams& sp, const uint32_t* words,
+                                               const CJLane& ln, CJSubRec& r, uint64_t lane0_in) {
+  int lane = threadIdx.x & 31;
+  bool dirty = false;
+  for (int it = 0; it < 34; it++) {
+    uint64_t pred = __shfl_up_sync(CJ_FULL, r.exit, 1);
+    uint64_t want = ln.head ? r.start : (lane == 0 ? lane0_in : pred);
+    bool change = ln.active && want != r.start;
+    if (!__any_sync(CJ_FULL, change)) break;
+    if (change) {
+      r = cj_spec_decode(sp, words, ln, want);
+      dirty = true;
+    }
+  }
+  return dirty;
+}
+
+// Errors are ordered by the block they occur in; the status keeps the first
+// (stored complemented so an all-zero status means "no error").
+__device__ __forceinline__ void cj_raise(CJStatus* st, int64_t block, int code) {
+  unsigned long long key = ((unsigned long long)block << 8) | (unsigned)code;
+  atomicMax(&st->err_key, ~key);
+}
+
+__device__ __forceinline__ void cj_raise_dec(CJStatus* st, int64_t block, int code) {
+  unsigned long long key = ((unsigned long long)block << 8) | (unsigned)code;
+  atomicMax(&st->dec_err_key, ~key);
+}
+
+// Segmented-sum operator over (head flag, sums).
+struct CJAgg5 {
+  int f, n, a, b, c;
+};
+__device__ __forceinline__ CJAgg5 cj_op(const CJAgg5& x, const CJAgg5& y) {
+  CJAgg5 r;
+  r.f = x.f | y.f;
+  if (y.f) {
+    r.n = y.n; r.a = y.a; r.b = y.b; r.c = y.c;
+  } else {
+    r.n = x.n + y.n; r.a = x.a + y.a; r.b = x.b + y.b; r.c = x.c + y.c;
+  }
+  return r;
+}
+
+struct CJCoefSink {
+  int16_t* blk;
+  __device__ __forceinline__ void operator()(int idx, int32_t v) const {
+    if (idx) blk[idx] = (int16_t)v;
+  }
+};
+
+// Segmented exclusive prefix, over the lanes of a warp, of each lane's blocks
+// and DC sums: from the last segment head at or before the lane, plus the
+// carry from earlier warps (cn, c0..c2) when the segment began before this warp.
+__device__ __forceinline__ void cj_warp_prefix(const CJSubRec& r, const CJLane& ln, int cn, int c0,
+                                               int c1, int c2, int64_t* blocks, int* d0, int* d1,
+                                               int* d2) {
+  const int lane = threadIdx.x & 31;
+  // Segmented exclusive prefix of (blocks, DC sums) over the warp.
+  int s0 = r.nblocks, s1 = r.dc[0], s2 = r.dc[1], s3 = r.dc[2];
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    int t0 = __shfl_up_sync(CJ_FULL, s0, d), t1 = __shfl_up_sync(CJ_FULL, s1, d);
+    int t2 = __shfl_up_sync(CJ_FULL, s2, d), t3 = __shfl_up_sync(CJ_FULL, s3, d);
+    if (lane >= d) {
+      s0 += t0; s1 += t1; s2 += t2; s3 += t3;
+    }
+  }
+  unsigned heads = __ballot_sync(CJ_FULL, ln.active && ln.head);
+  unsigned mine = heads & ((2u << lane) - 1u);  // heads at or before this lane
+  int a = mine ? 31 - __clz(mine) : 0;
+  int src = a > 0 ? a - 1 : 0;
+  int b0 = __shfl_sync(CJ_FULL, s0, src), b1 = __shfl_sync(CJ_FULL, s1, src);
+  int b2 = __shfl_sync(CJ_FULL, s2, src), b3 = __shfl_sync(CJ_FULL, s3, src);
+  if (a == 0) b0 = b1 = b2 = b3 = 0;
+  int e0 = s0 - r.nblocks - b0, e1 = s1 - r.dc[0] - b1, e2 = s2 - r.dc[1] - b2,
+      e3 = s3 - r.dc[2] - b3;
+  if (!mine) {
+    e0 += cn; e1 += c0; e2 += c1; e3 += c2;
+  }
+  *blocks = e0;
+  *d0 = e1;
+  *d1 = e2;
+  *d2 = e3;
+}
+
+// Final decode of one lane from its settled start: writes quantised int16
+// coefficients (natural order) of its blocks, DC predicted per component,
+// and records structural errors of its restart interval.
+__device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint32_t* words,
+                                              const CJLane& ln, const CJSegment& seg,
+                                              const CJSubRec& r, int64_t first_block, int dc0,
+                                              int dc1, int dc2, int16_t* __restrict__ coef,
+                                              CJStatus* st) {
+  int64_t b = first_block;
+  const int64_t bend = seg.first_block + seg.nblocks;
+  CJBits br;
+  br.init(words, ln.end_byte, cj_state_bit(r.start));
+  uint32_t m = cj_state_phase(r.start);
+  const uint64_t seg_end = seg.bit_end;
+  for (;;) {
+    const uint64_t p = br.pos;
+    if (!ln.last && p >= ln.end) break;
+    if (b >= bend) {
+      if (!ln.last) cj_raise_dec(st, b, CJ_DEV_EXTRA);
+      else if (seg.marker_follows) {
+        if (((p + 7) >> 3) != ln.end_byte) cj_raise_dec(st, b, CJ_DEV_TRAILING);
+      } else if (ln.end_byte > ((p + 7) >> 3) + 2) {
+        cj_raise_dec(st, b, CJ_DEV_TRAILING);
+      }
+      break;
+    }
+    if (seg.marker_follows && p >= seg_end) {
+      cj_raise_dec(st, b, CJ_DEV_OVERRUN);
+      break;
+    }
+    int c = sp.phase_comp[m];
+    int16_t* blk = coef + b * 64;
+    uint4 z = make_uint4(0, 0, 0, 0);
+#pragma unroll
+    for (int k = 0; k < 8; k++) reinterpret_cast<uint4*>(blk)[k] = z;
+    CJCoefSink sink{blk};
+    int32_t dd;
+    int err = cj_block(br, sp.huff[sp.comp_dc[c]], sp.huff[sp.comp_ac[c]], sp.zz, &dd, sink);
+    if (err) {
+      cj_raise_dec(st, b, err);
+      break;
+    }
+    if (seg.marker_follows && br.pos > seg_end) {
+      cj_raise_dec(st, b, CJ_DEV_OVERRUN);
+      break;
+    }
+    int v;
+    if (c == 0) v = dc0 += dd;
+    else if (c == 1) v = dc1 += dd;
+    else v = dc2 += dd;
+    if (v < -32768 || v > 32767) {
+      cj_raise_dec(st, b, CJ_DEV_DC_RANGE);
+      break;
+    }
+    blk[0] = (int16_t)v;
+    b++;
+    m = (m + 1 == (uint32_t)sp.bpm) ? 0 : m + 1;
+  }
+}

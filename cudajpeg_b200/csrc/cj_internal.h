@@ -88,6 +88,10 @@ int cj_pixel_launch(JPGReader* jpg, bool copy_out);
 // Export int32 dequantised coefficients to channels[c].working_space.
 int cj_export_coefficients(JPGReader* jpg);
 
+// Host parse helpers (format.cu / scan.cu)
+int cj_parse_sos(JPGReader* jpg);
+extern "C" int cj_parse_to_scan(JPGReader* r, const unsigned char* buf, size_t size);
+
 // Map a device status word to a format.h error code (0 = fine).
 int cj_status_error(const CJStatus* st);
 

@@ -213,7 +213,10 @@ void decodeDQT(JPGReader* jpg) {
 }
 
 // The marker loop of src/format.cu:159-215 over a file image in memory.
-static int cj_parse_and_decode(JPGReader* r, unsigned char* buf, size_t size) {
+// With stop_at_scan the loop returns 0 after the SOS header has been checked
+// (jpg->pos = first entropy-coded byte, jpg->end = last byte before EOI)
+// without launching any device work: the batch decoder's host parse.
+static int cj_marker_loop(JPGReader* r, unsigned char* buf, size_t size, bool stop_at_scan) {
   r->error = NO_ERROR;
   r->error_line = 0;
   r->error_file = r->error_func = NULL;
@@ -240,7 +243,14 @@ static int cj_parse_and_decode(JPGReader* r, unsigned char* buf, size_t size) {
       case 0xC4: decodeDHT(r); break;
       case 0xDB: decodeDQT(r); break;
       case 0xDD: decodeDRI(r); break;
-      case 0xDA: decodeScanGPU(r); break;
+      case 0xDA:
+        if (stop_at_scan) {
+          int e = cj_parse_sos(r);
+          if (!e) r->scan_seen = 1;
+          return r->error = e;
+        }
+        decodeScanGPU(r);
+        break;
       case 0xFE: skipBlock(r); break;
       case 0xD9: break;
       default:
@@ -261,6 +271,16 @@ static int cj_parse_and_decode(JPGReader* r, unsigned char* buf, size_t size) {
     }
   }
   return r->error;
+}
+
+static int cj_parse_and_decode(JPGReader* r, unsigned char* buf, size_t size) {
+  return cj_marker_loop(r, buf, size, false);
+}
+
+int cj_parse_to_scan(JPGReader* r, const unsigned char* buf, size_t size) {
+  int e = cj_marker_loop(r, (unsigned char*)buf, size, true);
+  if (!e && !r->scan_seen) e = r->error = SYNTAX_ERROR;  // EOI before any scan
+  return e;
 }
 
 int openJPGMem(JPGReader* r, const unsigned char* data, size_t size) {

@@ -19,63 +19,8 @@
 #include "../../include/pixelTransformGPU.h"
 #include "cj_internal.h"
 #include "cj_idct.cuh"
+#include "cj_pixel.cuh"
 
-#define CJ_PIX_THREADS 256
-
-// ---------------------------------------------------------------- TMA helpers
-__device__ __forceinline__ uint32_t cj_smem_addr(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void cj_mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(cj_smem_addr(bar)), "r"(count)
-               : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void cj_bulk_load(void* dst, const void* src, uint32_t bytes,
-                                             uint64_t* bar) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(cj_smem_addr(bar)),
-               "r"(bytes)
-               : "memory");
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          cj_smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(cj_smem_addr(bar))
-      : "memory");
-}
-
-// Wait for phase `parity` of the barrier; gives up after a bounded number of
-// polls and returns false.
-__device__ __forceinline__ bool cj_mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t it = 0; it < (1u << 22); it++) {
-    uint32_t ok;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(ok)
-        : "r"(cj_smem_addr(bar)), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if (it > 64) __nanosleep(32);
-  }
-  return false;
-}
-
-// ---------------------------------------------------------------- fused kernel
-
-struct CJPixGeom {
-  int nch, bpm, mcux, mcuy, width, height;
-  int hmax, vmax, xs, ys;
-  int T;                 // MCUs per CTA (one MCU row)
-  int y_stride, c_stride; // tile plane strides (bytes)
-  int tmp_off, y_off, cb_off, cr_off;
-};
-
-struct CJPixSmemParams {
-  int16_t q[4][64];
-  uint8_t pc[CJ_MAX_BPM], pb[CJ_MAX_BPM];
-  uint8_t cq[4], csx[4], csy[4];
-};
 
 __global__ void __launch_bounds__(CJ_PIX_THREADS)
 k_pixel(const CJScanParams* __restrict__ prm, const int16_t* __restrict__ coef,
@@ -83,94 +28,9 @@ k_pixel(const CJScanParams* __restrict__ prm, const int16_t* __restrict__ coef,
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ uint64_t bar;
   __shared__ CJPixSmemParams P;
-  const int mrow = blockIdx.y;
-  const int mc0 = blockIdx.x * g.T;
-  const int nm = min(g.T, g.mcux - mc0);
-  const int nblk = nm * g.bpm;
-  int16_t* sc = reinterpret_cast<int16_t*>(smem);
-  int* tmp = reinterpret_cast<int*>(smem + g.tmp_off);
-  uint8_t* py = smem + g.y_off;
-  uint8_t* pcb = smem + g.cb_off;
-  uint8_t* pcr = smem + g.cr_off;
-
   if (threadIdx.x == 0) cj_mbar_init(&bar, 1);
   __syncthreads();
-  if (threadIdx.x == 0) {
-    const int16_t* src = coef + ((int64_t)mrow * g.mcux + mc0) * g.bpm * 64;
-    cj_bulk_load(sc, src, (uint32_t)nblk * 128u, &bar);
-  }
-  for (int k = threadIdx.x; k < 4 * 64; k += blockDim.x) P.q[k >> 6][k & 63] = prm->qnat[k >> 6][k & 63];
-  if (threadIdx.x < CJ_MAX_BPM) {
-    P.pc[threadIdx.x] = prm->phase_comp[threadIdx.x];
-    P.pb[threadIdx.x] = prm->phase_blk[threadIdx.x];
-  }
-  if (threadIdx.x < 3) {
-    P.cq[threadIdx.x] = prm->comp_q[threadIdx.x];
-    P.csx[threadIdx.x] = prm->comp_sx[threadIdx.x];
-    P.csy[threadIdx.x] = prm->comp_sy[threadIdx.x];
-  }
-  bool ok = cj_mbar_wait(&bar, 0);
-  if (!__syncthreads_and(ok)) {
-    if (threadIdx.x == 0) atomicMax(&st->err_key, ~((unsigned long long)CJ_DEV_CAPACITY));
-    return;
-  }
-
-  // Row pass: one thread per (block, row); dequantise on load.
-  for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
-    int k = t >> 3, r = t & 7;
-    int c = P.pc[k % g.bpm];
-    const int16_t* q = &P.q[P.cq[c]][r * 8];
-    uint4 raw = *reinterpret_cast<const uint4*>(sc + k * 64 + r * 8);
-    int v[8];
-    cj_unpack_dequant(raw, q, v);
-    cj_idct_row(v);
-    int4* o = reinterpret_cast<int4*>(tmp + k * 64 + r * 8);
-    o[0] = make_int4(v[0], v[1], v[2], v[3]);
-    o[1] = make_int4(v[4], v[5], v[6], v[7]);
-  }
-  __syncthreads();
-
-  // Column pass: one thread per (block, column); 8 samples into the plane tile.
-  for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
-    int k = t >> 3, col = t & 7;
-    int d[8];
-#pragma unroll
-    for (int j = 0; j < 8; j++) d[j] = tmp[k * 64 + j * 8 + col];
-    uint32_t o[8];
-    cj_idct_col(d, o);
-    int mi = k / g.bpm, ph = k - mi * g.bpm;
-    int c = P.pc[ph], bl = P.pb[ph], sxc = P.csx[c];
-    int bx = mi * sxc + bl % sxc, by = bl / sxc;
-    uint8_t* plane = c == 0 ? py : (c == 1 ? pcb : pcr);
-    int ps = c == 0 ? g.y_stride : g.c_stride;
-    uint8_t* dst = plane + (by * 8) * ps + bx * 8 + col;
-#pragma unroll
-    for (int j = 0; j < 8; j++) dst[j * ps] = (uint8_t)o[j];
-  }
-  __syncthreads();
-
-  // Upsample + colour (or copy for grey) into the output image.
-  const int X0 = mc0 * 8 * g.hmax, Y0 = mrow * 8 * g.vmax;
-  const int w = min(nm * 8 * g.hmax, g.width - X0);
-  const int h = min(8 * g.vmax, g.height - Y0);
-  if (w <= 0 || h <= 0) return;
-  if (g.nch == 3) {
-    for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
-      int y = t / w, x = t - y * w;
-      int yy = py[y * g.y_stride + x] << 8;
-      int ci = (y >> g.ys) * g.c_stride + (x >> g.xs);
-      int cb = (int)pcb[ci] - 128, cr = (int)pcr[ci] - 128;
-      uint8_t* o = out + ((int64_t)(Y0 + y) * g.width + X0 + x) * 3;
-      o[0] = (uint8_t)cj_clip8((yy + 359 * cr + 128) >> 8);
-      o[1] = (uint8_t)cj_clip8((yy - 88 * cb - 183 * cr + 128) >> 8);
-      o[2] = (uint8_t)cj_clip8((yy + 454 * cb + 128) >> 8);
-    }
-  } else {
-    for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
-      int y = t / w, x = t - y * w;
-      out[(int64_t)(Y0 + y) * g.width + X0 + x] = py[y * g.y_stride + x];
-    }
-  }
+  cj_pixel_tile(*prm, coef, out, st, g, blockIdx.y, blockIdx.x * g.T, smem, &bar, 0, &P);
 }
 
 // Dequantised int32 coefficients in the reference's per-channel layout
@@ -195,6 +55,8 @@ __global__ void k_export_coef(const CJScanParams* __restrict__ prm, const int16_
 
 static int cj_pixel_geom(JPGReader* jpg, CJPixGeom* g, size_t* smem) {
   const CJScanParams* hp = (const CJScanParams*)jpg->dev->h_params.p;
+  int err = cj_pix_check(hp);
+  if (err) return err;
   g->nch = hp->nch;
   g->bpm = hp->bpm;
   g->mcux = hp->mcux;
@@ -205,32 +67,8 @@ static int cj_pixel_geom(JPGReader* jpg, CJPixGeom* g, size_t* smem) {
   g->vmax = hp->vmax;
   g->xs = hp->xshift;
   g->ys = hp->yshift;
-  // the tile layout needs full-resolution luma and chroma at an exact power-
-  // of-two fraction of it (always true for the SOF0 geometries the parser
-  // accepts, except 1-pixel-wide or -high oddities)
-  if (hp->comp_sx[0] != hp->hmax || hp->comp_sy[0] != hp->vmax) return UNSUPPORTED_ERROR;
-  if (hp->nch == 3 && ((hp->comp_sx[1] << hp->xshift) != hp->hmax ||
-                       (hp->comp_sy[1] << hp->yshift) != hp->vmax))
-    return UNSUPPORTED_ERROR;
-  int T = 16 / g->hmax;
-  if (T < 1) T = 1;
-  while (T > 1 && T * g->bpm > 64) T >>= 1;
-  g->T = T;
-  g->y_stride = T * 8 * g->hmax;
-  g->c_stride = g->nch == 3 ? T * 8 * hp->comp_sx[1] : 0;
-  size_t coef_bytes = (size_t)T * g->bpm * 128;
-  size_t off = coef_bytes;
-  g->tmp_off = (int)off;
-  off += (size_t)T * g->bpm * 256;
-  g->y_off = (int)off;
-  off += (size_t)g->y_stride * 8 * g->vmax;
-  off = (off + 15) & ~(size_t)15;
-  g->cb_off = (int)off;
-  size_t csz = g->nch == 3 ? (size_t)g->c_stride * 8 * hp->comp_sy[1] : 0;
-  off += csz;
-  g->cr_off = (int)off;
-  off += csz;
-  *smem = (off + 15) & ~(size_t)15;
+  g->T = cj_pix_tile_mcus(hp->hmax, hp->bpm);
+  *smem = cj_pix_layout(g, hp->comp_sx[1], hp->comp_sy[1]);
   return 0;
 }
 

@@ -26,6 +26,7 @@
 
 #include "../../include/decodeScanGPU.h"
 #include "cj_internal.h"
+#include "cj_entropy.cuh"
 #include "cj_scan_util.cuh"
 #include "cj_tables.h"
 
@@ -131,8 +132,9 @@ void cj_after_launch(CJReaderDevice* d, int kernel_id) {
 }
 
 int cj_status_error(const CJStatus* st) {
-  if (!st->err_key) return 0;
-  unsigned long long key = ~st->err_key;
+  unsigned long long k = st->err_key > st->dec_err_key ? st->err_key : st->dec_err_key;
+  if (!k) return 0;
+  unsigned long long key = ~k;
   int code = (int)(key & 0xFF);
   if (code == CJ_DEV_DC_RANGE) return UNSUPPORTED_ERROR;
   if (code == CJ_DEV_CAPACITY) return PROGRAMMER_ERROR;
@@ -140,68 +142,6 @@ int cj_status_error(const CJStatus* st) {
 }
 
 // ---------------------------------------------------------------- device helpers
-
-// Errors are ordered by the block they occur in; the status keeps the first
-// (stored complemented so an all-zero status means "no error").
-__device__ __forceinline__ void cj_raise(CJStatus* st, int64_t block, int code) {
-  unsigned long long key = ((unsigned long long)block << 8) | (unsigned)code;
-  atomicMax(&st->err_key, ~key);
-}
-
-// 16 stuffed bytes starting at `base`, their neighbours, and what to keep.
-struct CJChunk {
-  uint32_t w[4];    // the 16 bytes, little-endian words
-  uint32_t keep;    // bit j: byte j is entropy data
-  uint32_t mark;    // bit j: byte j is the FF of an RSTn marker
-  uint32_t next;    // byte after the chunk (marker code of bit 15)
-  bool bad;         // an FF followed by anything but 00 / D0-D7
-};
-
-__device__ __forceinline__ uint32_t cj_byte(const CJChunk& c, int j) {
-  return (c.w[j >> 2] >> (8 * (j & 3))) & 0xFF;
-}
-
-__device__ __forceinline__ CJChunk cj_classify(const uint8_t* raw, int64_t n, int64_t base) {
-  CJChunk c;
-  c.keep = c.mark = 0;
-  c.bad = false;
-  if (base + 16 <= n) {
-    uint4 v = *reinterpret_cast<const uint4*>(raw + base);
-    c.w[0] = v.x; c.w[1] = v.y; c.w[2] = v.z; c.w[3] = v.w;
-  } else {
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      uint32_t x = 0;
-#pragma unroll
-      for (int b = 0; b < 4; b++) {
-        int64_t q = base + 4 * k + b;
-        if (q < n) x |= (uint32_t)raw[q] << (8 * b);
-      }
-      c.w[k] = x;
-    }
-  }
-  c.next = (base + 16 < n) ? raw[base + 16] : 0;
-  uint32_t prev = (base > 0 && base - 1 < n) ? raw[base - 1] : 0;
-#pragma unroll
-  for (int j = 0; j < 16; j++) {
-    if (base + j >= n) break;
-    uint32_t b = cj_byte(c, j);
-    uint32_t nx = (j < 15) ? cj_byte(c, j + 1) : c.next;
-    bool has_next = base + j + 1 < n;
-    if (prev == 0xFF && (base + j) > 0) {
-      // second byte of an FF pair: stuffing or the RSTn code, never data
-      if (b != 0x00 && (b & 0xF8) != 0xD0) c.bad = true;
-    } else if (b == 0xFF) {
-      if (has_next && nx == 0x00) c.keep |= 1u << j;
-      else if (has_next && (nx & 0xF8) == 0xD0) c.mark |= 1u << j;
-      else c.bad = true;
-    } else {
-      c.keep |= 1u << j;
-    }
-    prev = b;
-  }
-  return c;
-}
 
 // Stage 1a: kept bytes and markers per 4 KiB tile.
 __global__ void __launch_bounds__(CJ_TILE_THREADS)
@@ -343,90 +283,6 @@ __device__ __forceinline__ void cj_load_params(CJScanParams& sp, const CJScanPar
   __syncthreads();
 }
 
-struct CJLane {
-  uint64_t begin, end;   // this subsequence's bits
-  uint64_t end_byte;     // its segment's end (bytes)
-  int seg;
-  bool head, last, active;
-};
-
-__device__ __forceinline__ CJLane cj_lane(const CJSegment* segs, int nseg, int nsub, int i,
-                                          int sub_bits) {
-  CJLane l;
-  l.active = i < nsub;
-  l.begin = l.end = l.end_byte = 0;
-  l.seg = 0;
-  l.head = l.last = false;
-  if (!l.active) return l;
-  int lo = 0, hi = nseg - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (segs[mid].first_sub <= i) lo = mid;
-    else hi = mid - 1;
-  }
-  const CJSegment& s = segs[lo];
-  int j = i - s.first_sub;
-  l.seg = lo;
-  l.begin = s.bit_begin + (uint64_t)j * sub_bits;
-  l.end = min(s.bit_end, l.begin + (uint64_t)sub_bits);
-  if (l.begin > s.bit_end) l.begin = s.bit_end;
-  l.end_byte = s.bit_end >> 3;
-  l.head = (j == 0);
-  l.last = (j == s.nsub - 1);
-  return l;
-}
-
-// Speculative decode of one subsequence from `start`: blocks beginning
-// before the subsequence's end, their DC sums, and the state after them.
-__device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const uint32_t* words,
-                                                   const CJLane& ln, uint64_t start) {
-  uint64_t p = cj_state_bit(start);
-  uint32_t m = cj_state_phase(start);
-  int nb = 0, d0 = 0, d1 = 0, d2 = 0;
-  CJNullSink ns;
-  while (p < ln.end) {
-    int c = sp.phase_comp[m];
-    int err;
-    int32_t dd;
-    uint64_t ls;
-    p = cj_decode_block(words, ln.end_byte, p, sp.huff[sp.comp_dc[c]], sp.huff[sp.comp_ac[c]],
-                        sp.zz, &dd, &err, ns, &ls);
-    d0 += (c == 0) ? dd : 0;
-    d1 += (c == 1) ? dd : 0;
-    d2 += (c == 2) ? dd : 0;
-    nb++;
-    m = (m + 1 == (uint32_t)sp.bpm) ? 0 : m + 1;
-  }
-  CJSubRec r;
-  r.start = start;
-  r.exit = cj_state(p, m);
-  r.nblocks = nb;
-  r.dc[0] = d0;
-  r.dc[1] = d1;
-  r.dc[2] = d2;
-  return r;
-}
-
-// Re-decode lanes whose input state (lane 0: `lane0_in`; others: the exit of
-// the previous lane) differs from the state they last decoded from, until no
-// lane changes.  Lane l settles after at most l+1 re-decodes.
-__device__ __forceinline__ bool cj_warp_settle(const CJScanParams& sp, const uint32_t* words,
-                                               const CJLane& ln, CJSubRec& r, uint64_t lane0_in) {
-  int lane = threadIdx.x & 31;
-  bool dirty = false;
-  for (int it = 0; it < 34; it++) {
-    uint64_t pred = __shfl_up_sync(CJ_FULL, r.exit, 1);
-    uint64_t want = ln.head ? r.start : (lane == 0 ? lane0_in : pred);
-    bool change = ln.active && want != r.start;
-    if (!__any_sync(CJ_FULL, change)) break;
-    if (change) {
-      r = cj_spec_decode(sp, words, ln, want);
-      dirty = true;
-    }
-  }
-  return dirty;
-}
-
 // Stage 3a: speculative decode + settle inside each warp.
 __global__ void __launch_bounds__(CJ_SYNC_THREADS)
 k_sync_intra(const CJScanParams* __restrict__ prm, const CJSegment* __restrict__ segs,
@@ -505,21 +361,6 @@ k_sync_inter(const CJScanParams* __restrict__ prm, const CJSegment* __restrict__
   }
 }
 
-// Segmented-sum operator over (head flag, sums).
-struct CJAgg5 {
-  int f, n, a, b, c;
-};
-__device__ __forceinline__ CJAgg5 cj_op(const CJAgg5& x, const CJAgg5& y) {
-  CJAgg5 r;
-  r.f = x.f | y.f;
-  if (y.f) {
-    r.n = y.n; r.a = y.a; r.b = y.b; r.c = y.c;
-  } else {
-    r.n = x.n + y.n; r.a = x.a + y.a; r.b = x.b + y.b; r.c = x.c + y.c;
-  }
-  return r;
-}
-
 // Stage 4a: exclusive segmented scan of the warp aggregates (one CTA).
 __global__ void __launch_bounds__(1024)
 k_scan_warps(const CJWarpAgg* __restrict__ wagg, CJWarpAgg* carry, const CJStatus* st) {
@@ -558,13 +399,6 @@ k_scan_warps(const CJWarpAgg* __restrict__ wagg, CJWarpAgg* carry, const CJStatu
   }
 }
 
-struct CJCoefSink {
-  int16_t* blk;
-  __device__ __forceinline__ void operator()(int idx, int32_t v) const {
-    if (idx) blk[idx] = (int16_t)v;
-  }
-};
-
 // Stage 5: final decode from the settled start states, writing coefficients.
 __global__ void __launch_bounds__(CJ_SYNC_THREADS)
 k_decode_write(const CJScanParams* __restrict__ prm, const CJSegment* __restrict__ segs,
@@ -585,82 +419,13 @@ k_decode_write(const CJScanParams* __restrict__ prm, const CJSegment* __restrict
     r.start = r.exit = 0;
     r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
   }
-  // Segmented exclusive prefix of (blocks, DC sums) over the warp.
-  int s0 = r.nblocks, s1 = r.dc[0], s2 = r.dc[1], s3 = r.dc[2];
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    int t0 = __shfl_up_sync(CJ_FULL, s0, d), t1 = __shfl_up_sync(CJ_FULL, s1, d);
-    int t2 = __shfl_up_sync(CJ_FULL, s2, d), t3 = __shfl_up_sync(CJ_FULL, s3, d);
-    if (lane >= d) {
-      s0 += t0; s1 += t1; s2 += t2; s3 += t3;
-    }
-  }
-  unsigned heads = __ballot_sync(CJ_FULL, ln.active && ln.head);
-  unsigned mine = heads & ((2u << lane) - 1u);  // heads at or before this lane
-  int a = mine ? 31 - __clz(mine) : 0;
-  int src = a > 0 ? a - 1 : 0;
-  int b0 = __shfl_sync(CJ_FULL, s0, src), b1 = __shfl_sync(CJ_FULL, s1, src);
-  int b2 = __shfl_sync(CJ_FULL, s2, src), b3 = __shfl_sync(CJ_FULL, s3, src);
-  if (a == 0) b0 = b1 = b2 = b3 = 0;
-  int e0 = s0 - r.nblocks - b0, e1 = s1 - r.dc[0] - b1, e2 = s2 - r.dc[1] - b2,
-      e3 = s3 - r.dc[2] - b3;
-  if (!mine) {
-    CJWarpAgg cw = carry[warp];
-    e0 += cw.nblocks; e1 += cw.dc[0]; e2 += cw.dc[1]; e3 += cw.dc[2];
-  }
+  int64_t e0;
+  int e1, e2, e3;
+  const CJWarpAgg cw = carry[warp];
+  cj_warp_prefix(r, ln, cw.nblocks, cw.dc[0], cw.dc[1], cw.dc[2], &e0, &e1, &e2, &e3);
   if (!ln.active) return;
   const CJSegment seg = segs[ln.seg];
-  int64_t b = seg.first_block + e0;
-  const int64_t bend = seg.first_block + seg.nblocks;
-  int dc[3] = {e1, e2, e3};
-  uint64_t p = cj_state_bit(r.start);
-  uint32_t m = cj_state_phase(r.start);
-  const uint64_t seg_end = seg.bit_end;
-  for (;;) {
-    if (!ln.last && p >= ln.end) break;
-    if (b >= bend) {
-      if (!ln.last) cj_raise(st, b, CJ_DEV_EXTRA);
-      else if (seg.marker_follows) {
-        if (((p + 7) >> 3) != ln.end_byte) cj_raise(st, b, CJ_DEV_TRAILING);
-      } else if (ln.end_byte > ((p + 7) >> 3) + 2) {
-        cj_raise(st, b, CJ_DEV_TRAILING);
-      }
-      break;
-    }
-    if (seg.marker_follows && p >= seg_end) {
-      cj_raise(st, b, CJ_DEV_OVERRUN);
-      break;
-    }
-    int c = sp.phase_comp[m];
-    int16_t* blk = coef + b * 64;
-    uint4 z = make_uint4(0, 0, 0, 0);
-#pragma unroll
-    for (int k = 0; k < 8; k++) reinterpret_cast<uint4*>(blk)[k] = z;
-    CJCoefSink sink{blk};
-    int err;
-    int32_t dd;
-    uint64_t ls;
-    uint64_t q = cj_decode_block(words, ln.end_byte, p, sp.huff[sp.comp_dc[c]],
-                                 sp.huff[sp.comp_ac[c]], sp.zz, &dd, &err, sink, &ls);
-    if (err) {
-      cj_raise(st, b, err);
-      break;
-    }
-    if (seg.marker_follows && q > seg_end) {
-      cj_raise(st, b, CJ_DEV_OVERRUN);
-      break;
-    }
-    int v = dc[c] + dd;
-    dc[c] = v;
-    if (v < -32768 || v > 32767) {
-      cj_raise(st, b, CJ_DEV_DC_RANGE);
-      break;
-    }
-    blk[0] = (int16_t)v;
-    p = q;
-    b++;
-    m = (m + 1 == (uint32_t)sp.bpm) ? 0 : m + 1;
-  }
+  cj_write_lane(sp, words, ln, seg, r, seg.first_block + e0, e1, e2, e3, coef, st);
 }
 
 // ---------------------------------------------------------------- host side
@@ -791,6 +556,7 @@ int cj_scan_write(JPGReader* jpg) {
   cudaStream_t s = d->stream;
   CJStatus* st = (CJStatus*)d->status.p;
   const int sync_blocks = (d->nwarp_cap + (CJ_SYNC_THREADS / 32) - 1) / (CJ_SYNC_THREADS / 32);
+  CJ_CUDA_TRY(cudaMemsetAsync(&st->dec_err_key, 0, sizeof(unsigned long long), s), CUDA_MEM_ERROR);
   k_scan_warps<<<1, 1024, 0, s>>>((const CJWarpAgg*)d->wagg.p, (CJWarpAgg*)d->carry.p, st);
   cj_after_launch(d, CJ_K_SCAN_WARPS);
   k_decode_write<<<sync_blocks, CJ_SYNC_THREADS, 0, s>>>(
@@ -828,29 +594,37 @@ int cj_scan_resync(JPGReader* jpg) {
   return cj_scan_write(jpg);
 }
 
-extern "C" void decodeScanGPU(JPGReader* jpg) {
-  // SOS header: the checks of src/decodeScanGPU.cu:124-141
+// SOS header: the checks of src/decodeScanGPU.cu:124-141.  Returns 0 or a
+// format.h error code; on success jpg->pos is on the first entropy byte.
+int cj_parse_sos(JPGReader* jpg) {
   unsigned char* pos = jpg->pos;
-  if (pos + 2 > jpg->end + 2) THROW(SYNTAX_ERROR);
+  if (pos + 2 > jpg->end + 2) return SYNTAX_ERROR;
   unsigned int header_len = read16(pos);
-  if (pos + header_len > jpg->end) THROW(SYNTAX_ERROR);
+  if (pos + header_len > jpg->end) return SYNTAX_ERROR;
   pos += 2;
-  if (!jpg->num_channels) THROW(SYNTAX_ERROR);  // SOS before SOF
-  if (header_len < 4u + 2u * jpg->num_channels) THROW(SYNTAX_ERROR);
-  if (*(pos++) != jpg->num_channels) THROW(UNSUPPORTED_ERROR);
+  if (!jpg->num_channels) return SYNTAX_ERROR;  // SOS before SOF
+  if (header_len < 4u + 2u * jpg->num_channels) return SYNTAX_ERROR;
+  if (*(pos++) != jpg->num_channels) return UNSUPPORTED_ERROR;
   for (int i = 0; i < jpg->num_channels; i++, pos += 2) {
     ColourChannel* ch = &jpg->channels[i];
-    if (pos[0] != ch->id) THROW(SYNTAX_ERROR);
-    if (pos[1] & 0xEE) THROW(SYNTAX_ERROR);
+    if (pos[0] != ch->id) return SYNTAX_ERROR;
+    if (pos[1] & 0xEE) return SYNTAX_ERROR;
     ch->dc_id = pos[1] >> 4;
     ch->ac_id = (pos[1] & 1) | 2;
     // the reference would decode with an uninitialised table here
     if (!(jpg->huff_defined & (1 << ch->dc_id)) || !(jpg->huff_defined & (1 << ch->ac_id)))
-      THROW(SYNTAX_ERROR);
+      return SYNTAX_ERROR;
   }
-  if (pos[0] || pos[1] != 63 || pos[2]) THROW(UNSUPPORTED_ERROR);
+  if (pos[0] || pos[1] != 63 || pos[2]) return UNSUPPORTED_ERROR;
   jpg->pos += header_len;
-  int err = cj_scan_launch(jpg);
+  if ((size_t)(jpg->end - jpg->pos) > CJ_MAX_SCAN_BYTES) return UNSUPPORTED_ERROR;
+  return 0;
+}
+
+extern "C" void decodeScanGPU(JPGReader* jpg) {
+  int err = cj_parse_sos(jpg);
+  if (err) THROW(err);
+  err = cj_scan_launch(jpg);
   if (err) THROW(err);
   // The entropy-coded data runs to the end of the file (as in the reference,
   // which unstuffs and decodes up to jpg->end); device errors are folded in

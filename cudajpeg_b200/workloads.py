@@ -58,6 +58,9 @@ def encode(arr: np.ndarray, mode: str, quality: int, restart: int = 0,
     else:
         img = Image.fromarray(arr, "RGB")
         kw["subsampling"] = SUBSAMPLING[mode]
+    # (optimize=True fails inside Pillow when the compressed scan outgrows
+    # the encoder buffer it sizes from the pixel count: near-incompressible
+    # content at quality >= 95)
     img.save(buf, "JPEG", **kw)
     return buf.getvalue()
 
@@ -128,20 +131,38 @@ def precision_8192(mode: str, seed: int = 3, size: int = 8192) -> JpegSample:
     return JpegSample(encode(arr if ch == 3 else arr[..., 0], mode, 95), size, size, mode, 95, 0)
 
 
-def mixed_batch(n: int = 1024, seed: int = 4, max_side: int = 2048) -> list:
+def _mixed_one(args) -> JpegSample:
+    seed, k, w, h, mode, q, ri = args
+    rng = np.random.default_rng([seed, k])
+    arr = smooth_content(rng, w, h, 1 if mode == "gray" else 3)
+    return JpegSample(encode(arr if mode != "gray" else arr[..., 0], mode, q, ri), w, h, mode, q, ri)
+
+
+def mixed_batch_plan(n: int = 1024, seed: int = 4, max_side: int = 2048) -> list:
+    """Per-image (seed, index, w, h, mode, quality, restart) of a mixed batch."""
     rng = np.random.default_rng(seed)
-    out = []
     modes = np.array(["420", "422", "444", "gray"])
-    for _ in range(n):
+    plan = []
+    for k in range(n):
         w, h = (np.exp(rng.uniform(np.log(64), np.log(max_side), 2)) / 8).round().astype(int) * 8
         w, h = int(max(w, 8)), int(max(h, 8))
         mode = str(rng.choice(modes, p=[0.6, 0.2, 0.1, 0.1]))
         q = int(rng.integers(50, 96))
         ri = int(rng.integers(16, 65)) if rng.random() < 0.3 else 0
-        arr = smooth_content(rng, w, h, 1 if mode == "gray" else 3)
-        out.append(JpegSample(encode(arr if mode != "gray" else arr[..., 0], mode, q, ri),
-                              w, h, mode, q, ri))
-    return out
+        plan.append((seed, k, w, h, mode, q, ri))
+    return plan
+
+
+def mixed_batch(n: int = 1024, seed: int = 4, max_side: int = 2048, workers: int = 0) -> list:
+    """The mixed batch; `workers` > 1 encodes in a spawn-started process pool
+    (safe to call after CUDA has been initialised)."""
+    plan = mixed_batch_plan(n, seed, max_side)
+    if workers and workers > 1 and n > 8:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_mixed_one, plan, chunksize=8))
+    return [_mixed_one(a) for a in plan]
 
 
 def small_case(seed: int, w: int, h: int, mode: str, quality: int = 85, restart: int = 0,

@@ -81,6 +81,49 @@ long long cjReaderLaunchCount(const JPGReader *r);
 int cjDebugHuffDecode(const unsigned char counts[16], const unsigned char *symbols,
                       unsigned int win16);
 
+/* ---- Batched decoder: many JPEGs in one persistent, cooperative kernel ----
+ *
+ * The files of a batch lie back to back in one host buffer `blob` (pinned
+ * memory gives the fastest copy) at offsets[i], sizes[i].  Each image is
+ * parsed on the host up to its scan; everything after -- Huffman table
+ * build, destuffing, restart intervals, the parallel Huffman decode,
+ * coefficient write-out and the fused iDCT / upsample / colour stage -- runs
+ * in ONE kernel launch for the whole batch.  Images are independent: a
+ * corrupt image reports its own error and the others still decode.  Output
+ * i is RGB (width*height*3) or grey (width*height), identical to openJPG's
+ * for the same file. */
+typedef struct CJBatch CJBatch;
+
+CJBatch *cjBatchCreate(void);
+void cjBatchDestroy(CJBatch *b);
+int cjBatchSetSubsequenceBits(CJBatch *b, int bits);
+
+/* Parse, plan and queue the host->device copy of a batch (asynchronous). */
+int cjBatchStage(CJBatch *b, int n, const unsigned char *blob, const int64_t *offsets,
+                 const int64_t *sizes);
+/* Queue the decode kernel over the staged batch (inputs already on the
+ * device; may be re-run to re-decode them). */
+int cjBatchRun(CJBatch *b);
+/* Queue the device->host copy of all outputs into the batch's pinned buffer. */
+int cjBatchFetch(CJBatch *b);
+/* Wait for the queued work; errors[i] (may be NULL) gets image i's format.h
+ * code.  Returns 0 or a batch-level error. */
+int cjBatchWait(CJBatch *b, int *errors);
+/* Stage + run + fetch + wait. */
+int cjBatchDecode(CJBatch *b, int n, const unsigned char *blob, const int64_t *offsets,
+                  const int64_t *sizes, int *errors);
+/* Output of image i after a fetch (host) or a run (device); NULL if image i
+ * was rejected by the host parse. */
+const unsigned char *cjBatchImage(const CJBatch *b, int i, int *width, int *height, int *channels);
+const unsigned char *cjBatchDeviceImage(const CJBatch *b, int i);
+void *cjBatchStream(const CJBatch *b);
+/* stats[0..10]: images submitted, images on the device, grid CTAs, warp
+ * items, destuff tiles, pixel tiles, fix-up passes of the last run, input
+ * bytes, output bytes, dynamic shared memory, kernel launches so far. */
+void cjBatchStats(const CJBatch *b, int64_t *stats);
+/* Device time of the last cjBatchRun, in milliseconds. */
+float cjBatchKernelMs(const CJBatch *b);
+
 #ifdef __cplusplus
 }
 #endif

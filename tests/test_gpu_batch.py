@@ -1,0 +1,79 @@
+"""The batched decoder (one persistent cooperative kernel per batch) against
+the oracle: every image of a mixed batch -- uneven sizes, all subsampling
+modes, restart intervals, corrupt files -- decodes exactly as alone."""
+import numpy as np
+import pytest
+
+from cudajpeg_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def check_batch(cj, oracle_mod, files, sub_bits=0):
+    with cj.Batch(sub_bits=sub_bits) as b:
+        imgs, errs = b.decode(files)
+        stats = b.stats()
+    for k, data in enumerate(files):
+        ref = oracle_mod.decode(data)
+        assert errs[k] == ref.error, (k, errs[k], ref.error)
+        if ref.error == 0:
+            assert np.array_equal(imgs[k], ref.pixels), k
+    return stats
+
+
+def test_mixed_batch_matches_oracle(cj, oracle_mod):
+    files = [s.data for s in W.mixed_batch(n=40, seed=21, max_side=700)]
+    stats = check_batch(cj, oracle_mod, files)
+    assert stats["on_device"] == 40 and stats["launches"] == 1
+
+
+def test_golden_cases_in_one_batch(cj, golden, oracle_mod):
+    """Valid, unsupported and corrupt files side by side: each keeps its own
+    result (a corrupt file fails alone)."""
+    names = sorted(golden)
+    files = [golden[n]["jpeg"].tobytes() for n in names]
+    with cj.Batch() as b:
+        imgs, errs = b.decode(files)
+    for n, img, e in zip(names, imgs, errs):
+        case = golden[n]
+        assert e == int(case["error"]), (n, e)
+        if e == 0:
+            ref = case["pixels"] if "pixels" in case else oracle_mod.decode(case["jpeg"].tobytes()).pixels
+            assert np.array_equal(img, ref), n
+
+
+@pytest.mark.parametrize("sub_bits", [256, 1024, 4096])
+def test_batch_subsequence_sizes(cj, oracle_mod, sub_bits):
+    files = [s.data for s in W.mixed_batch(n=12, seed=5, max_side=900)]
+    check_batch(cj, oracle_mod, files, sub_bits)
+
+
+def test_batch_rerun_and_large_image(cj, oracle_mod):
+    big = W.single_4096().data
+    files = [big] + [s.data for s in W.mixed_batch(n=6, seed=8, max_side=300)]
+    with cj.Batch() as b:
+        imgs, errs = b.decode(files)
+        assert errs == [0] * len(files)
+        first = [im.copy() for im in imgs]
+        b.run()         # device-resident re-decode of the staged batch
+        b.fetch()
+        assert b.wait() == [0] * len(files)
+        for k in range(len(files)):
+            assert np.array_equal(b.image(k), first[k])
+    assert np.array_equal(first[0], oracle_mod.decode(big).pixels)
+
+
+def test_batch_same_result_alone_and_in_mix(cj):
+    files = [s.data for s in W.mixed_batch(n=16, seed=33, max_side=600)]
+    with cj.Batch() as b:
+        mixed, errs = b.decode(files)
+        assert all(e == 0 for e in errs)
+        for k in (0, 5, 15):
+            alone, e2 = b.decode([files[k]])
+            assert e2 == [0] and np.array_equal(alone[0], mixed[k])
+
+
+def test_batch_all_rejected_on_host(cj):
+    with cj.Batch() as b:
+        imgs, errs = b.decode([b"\xff\xd8\xff\xd9", b"not a jpeg at all"])
+    assert errs == [1, 5] and imgs == [None, None]

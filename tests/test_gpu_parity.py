@@ -55,7 +55,7 @@ CASES = [(100 + i, w, h, m, q, ri, cont) for i, (w, h, m, q, ri, cont) in enumer
 
 @pytest.mark.parametrize("seed,w,h,mode,q,ri,content", CASES)
 def test_random_images_against_oracle(cj, oracle_mod, seed, w, h, mode, q, ri, content):
-    s = W.small_case(seed, w, h, mode, q, ri, content, optimize=(seed % 3 == 0))
+    s = W.small_case(seed, w, h, mode, q, ri, content, optimize=(seed % 3 == 0 and content != "noise"))
     ref = oracle_mod.decode(s.data)
     assert ref.error == 0
     err, coefs, px = decode_all(cj, s.data)
