@@ -2,22 +2,28 @@
 """bench.py -- decoded MPix/s of the baseline-JPEG decode path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cudajpeg|reference]
-                    [--workload single_4096|single_1024]
+                    [--workload mixed_batch|single_4096|single_1024]
 
-One step = one decode of one synthetic JPEG (default: 4096x4096 4:2:0 q90,
-about 2.6 MB of entropy-coded data) through the whole path: destuff, parallel
-Huffman decode, coefficient write-out, fused iDCT + upsample + colour.
+Default workload (the batching configuration): one batch of 1024 seeded
+synthetic baseline JPEGs, W and H log-uniform in [64, 2048], 4:2:0 / 4:2:2 /
+4:4:4 / grey with p = .6/.2/.1/.1, quality U[50, 95], 30% with restart
+intervals of 16-64 MCUs (about 320 MPix, 58 MB of JPEG).  One step = one
+decode of the whole batch by the persistent batch kernel (cjBatchRun).
+The single_* workloads time the plain per-image path (openJPG) instead.
 
 * ``value``   device-resident throughput: the compressed bytes are already in
-  HBM when the timed region starts (cjReaderRedecodeDevice); each step is
-  timed with CUDA events on the decoder's stream, and L2 is flushed (256 MiB
-  write) before every step, outside the events.  Max over ranks.
-* ``e2e``     the same metric through the public C API (openJPGMem): per step
-  the host->device copy of the scan from pinned memory, the decode, and the
-  device->host copy of the RGB image into the reader's pinned buffer.
-* ``roofline`` the dominant kernel's algorithmic bytes / its mean duration
-  (per-kernel CUDA events inside the timed region) against the measured HBM
-  copy bandwidth in MEASURED_PEAKS.json.
+  HBM when the timed region starts; each step is timed with CUDA events on
+  the decoder's stream.  The batch's working set (inputs, coefficients,
+  outputs: ~1.6 GB) is far larger than L2; for the single-image workloads L2
+  is flushed (256 MiB write) before every step, outside the events.  Max
+  over ranks.
+* ``e2e``     the same metric through the public C API: per step the host
+  parse, the host->device copy of the files from pinned memory, the decode,
+  and the device->host copy of every decoded image into pinned memory.
+* ``roofline`` the dominant kernel's algorithmic bytes (entropy-coded bytes
+  read + output pixels written) / its mean duration, against the measured
+  HBM copy bandwidth in MEASURED_PEAKS.json.
+* ``plain_path`` (batch workload) the per-image path over the same images.
 * ``cpu_baseline`` the reference's own CPUonly decoder (compiled from its
   sources into oracle/_ref) on the host cores, on a bounded sample.
 
@@ -66,112 +72,128 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="cudajpeg", choices=["cudajpeg", "reference"])
-    ap.add_argument("--workload", default="single_4096", choices=["single_4096", "single_1024"])
+    ap.add_argument("--workload", default="mixed_batch",
+                    choices=["mixed_batch", "single_4096", "single_1024"])
+    ap.add_argument("--batch-size", type=int, default=1024)
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
-def make_workload(name: str):
-    from cudajpeg_b200 import workloads as W
-    s = W.single_4096() if name == "single_4096" else W.single_1024()
-    cfg = {"workload": f"{name}_{s.mode}_q{s.quality}", "width": s.width, "height": s.height,
-           "subsampling": {"420": "4:2:0", "422": "4:2:2", "444": "4:4:4"}.get(s.mode, "grey"),
-           "quality": s.quality, "restart_interval": s.restart, "file_bytes": len(s.data),
-           "data": "synthetic, seeded (cudajpeg_b200/workloads.py), Pillow/libjpeg encoder with "
-                   "Annex K Huffman tables"}
-    return s, cfg
+class Workload:
+    """The files of one step, their pixel count and the JSON `config`."""
+
+    def __init__(self, name: str, batch_size: int):
+        from cudajpeg_b200 import workloads as W
+        self.name = name
+        if name == "mixed_batch":
+            samples = W.mixed_batch(n=batch_size, workers=min(32, os.cpu_count() or 1))
+            self.config = {"workload": f"mixed_batch_{batch_size}", "images": batch_size,
+                           "sides": "log-uniform [64, 2048], multiples of 8",
+                           "subsampling": "4:2:0/4:2:2/4:4:4/grey p=.6/.2/.1/.1",
+                           "quality": "U[50, 95]",
+                           "restart": "30% with 16-64 MCU intervals"}
+        else:
+            samples = [W.single_4096() if name == "single_4096" else W.single_1024()]
+            s = samples[0]
+            self.config = {"workload": f"{name}_{s.mode}_q{s.quality}", "images": 1,
+                           "width": s.width, "height": s.height, "subsampling": s.mode,
+                           "quality": s.quality, "restart": s.restart}
+        self.samples = samples
+        self.files = [s.data for s in samples]
+        self.pixels = sum(s.pixels for s in samples)
+        self.out_bytes = sum(s.pixels * (1 if s.mode == "gray" else 3) for s in samples)
+        self.file_bytes = sum(len(f) for f in self.files)
+        self.config.update({"MPix": round(self.pixels / 1e6, 3), "file_MB": round(self.file_bytes / 1e6, 3),
+                            "data": "synthetic, seeded (cudajpeg_b200/workloads.py); Pillow/libjpeg "
+                                    "encoder, Annex K Huffman tables"})
 
 
 # ---------------------------------------------------------------- CPU baseline
 
-def ref_cpu_time(data: bytes, threads: int, budget_s: float):
-    """Time the reference CPUonly decoder (oracle/_ref) -- or, if that build
-    is absent, the oracle port -- with one image per thread on `threads`
-    host threads for about `budget_s` seconds.  Returns (kind, seconds,
-    decoded pixels)."""
+def ref_cpu_time(files, threads: int, budget_s: float):
+    """Time the reference CPUonly decoder (oracle/_ref) -- or, if that build is
+    absent, the oracle port -- decoding `files` from /dev/shm, one image per
+    thread at a time on `threads` threads, for about `budget_s` seconds.
+    Returns (kind, seconds, decoded pixels, failed decodes)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     d = "/dev/shm" if os.path.isdir("/dev/shm") else tempfile.gettempdir()
-    fd, path = tempfile.mkstemp(suffix=".jpg", dir=d)
-    with os.fdopen(fd, "wb") as f:
-        f.write(data)
+    tmp = tempfile.mkdtemp(dir=d)
+    paths = []
+    for k, data in enumerate(files):
+        p = os.path.join(tmp, f"{k}.jpg")
+        with open(p, "wb") as f:
+            f.write(data)
+        paths.append(p)
     try:
         if O.ref_available():
-            secs, px, fails = O.ref_cpu_bench([path], 1, 1)  # calibrate: one decode
-            if fails:
-                raise RuntimeError("reference CPUonly decoder failed on the workload")
-            iters = max(1, int(budget_s / max(secs, 1e-4)))
-            secs, px, fails = O.ref_cpu_bench([path] * threads, iters, threads)
-            return "reference", secs, px
+            secs, px, fails = O.ref_cpu_bench(paths, 1, threads)  # one pass calibrates
+            iters = max(1, int(budget_s / max(secs, 1e-3)))
+            if iters > 1:
+                secs, px, fails = O.ref_cpu_bench(paths, iters, threads)
+            else:
+                iters = 1
+            return "reference", secs, px, fails
         from concurrent.futures import ThreadPoolExecutor
-        t0 = time.perf_counter()
-        ref = O.decode(data)
-        per = time.perf_counter() - t0
-        iters = max(1, int(budget_s / per))
+
+        def one(data):
+            r = O.decode(data)
+            return (r.width * r.height, 0) if r.error == 0 else (0, 1)
         t0 = time.perf_counter()
         with ThreadPoolExecutor(threads) as ex:
-            list(ex.map(lambda _: O.decode(data), range(iters * threads)))
-        return "port", time.perf_counter() - t0, iters * threads * ref.width * ref.height
+            res = list(ex.map(one, files))
+        secs = time.perf_counter() - t0
+        return "port", secs, sum(r[0] for r in res), sum(r[1] for r in res)
     finally:
-        os.unlink(path)
+        for p in paths:
+            os.unlink(p)
+        os.rmdir(tmp)
 
 
-def cpu_baseline(sample, threads: int, budget_s: float) -> dict:
-    kind, secs, px = ref_cpu_time(sample.data, threads, budget_s)
-    nimg = px // sample.pixels
+def cpu_baseline(wl: Workload, threads: int, budget_s: float) -> dict:
+    kind, secs, px, fails = ref_cpu_time(wl.files, threads, budget_s)
     who = ("reference CPUonly openJPG, CPUonly/src/main.c:10" if kind == "reference"
            else "oracle port of the reference path")
+    note = (f"; {fails} decodes failed (CPUonly rejects restart markers, "
+            f"CPUonly/src/decodeScanCPU.c:41-43), their pixels are not counted") if fails else ""
     return {"value": round(px / secs / 1e6, 3), "unit": "MPix/s", "cores": threads, "kind": kind,
-            "sample": f"{nimg} decodes of the workload file from /dev/shm in {secs:.1f} s "
-                      f"({who}, one image per thread)"}
+            "sample": f"{px / 1e6:.1f} MPix decoded in {secs:.1f} s from /dev/shm, "
+                      f"{wl.config['workload']} files ({who}, one image per thread){note}"}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sample, cfg = make_workload(args.workload)
+    wl = Workload(args.workload, args.batch_size)
     threads = os.cpu_count() or 1
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     if not O.ref_available():
         O.build()
-    # per step: every thread decodes the workload once
-    d = "/dev/shm" if os.path.isdir("/dev/shm") else tempfile.gettempdir()
-    fd, path = tempfile.mkstemp(suffix=".jpg", dir=d)
-    with os.fdopen(fd, "wb") as f:
-        f.write(sample.data)
-    try:
-        kind = "reference" if O.ref_available() else "port"
-        times = []
-        for k in range(args.warmup + args.steps):
-            if kind == "reference":
-                secs, px, fails = O.ref_cpu_bench([path] * threads, 1, threads)
-                if fails:
-                    raise RuntimeError("reference decode failed")
-            else:
-                from concurrent.futures import ThreadPoolExecutor
-                t0 = time.perf_counter()
-                with ThreadPoolExecutor(threads) as ex:
-                    list(ex.map(lambda _: O.decode(sample.data), range(threads)))
-                secs = time.perf_counter() - t0
-            if k >= args.warmup:
-                times.append(secs)
-    finally:
-        os.unlink(path)
+    times, pix, fails = [], 0, 0
+    for k in range(args.warmup + args.steps):
+        # each step decodes the workload's files once, spread over all threads
+        kind, secs, px, f = ref_cpu_time(wl.files, threads, 0.0)
+        if k >= args.warmup:
+            times.append(secs)
+            pix += px
+            fails = f
     total = sum(times)
-    value = threads * sample.pixels * args.steps / total / 1e6
+    value = pix / total / 1e6
+    note = (f"; {fails} of {len(wl.files)} files fail in CPUonly (restart markers) and "
+            f"their pixels are not counted") if fails else ""
     line = {"metric": METRIC, "value": round(value, 3), "unit": "MPix/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic",
-            "config": cfg, "impl": "reference",
+            "config": wl.config, "impl": "reference",
             "cpu_baseline": {"value": round(value, 3), "unit": "MPix/s", "cores": threads,
                              "kind": kind,
-                             "sample": f"each step decodes the workload once on each of {threads} "
-                                       f"threads (CPUonly openJPG from /dev/shm)"},
+                             "sample": f"each step decodes the {len(wl.files)} workload files once "
+                                       f"on {threads} threads (CPUonly openJPG from /dev/shm){note}"},
             "e2e": {"value": round(value, 3), "unit": "MPix/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -249,25 +271,140 @@ def read_traffic(kernel: str, workload: str):
     return float(m.group(1)) if m else None
 
 
-def run_gpu(args):
+def plain_path_value(cj, files) -> dict:
+    """The plain per-image path over the same files: device-resident re-decode
+    of each image (cjReaderRedecodeDevice), device time summed."""
+    import torch
+    r = cj.Reader()
+    ext = None
+    total_ms, px = 0.0, 0
+    for data in files:
+        if r.open_bytes(data, check=False):
+            continue
+        if ext is None:  # the reader's stream exists after its first decode
+            ext = torch.cuda.ExternalStream(r.stream())
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(ext)
+        r.redecode_device()
+        e.record(ext)
+        e.synchronize()
+        total_ms += s.elapsed_time(e)
+        inf = r.info()
+        px += inf["width"] * inf["height"]
+    r.close()
+    return {"value": round(px / total_ms / 1e3, 2), "unit": "MPix/s",
+            "how": "openJPG per image, then cjReaderRedecodeDevice timed with CUDA events "
+                   "per image, summed over the same files"}
+
+
+def run_batch(args, wl, world, rank, local, dist):
     import numpy as np
     import torch
 
     import cudajpeg_b200 as cj
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
+    blob, offsets, sizes = cj.Batch.pack(wl.files)
+    src = torch.empty(len(blob), dtype=torch.uint8, pin_memory=True)
+    src.numpy()[:] = blob
+    b = cj.Batch()
+    b.stage(src.data_ptr(), offsets, sizes)
+    b.run()
+    b.fetch()
+    errs = b.wait()
+    if any(errs):
+        raise RuntimeError(f"batch decode errors: {sum(1 for e in errs if e)}")
+    ext = torch.cuda.ExternalStream(b.stream())
+    for _ in range(args.warmup):
+        b.run()
+    b.wait()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    phases: dict = {}
+    launches0 = b.stats()["launches"]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            starts[k].record(ext)
+            b.run()
+            ends[k].record(ext)
+            if any(b.wait()):
+                raise RuntimeError("batch run reported image errors")
+            for name, ms in b.phase_ms().items():
+                phases.setdefault(name, []).append(ms)
+        torch.cuda.synchronize()
+    launches = b.stats()["launches"] - launches0
+    if dist:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * wl.pixels * args.steps / (total_ms / 1e3) / 1e6
 
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    # end to end: host parse + H2D of the pinned blob + decode + D2H of all images
+    e2e_ms = []
+    if dist:
+        dist.barrier()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        b.stage(src.data_ptr(), offsets, sizes)
+        b.run()
+        b.fetch()
+        if any(b.wait()):
+            raise RuntimeError("batch decode errors")
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e_total = sum(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * wl.pixels * args.steps / (e2e_total / 1e3) / 1e6
+    st = b.stats()
+    b.close()
 
-    sample, cfg = make_workload(args.workload)
+    peaks = read_peaks()
+    mean_ms = total_ms / args.steps
+    alg = wl.file_bytes + wl.out_bytes
+    achieved = alg / (mean_ms / 1e3) / 1e9
+    pm = {k: round(statistics.mean(v), 4) for k, v in phases.items()}
+    lat = sorted(e2e_ms)
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean_ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8/int16/int32", "data": "synthetic",
+            "config": dict(wl.config, parallelism=f"replicas{world}",
+                           l2="working set ~1.6 GB per step, larger than L2 (126 MB)",
+                           compressed_MB_per_s=round(world * wl.file_bytes * args.steps
+                                                     / (total_ms / 1e3) / 1e6, 1),
+                           passes=st["passes"], grid_ctas=st["grid"], warp_items=st["warp_items"]),
+            "e2e": {"value": round(e2e_value, 2), "unit": "MPix/s",
+                    "h2d_bytes_per_step": int(len(blob)),
+                    "d2h_bytes_per_step": int(wl.out_bytes),
+                    "latency_ms_p50": round(lat[len(lat) // 2], 3),
+                    "latency_ms_p99": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 3)},
+            "roofline": {"bound": "hbm", "kernel": "k_decode_batch", "achieved": round(achieved, 1),
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": round(achieved / peaks["hbm_gbs"], 4),
+                         "traffic": read_traffic("k_decode_batch", args.workload),
+                         "algorithmic_bytes": int(alg), "peak_source": peaks["source"]},
+            "phase_ms": pm, "gpu_launches": int(launches), "clocks": clocks.summary()}
+    if rank == 0 and world == 1:
+        line["plain_path"] = plain_path_value(cj, wl.files)
+        line["plain_path"]["batched_over_plain"] = round(value / line["plain_path"]["value"], 2)
+    return line
+
+
+def run_single(args, wl, world, rank, local, dist):
+    import numpy as np
+    import torch
+
+    import cudajpeg_b200 as cj
+
+    sample = wl.samples[0]
     n = len(sample.data)
     src = torch.empty(n, dtype=torch.uint8, pin_memory=True)
     src.numpy()[:] = np.frombuffer(sample.data, np.uint8)
@@ -276,20 +413,14 @@ def run_gpu(args):
     info = reader.info()
     ext = torch.cuda.ExternalStream(reader.stream())
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
-    npix = sample.pixels
-    out_bytes = npix * (3 if info["channels"] == 3 else 1)
     nblocks = info["mcux"] * info["mcuy"] * info["bpm"]
-    geom = {"B": info["scan_bytes"], "Bd": info["destuffed"], "n": nblocks, "P": out_bytes}
-
-    # warm-up (device-resident path, then the public API path)
+    geom = {"B": info["scan_bytes"], "Bd": info["destuffed"], "n": nblocks, "P": wl.out_bytes}
     for _ in range(args.warmup):
         reader.redecode_device()
     reader.open_bytes((src.data_ptr(), n))
     torch.cuda.synchronize()
     if reader.sync():
         raise RuntimeError("warm-up decode reported an error")
-
-    # ---- timed: device-resident decode
     reader.set_profile(True)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -315,15 +446,12 @@ def run_gpu(args):
     if reader.sync():
         raise RuntimeError("device decode reported an error")
     reader.set_profile(False)
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
+    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     if dist:
         t = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = world * npix * args.steps / (total_ms / 1e3) / 1e6
-
-    # ---- timed: end to end through openJPGMem (H2D + decode + D2H)
+    value = world * wl.pixels * args.steps / (total_ms / 1e3) / 1e6
     e2e_ms = []
     if dist:
         dist.barrier()
@@ -339,42 +467,57 @@ def run_gpu(args):
         t = torch.tensor([e2e_total], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
-    e2e_value = world * npix * args.steps / (e2e_total / 1e3) / 1e6
+    e2e_value = world * wl.pixels * args.steps / (e2e_total / 1e3) / 1e6
     lat = sorted(e2e_ms)
-
-    # ---- roofline of the dominant kernel
     means = {k: statistics.mean(v) for k, v in kern_ms.items()}
     dom = max(means, key=means.get)
     peaks = read_peaks()
     alg = KERNEL_BYTES[dom](geom)
     achieved = alg / (means[dom] / 1e3) / 1e9
-    traffic = read_traffic(dom, args.workload)
-    kshare = {k: round(v / sum(means.values()), 4) for k, v in means.items()}
-
-    line = {"metric": METRIC, "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
+    reader.close()
+    return {"metric": METRIC, "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8/int16/int32", "data": "synthetic",
-            "config": dict(cfg, parallelism=f"replicas{world}",
+            "config": dict(wl.config, parallelism=f"replicas{world}",
                            l2="flushed before each step (256 MiB write, outside the timing)",
                            compressed_MB_per_s=round(world * info["scan_bytes"] * args.steps
                                                      / (total_ms / 1e3) / 1e6, 1)),
             "e2e": {"value": round(e2e_value, 2), "unit": "MPix/s",
                     "h2d_bytes_per_step": info["scan_bytes"] + info["param_bytes"],
-                    "d2h_bytes_per_step": out_bytes + 32,
+                    "d2h_bytes_per_step": wl.out_bytes + 32,
                     "latency_ms_p50": round(lat[len(lat) // 2], 3),
                     "latency_ms_p99": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 3)},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": round(achieved / peaks["hbm_gbs"], 4),
-                         "traffic": traffic, "algorithmic_bytes": int(alg),
+                         "traffic": read_traffic(dom, args.workload), "algorithmic_bytes": int(alg),
                          "peak_source": peaks["source"]},
-            "kernel_ms": {k: round(v, 4) for k, v in means.items()}, "kernel_share": kshare,
-            "gpu_launches": int(launches),
-            "clocks": clocks.summary()}
+            "kernel_ms": {k: round(v, 4) for k, v in means.items()},
+            "gpu_launches": int(launches), "clocks": clocks.summary()}
+
+
+def run_gpu(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    # the workload is generated in a spawn-started pool before CUDA starts
+    wl = Workload(args.workload, args.batch_size)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    if args.workload == "mixed_batch":
+        line = run_batch(args, wl, world, rank, local, dist)
+    else:
+        line = run_single(args, wl, world, rank, local, dist)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(sample, os.cpu_count() or 1, args.cpu_seconds)
-    reader.close()
+        line["cpu_baseline"] = cpu_baseline(wl, os.cpu_count() or 1, args.cpu_seconds)
     if dist:
         dist.destroy_process_group()
     if rank == 0:

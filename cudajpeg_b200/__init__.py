@@ -34,6 +34,7 @@ ERROR_NAMES = {0: "NO_ERROR", 1: "SYNTAX_ERROR", 2: "UNSUPPORTED_ERROR", 3: "OOM
                -1: "PROGRAMMER_ERROR"}
 
 READER_HOST_COEFFICIENTS = 1
+IDCT_INT, IDCT_F32, IDCT_TC = 0, 1, 2
 
 # Every symbol the C headers in include/ declare (checked by the CPU tests).
 EXPORTED = [
@@ -46,8 +47,11 @@ EXPORTED = [
     "cjReaderDevicePixels", "cjReaderSetProfile", "cjReaderKernelTimes", "cjReaderLaunchCount",
     "cjBatchCreate", "cjBatchDestroy", "cjBatchSetSubsequenceBits", "cjBatchStage", "cjBatchRun",
     "cjBatchFetch", "cjBatchWait", "cjBatchDecode", "cjBatchImage", "cjBatchDeviceImage",
-    "cjBatchStream", "cjBatchStats", "cjBatchKernelMs",
+    "cjBatchStream", "cjBatchStats", "cjBatchKernelMs", "cjBatchPhaseTimes",
 ]
+
+BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
+                "fixup", "warp_scan", "write", "pixel"]
 
 KERNEL_NAMES = ["k_destuff_count", "k_scan_tiles", "k_destuff_scatter", "k_build_segments",
                 "k_sync_intra", "k_sync_inter", "k_scan_warps", "k_decode_write", "k_pixel"]
@@ -124,6 +128,7 @@ def load(build_if_missing: bool = True):
     lib.cjBatchStats.argtypes = [vp, i64p]
     lib.cjBatchKernelMs.restype = C.c_float
     lib.cjBatchKernelMs.argtypes = [vp]
+    lib.cjBatchPhaseTimes.argtypes = [vp, C.POINTER(C.c_float)]
     _lib = lib
     return lib
 
@@ -248,6 +253,26 @@ class Reader:
     def launch_count(self) -> int:
         return int(self.lib.cjReaderLaunchCount(self.ptr))
 
+    def plane(self, c: int, mode: int = 0):
+        """iDCT of component c of the last decode through cjIDCTPlane into a
+        padded uint8 plane [rows, stride] (mode: IDCT_INT / IDCT_F32 / IDCT_TC)."""
+        import torch
+        fields = _Reader.from_address(self.ptr)
+        ch = fields.channels[c]
+        bpm = self.info()["bpm"]
+        first = sum(fields.channels[k].samples_x * fields.channels[k].samples_y for k in range(c))
+        plane = torch.zeros((ch.block_stride, ch.stride), dtype=torch.uint8, device="cuda")
+        coef, _ = self.device_coefficients()
+        q = self.lib.cjReaderDeviceQuantTable(self.ptr, ch.dq_id)
+        torch.cuda.synchronize()
+        err = self.lib.cjIDCTPlane(C.c_void_p(coef), bpm, first, ch.samples_x, ch.samples_y,
+                                   fields.num_blocks_x, fields.num_blocks_y, C.c_void_p(q),
+                                   C.c_void_p(plane.data_ptr()), ch.stride, mode, None)
+        if err:
+            raise DecodeError(err, "cjIDCTPlane")
+        torch.cuda.synchronize()
+        return plane.cpu().numpy()
+
     def device_coefficients(self):
         n = C.c_int64(0)
         p = self.lib.cjReaderDeviceCoefficients(self.ptr, C.byref(n))
@@ -353,6 +378,11 @@ class Batch:
     def kernel_ms(self) -> float:
         return float(self.lib.cjBatchKernelMs(self.ptr))
 
+    def phase_ms(self) -> dict:
+        a = (C.c_float * 16)()
+        n = self.lib.cjBatchPhaseTimes(self.ptr, a)
+        return {BATCH_PHASES[k]: float(a[k]) for k in range(n)}
+
     def stream(self) -> int:
         return self.lib.cjBatchStream(self.ptr)
 
@@ -395,6 +425,24 @@ def _working_space(ptr, c):
     r = _Reader.from_address(ptr)
     ws = r.channels[c].working_space
     return ws.mem, ws.size
+
+
+def idct_blocks_raw(coef_q: np.ndarray, q_nat: np.ndarray, mode: int) -> np.ndarray:
+    """Raw FP32 iDCT (before +128 / rounding / clip) of quantised int16 blocks
+    [n, 64] sharing the natural-order quantisation table q_nat, on the GPU
+    through cjIDCTBlocksRaw (mode IDCT_F32 or IDCT_TC)."""
+    import torch
+    lib = load()
+    c = torch.from_numpy(np.ascontiguousarray(coef_q, np.int16).reshape(-1, 64)).cuda()
+    q = torch.from_numpy(np.ascontiguousarray(q_nat, np.int16).reshape(64)).cuda()
+    out = torch.empty((c.shape[0], 64), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    err = lib.cjIDCTBlocksRaw(C.c_void_p(c.data_ptr()), c.shape[0], C.c_void_p(q.data_ptr()),
+                              C.c_void_p(out.data_ptr()), mode, None)
+    if err:
+        raise DecodeError(err, "cjIDCTBlocksRaw")
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
 
 
 def decode(data, sub_bits: int = 0) -> np.ndarray:

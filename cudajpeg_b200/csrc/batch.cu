@@ -65,13 +65,23 @@ struct CJImageDesc {
   int64_t out_off;           // output byte offset
 };
 
+#define BT_NPHASE 10
 struct CJBatchCtl {
   unsigned bar_count, bar_gen;
   int unstable[3];
   int timeout;
   int passes;
   int pad;
+  unsigned long long t[BT_NPHASE + 1];  // %globaltimer (ns) at each phase start (CTA 0)
 };
+
+__device__ __forceinline__ void bt_stamp(CJBatchCtl* ctl, int k) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    ctl->t[k] = t;
+  }
+}
 
 struct CJBatchArgs {
   const CJImageHeader* hdr;
@@ -239,6 +249,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   const int gwarp0 = blockIdx.x * BT_WARPS + (threadIdx.x >> 5);
   const int gwarps = gridDim.x * BT_WARPS;
 
+  bt_stamp(a.ctl, 0);
   // ---- phase 0: tables + status
   for (int i = blockIdx.x; i < a.n; i += gridDim.x) {
     bt_build_params(a.hdr[i], a.prm[i]);
@@ -250,6 +261,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   }
   bt_grid_sync(a.ctl, gen);
 
+  bt_stamp(a.ctl, 1);
   // ---- phase 1: destuff count
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     int i = bt_find(a.n, t, [&](int k) { return a.desc[k].tile0; });
@@ -266,6 +278,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   }
   bt_grid_sync(a.ctl, gen);
 
+  bt_stamp(a.ctl, 2);
   // ---- phase 2: per-image tile offsets
   for (int i = blockIdx.x; i < a.n; i += gridDim.x) {
     const CJImageDesc& d = a.desc[i];
@@ -290,6 +303,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   }
   bt_grid_sync(a.ctl, gen);
 
+  bt_stamp(a.ctl, 3);
   // ---- phase 3: destuff scatter
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     int i = bt_find(a.n, t, [&](int k) { return a.desc[k].tile0; });
@@ -315,6 +329,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   }
   bt_grid_sync(a.ctl, gen);
 
+  bt_stamp(a.ctl, 4);
   // ---- phase 4: segments and subsequences, one CTA per image
   for (int i = blockIdx.x; i < a.n; i += gridDim.x) {
     const CJImageDesc& d = a.desc[i];
@@ -381,6 +396,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   }
   bt_grid_sync(a.ctl, gen);
 
+  bt_stamp(a.ctl, 5);
   // ---- phase 5: speculative decode + warp settle
   for (int w = gwarp0; w < a.nwarps; w += gwarps) {
     int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
@@ -407,6 +423,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   }
   bt_grid_sync(a.ctl, gen);
 
+  bt_stamp(a.ctl, 6);
   // ---- phase 6: fix-up passes until no warp's last exit moves
   int pass = 0;
   for (; pass < a.max_passes; pass++) {
@@ -472,6 +489,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->passes = pass + 1;
   // the last pass wrote its exits into the other snapshot; nothing reads them
 
+  bt_stamp(a.ctl, 7);
   // ---- phase 7: segmented scan of the warp aggregates (CTA 0)
   if (blockIdx.x == 0) {
     CJAgg5* sm = reinterpret_cast<CJAgg5*>(smem);  // BT_THREADS entries
@@ -508,6 +526,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   }
   bt_grid_sync(a.ctl, gen);
 
+  bt_stamp(a.ctl, 8);
   // ---- phase 8: coefficient write-out
   for (int w = gwarp0; w < a.nwarps; w += gwarps) {
     int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
@@ -536,6 +555,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   }
   bt_grid_sync(a.ctl, gen);
 
+  bt_stamp(a.ctl, 9);
   // ---- phase 9: pixel tiles
   uint32_t parity = 0;
   for (int t = blockIdx.x; t < a.nptiles; t += gridDim.x) {
@@ -908,6 +928,17 @@ const unsigned char* cjBatchDeviceImage(const CJBatch* b, int i) {
 }
 
 void* cjBatchStream(const CJBatch* b) { return (void*)b->stream; }
+
+int cjBatchPhaseTimes(const CJBatch* b, float* ms) {
+  const CJBatchCtl* ctl = (const CJBatchCtl*)b->h_ctl.p;
+  if (!ctl) return 0;
+  float total = cjBatchKernelMs(b);
+  for (int k = 0; k < BT_NPHASE; k++) {
+    if (k + 1 < BT_NPHASE) ms[k] = (float)((ctl->t[k + 1] - ctl->t[k]) * 1e-6);
+    else ms[k] = total - (float)((ctl->t[k] - ctl->t[0]) * 1e-6);
+  }
+  return BT_NPHASE;
+}
 
 void cjBatchStats(const CJBatch* b, int64_t* s) {
   const CJBatchCtl* ctl = (const CJBatchCtl*)b->h_ctl.p;

@@ -7,12 +7,17 @@
 //                in idct_tc.cu.
 // Input is the quantised int16 block buffer decodeScanGPU leaves on the
 // device; the component's blocks are gathered from the MCU-interleaved order.
+#include <cuda_fp16.h>
 #include <math.h>
 #include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
 
 #include "../../include/pixelTransformGPU.h"
 #include "cj_internal.h"
 #include "cj_idct.cuh"
+#include "cj_pixel.cuh"
 
 #define CJ_PLANE_BLOCKS 32   // 8x8 blocks per CTA
 #define CJ_PLANE_THREADS 256  // one thread per (block, row)
@@ -140,7 +145,258 @@ int cj_upload_basis() {
   return 0;
 }
 
-int cj_idct_tc_plane(const CJPlaneArgs& a, cudaStream_t s);  // idct_tc.cu
+
+// ---------------------------------------------------------------- tensor cores
+//
+// The 2-D iDCT of a block is one linear map on its 64 coefficients:
+//   s[8y+x] = sum_{v,u} F[8v+u] * B[v][y] * B[u][x],   B = c_idct_basis
+// so a tile of 128 blocks is one GEMM  D[128 x 64] = A[128 x 64] * K[64 x 64]
+// with K[8v+u][8y+x] = B[v][y] B[u][x].  A holds the dequantised
+// coefficients in FP16 (exact: |value| <= 2048 for every block a real encoder
+// produces; larger blocks are redone on CUDA cores in FP32).  K is split into
+// FP16 halves Khi = fp16(K), Klo = fp16(K - Khi), and D = A*Khi + A*Klo is
+// accumulated in FP32 in tensor memory by tcgen05.mma (M=128, N=64, K=16 per
+// instruction, 8 instructions per tile), issued by one thread.
+//
+// Shared-memory operands use the K-major no-swizzle canonical layout: 8x8
+// "core matrices" of 8 rows x 16 bytes; core (r8, k8) of a 64-wide K operand
+// sits at ((r8 * 8 + k8) * 128) bytes.  LBO (next core along K) = 128 B,
+// SBO (next 8-row group) = 1024 B.
+
+#define TC_M 128
+#define TC_THREADS 128
+
+static uint16_t* g_tc_basis = nullptr;  // device: Khi then Klo, core-matrix layout
+
+__device__ __forceinline__ uint32_t tc_core_off(int r, int k) {
+  return (uint32_t)((((r >> 3) * 8 + (k >> 3)) * 128) + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(1024 >> 4) << 32) | (1ull << 46);
+}
+
+// kind::f16, D = F32, A = B = F16, both K-major, N = 64, M = 128
+#define TC_IDESC ((1u << 4) | (0u << 7) | (0u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24))
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"((uint32_t)TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
+}
+
+// FP32 CUDA-core iDCT of one block straight from global memory (the range
+// fallback of the tensor-core kernel): out[8y+x].
+__device__ void tc_block_f32(const int16_t* blk, const int16_t* q, float* out) {
+  float tmp[64];
+  for (int v = 0; v < 8; v++) {
+    int in[8];
+    for (int u = 0; u < 8; u++) in[u] = (int)blk[8 * v + u] * q[8 * v + u];
+    cj_idct8_f32(in, c_idct_basis, tmp + 8 * v);
+  }
+  for (int x = 0; x < 8; x++) {
+    float col[8], s[8];
+    for (int v = 0; v < 8; v++) col[v] = tmp[8 * v + x];
+    cj_idct8_f32f(col, c_idct_basis, s);
+    for (int y = 0; y < 8; y++) out[8 * y + x] = s[y];
+  }
+}
+
+// RAW = true: write the FP32 values (before +128 / rounding / clip) of block
+// list entries to raw_out; RAW = false: write pixels into the plane.
+template <bool RAW>
+__global__ void __launch_bounds__(TC_THREADS) k_idct_tc(CJPlaneArgs a, const uint16_t* __restrict__ basis,
+                                                       float* raw_out, int* status) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int16_t q[64];
+  uint8_t* sA = smem;               // 128 x 64 fp16 = 16 KiB
+  uint8_t* sB = smem + 16384;       // Khi, Klo: 2 x 64 x 64 fp16 = 16 KiB
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int k = tid; k < 16384 / 16; k += TC_THREADS)
+    reinterpret_cast<uint4*>(sB)[k] = __ldg(reinterpret_cast<const uint4*>(basis) + k);
+  if (tid < 64) q[tid] = a.qnat[tid];
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     cj_smem_addr(&tmem_base)),
+                 "r"(64u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) cj_mbar_init(&bar, 1);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const uint32_t aaddr = cj_smem_addr(sA), baddr = cj_smem_addr(sB);
+  const int64_t ntiles = (a.nblocks + TC_M - 1) / TC_M;
+  uint32_t parity = 0;
+  bool failed = false;
+  for (int64_t t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
+    // ---- A tile: thread m owns block m; dequantise, check range, FP16
+    const int m = tid;
+    const int64_t kb = t * TC_M + m;
+    const bool live = kb < a.nblocks;
+    int bx = 0, by = 0;
+    int64_t gb = 0;
+    bool big = false;
+    if (live) gb = RAW ? kb : cj_plane_src(a, kb, &bx, &by);
+#pragma unroll
+    for (int k8 = 0; k8 < 8; k8++) {
+      uint4 packed = make_uint4(0, 0, 0, 0);
+      if (live) {
+        uint4 raw = __ldg(reinterpret_cast<const uint4*>(a.coef + gb * 64 + k8 * 8));
+        int v[8];
+        cj_unpack_dequant(raw, q + k8 * 8, v);
+        uint32_t h[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          big |= (v[2 * j] > 2048 || v[2 * j] < -2048 || v[2 * j + 1] > 2048 || v[2 * j + 1] < -2048);
+          __half2 p2 = __floats2half2_rn((float)v[2 * j], (float)v[2 * j + 1]);
+          h[j] = *reinterpret_cast<uint32_t*>(&p2);
+        }
+        packed = make_uint4(h[0], h[1], h[2], h[3]);
+      }
+      *reinterpret_cast<uint4*>(sA + tc_core_off(m, k8 * 8)) = packed;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    // ---- 8 MMAs: A * Khi then A * Klo, K = 16 per instruction
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++)
+        tc_mma(tmem, tc_smem_desc(aaddr + kk * 256), tc_smem_desc(baddr + kk * 256), kk > 0);
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++)
+        tc_mma(tmem, tc_smem_desc(aaddr + kk * 256), tc_smem_desc(baddr + 8192 + kk * 256), 1u);
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       cj_smem_addr(&bar))
+                   : "memory");
+    }
+    bool ok = cj_mbar_wait(&bar, parity);
+    parity ^= 1;
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) atomicExch(status, 1);
+      cj_mbar_wait(&bar, parity ^ 1);  // give an in-flight MMA a bounded chance to land
+      failed = true;
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // ---- D row m = block m: 64 FP32 values, lanes 32*warp .. 32*warp+31
+    float d[64];
+    tc_ld32(tmem + ((uint32_t)(32 * warp) << 16), d);
+    tc_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 32, d + 32);
+    if (live) {
+      if (big) tc_block_f32(a.coef + gb * 64, q, d);
+      if (RAW) {
+        float4* o = reinterpret_cast<float4*>(raw_out + kb * 64);
+#pragma unroll
+        for (int k = 0; k < 16; k++) o[k] = make_float4(d[4 * k], d[4 * k + 1], d[4 * k + 2], d[4 * k + 3]);
+      } else {
+#pragma unroll
+        for (int y = 0; y < 8; y++) {
+          uint32_t lo = 0, hi = 0;
+#pragma unroll
+          for (int x = 0; x < 4; x++) lo |= cj_clip8(__float2int_rn(d[8 * y + x]) + 128) << (8 * x);
+#pragma unroll
+          for (int x = 0; x < 4; x++) hi |= cj_clip8(__float2int_rn(d[8 * y + 4 + x]) + 128) << (8 * x);
+          *reinterpret_cast<uint2*>(a.plane + (int64_t)(by * 8 + y) * a.stride + bx * 8) = make_uint2(lo, hi);
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();  // TMEM and the A tile are free for the next tile
+  }
+  (void)lane;
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64u) : "memory");
+}
+
+// Khi / Klo of the Kronecker basis in the K-major core-matrix layout of B
+// (row = pixel n = 8y+x, column = coefficient k = 8v+u).
+static int cj_tc_basis() {
+  if (g_tc_basis) return 0;
+  static uint16_t h[2 * 64 * 64];
+  double b[8][8];
+  for (int u = 0; u < 8; u++)
+    for (int x = 0; x < 8; x++)
+      b[u][x] = (u ? 0.5 : 0.5 / sqrt(2.0)) * cos((2 * x + 1) * u * 3.14159265358979323846 / 16.0);
+  for (int n = 0; n < 64; n++)
+    for (int k = 0; k < 64; k++) {
+      int y = n >> 3, x = n & 7, v = k >> 3, u = k & 7;
+      double w = b[v][y] * b[u][x];
+      __half hi = __double2half(w);
+      __half lo = __double2half(w - (double)__half2float(hi));
+      size_t off = (((n >> 3) * 8 + (k >> 3)) * 128 + (n & 7) * 16 + (k & 7) * 2) / 2;
+      h[off] = *reinterpret_cast<uint16_t*>(&hi);
+      h[4096 + off] = *reinterpret_cast<uint16_t*>(&lo);
+    }
+  CJ_CUDA_TRY(cudaMalloc(&g_tc_basis, sizeof(h)), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaMemcpy(g_tc_basis, h, sizeof(h), cudaMemcpyHostToDevice), CUDA_MEM_ERROR);
+  return 0;
+}
+
+static int* g_tc_status = nullptr;
+
+static int cj_idct_tc_launch(const CJPlaneArgs& a, float* raw, bool is_raw, cudaStream_t s) {
+  if (cj_upload_basis() || cj_tc_basis()) return CUDA_MEM_ERROR;
+  if (!g_tc_status) {
+    CJ_CUDA_TRY(cudaMalloc(&g_tc_status, sizeof(int)), CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaMemset(g_tc_status, 0, sizeof(int)), CUDA_MEM_ERROR);
+  }
+  static bool attr = false;
+  const int smem = 32768;
+  if (!attr) {
+    cudaFuncSetAttribute(k_idct_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_idct_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = true;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int64_t ntiles = (a.nblocks + TC_M - 1) / TC_M;
+  unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)sms * 4);
+  if (grid < 1) grid = 1;
+  if (is_raw)
+    k_idct_tc<true><<<grid, TC_THREADS, smem, s>>>(a, g_tc_basis, raw, g_tc_status);
+  else
+    k_idct_tc<false><<<grid, TC_THREADS, smem, s>>>(a, g_tc_basis, raw, g_tc_status);
+  CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
+  return 0;
+}
+
+int cj_idct_tc_plane(const CJPlaneArgs& a, cudaStream_t s) { return cj_idct_tc_launch(a, nullptr, false, s); }
+
+int cj_idct_tc_raw(const int16_t* coef, const int16_t* qnat, float* out, int64_t nblocks, cudaStream_t s) {
+  CJPlaneArgs a;
+  memset(&a, 0, sizeof(a));
+  a.coef = coef;
+  a.qnat = qnat;
+  a.nblocks = nblocks;
+  return cj_idct_tc_launch(a, out, true, s);
+}
 
 extern "C" int cjIDCTPlane(const short* d_coef, int bpm, int first, int samples_x, int samples_y,
                            int mcux, int mcuy, const short* d_qnat, unsigned char* d_plane,
@@ -175,8 +431,6 @@ extern "C" int cjIDCTPlane(const short* d_coef, int bpm, int first, int samples_
   return 0;
 }
 
-int cj_idct_tc_raw(const int16_t* coef, const int16_t* qnat, float* out, int64_t nblocks,
-                   cudaStream_t s);  // idct_tc.cu
 
 extern "C" int cjIDCTBlocksRaw(const short* d_coef, long long nblocks, const short* d_qnat,
                                float* d_out, int mode, void* stream) {

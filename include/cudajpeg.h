@@ -123,6 +123,10 @@ void *cjBatchStream(const CJBatch *b);
 void cjBatchStats(const CJBatch *b, int64_t *stats);
 /* Device time of the last cjBatchRun, in milliseconds. */
 float cjBatchKernelMs(const CJBatch *b);
+/* Split of the last run (after cjBatchWait) into its 10 phases, in ms:
+ * tables, destuff-count, tile-scan, destuff-scatter, segments, sync, fix-up,
+ * warp-scan, write, pixel.  Returns the number of entries. */
+int cjBatchPhaseTimes(const CJBatch *b, float *ms);
 
 #ifdef __cplusplus
 }

@@ -181,10 +181,30 @@ def _load_ref():
     return _ref_cpu, _ref_gpu
 
 
+class _QuietStdout:
+    """The reference decoders printf diagnostics to stdout (e.g.
+    CPUonly/src/decodeScanCPU.c:41,152); route fd 1 to /dev/null meanwhile."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *a):
+        C.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 def ref_cpu_pixels(path: str):
     """Reference CPUonly decode of a file -> pixels array, or None on failure."""
     cpu, _ = _load_ref()
-    h = cpu.refcpu_open(path.encode())
+    with _QuietStdout():
+        h = cpu.refcpu_open(path.encode())
     if not h:
         return None
     try:
@@ -204,7 +224,8 @@ def ref_gpu_coefs(path: str):
     _, gpu = _load_ref()
     r = gpu.refgpu_new()
     try:
-        err = gpu.refgpu_open(r, path.encode())
+        with _QuietStdout():
+            err = gpu.refgpu_open(r, path.encode())
         if err:
             return err, []
         info = np.zeros(18, np.int32)
@@ -226,5 +247,6 @@ def ref_cpu_bench(paths, iters: int, threads: int):
     arr = (C.c_char_p * len(paths))(*[p.encode() for p in paths])
     px = C.c_longlong(0)
     fails = C.c_int(0)
-    secs = cpu.refcpu_bench(arr, len(paths), iters, threads, C.byref(px), C.byref(fails))
+    with _QuietStdout():
+        secs = cpu.refcpu_bench(arr, len(paths), iters, threads, C.byref(px), C.byref(fails))
     return secs, px.value, fails.value
