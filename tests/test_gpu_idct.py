@@ -46,10 +46,15 @@ def test_raw_error_against_fp64(cj, oracle_mod):
 def test_tensor_core_range_fallback(cj, oracle_mod):
     """Blocks whose dequantised values exceed FP16's exact range go to FP32."""
     rng = np.random.default_rng(3)
-    quant = rng.integers(-300, 300, (300, 64)).astype(np.int16)
+    quant = rng.integers(-20, 20, (300, 64)).astype(np.int16)
     quant[::7] = rng.integers(-20000, 20000, (43, 64))
-    q = rng.integers(1, 120, 64).astype(np.int16)
-    exact = oracle_mod.idct_f64(quant.astype(np.int32) * q[None, :].astype(np.int32))
+    q = rng.integers(1, 100, 64).astype(np.int16)
+    deq = quant.astype(np.int64) * q[None, :].astype(np.int64)
+    exact = oracle_mod.idct_f64(deq.astype(np.int32))
     got = cj.idct_blocks_raw(quant, q, cj.IDCT_TC)
-    scale = np.maximum(1.0, np.abs(exact))
-    assert np.all(np.abs(got - exact) / scale < 1e-4)
+    # FP32 rounding error of a sum of 64 products scales with sum |F| / 8
+    scale = np.maximum(1.0, np.abs(deq).sum(axis=1, keepdims=True) / 8.0)
+    assert np.all(np.abs(got - exact) / scale < 1e-5)
+    small = np.abs(deq).max(axis=1) <= 2048  # blocks that took the tensor-core path
+    assert small.any() and (~small).any()
+    assert np.abs(got[small] - exact[small]).max() < 0.5

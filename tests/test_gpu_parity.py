@@ -124,3 +124,25 @@ def test_entropy_corruption_agrees_with_reference(cj, golden):
         assert err == int(case["error"]), name
         if not err and "pixels" in case:
             assert np.array_equal(px, case["pixels"]), name
+
+
+def test_reference_main_dropin(tmp_path, oracle_mod):
+    """The reference's unmodified src/main.cu, built against include/ and
+    libcudajpeg.so (oracle/_ref/main_dropin), decodes like the oracle."""
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(oracle_mod.__file__), "_ref", "main_dropin")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/main_dropin not built")
+    for mode in ("420", "gray"):
+        s = W.small_case(81, 301, 187, mode, 88, 0, "texture")
+        p = tmp_path / f"in_{mode}.jpg"
+        p.write_bytes(s.data)
+        out = subprocess.run([exe, str(p)], cwd=tmp_path, capture_output=True, text=True, timeout=120)
+        assert out.returncode == 0, out.stdout + out.stderr
+        name = "outfile.pgm" if mode == "gray" else "outfile.ppm"
+        raw = (tmp_path / name).read_bytes()
+        header = b"P5\n301 187\n255\n" if mode == "gray" else b"P6\n301 187\n255\n"
+        assert raw.startswith(header)
+        px = np.frombuffer(raw[len(header):], np.uint8)
+        assert np.array_equal(px, oracle_mod.decode(s.data).pixels.reshape(-1))
