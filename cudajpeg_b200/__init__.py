@@ -48,6 +48,7 @@ EXPORTED = [
     "cjBatchCreate", "cjBatchDestroy", "cjBatchSetSubsequenceBits", "cjBatchStage", "cjBatchRun",
     "cjBatchFetch", "cjBatchWait", "cjBatchDecode", "cjBatchImage", "cjBatchDeviceImage",
     "cjBatchStream", "cjBatchStats", "cjBatchKernelMs", "cjBatchPhaseTimes",
+    "cjDecodeNoAlloc",
 ]
 
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
@@ -129,6 +130,8 @@ def load(build_if_missing: bool = True):
     lib.cjBatchKernelMs.restype = C.c_float
     lib.cjBatchKernelMs.argtypes = [vp]
     lib.cjBatchPhaseTimes.argtypes = [vp, C.POINTER(C.c_float)]
+    ip = C.POINTER(C.c_int)
+    lib.cjDecodeNoAlloc.argtypes = [vp, C.c_size_t, vp, C.c_size_t, ip, ip, ip, vp]
     _lib = lib
     return lib
 

@@ -962,3 +962,200 @@ float cjBatchKernelMs(const CJBatch* b) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- no-allocation decode
+//
+// cjDecodeNoAlloc: the batch kernel above run on one image whose every piece
+// of working memory -- compressed bytes, destuffed bytes, tables, segments,
+// subsequence records, coefficient blocks, status -- lives in one statically
+// sized device array, so the call itself never allocates device (or host)
+// memory.  The array is held by every GPU that loads the library until the
+// process exits.
+
+#define CJ_NOALLOC_SCRATCH_BYTES (24u << 20)  // 24 MiB per device
+#define CJ_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CJ_NOALLOC_SCRATCH_BYTES];
+static unsigned char* g_noalloc_ptr[CJ_NOALLOC_MAX_DEVICES];  // device address per device
+
+static size_t bt_align(size_t x) { return (x + 255) & ~(size_t)255; }
+
+extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned char* d_out,
+                               size_t out_capacity, int* width, int* height, int* channels,
+                               void* stream) {
+  if (!jpeg || !d_out) return PROGRAMMER_ERROR;
+  int dev = 0;
+  CJ_CUDA_TRY(cudaGetDevice(&dev), CUDA_MEM_ERROR);
+  if (dev < 0 || dev >= CJ_NOALLOC_MAX_DEVICES) return UNSUPPORTED_ERROR;
+  if (!g_noalloc_ptr[dev]) {
+    // one-time set-up on this device: the static array's device address
+    // (the host-side symbol is not a device pointer)
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cj_note_cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+      return CUDA_MEM_ERROR;
+    }
+    CJ_CUDA_TRY(cudaFuncSetAttribute(k_decode_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
+                CUDA_MEM_ERROR);
+    g_noalloc_ptr[dev] = (unsigned char*)p;
+  }
+  unsigned char* base = g_noalloc_ptr[dev];
+
+  // host parse on the stack
+  JPGReader r;
+  memset(&r, 0, sizeof(r));
+  CJReaderDevice rd;
+  r.dev = &rd;
+  int err = cj_parse_to_scan(&r, jpeg, size);
+  if (err) return err;
+  CJImageHeader h;
+  CJImageDesc d;
+  memset(&h, 0, sizeof(h));
+  memset(&d, 0, sizeof(d));
+  for (int s = 0; s < 4; s++) {
+    memcpy(h.counts[s], rd.huff[s].counts, 16);
+    memcpy(h.symbols[s], rd.huff[s].symbols, 256);
+  }
+  h.huff_mask = (uint8_t)r.huff_defined;
+  memcpy(h.dq, r.dq_tables, sizeof(h.dq));
+  h.nch = r.num_channels;
+  int bpm = 0;
+  for (int c = 0; c < r.num_channels; c++) {
+    h.comp_dc[c] = (uint8_t)r.channels[c].dc_id;
+    h.comp_ac[c] = (uint8_t)r.channels[c].ac_id;
+    h.comp_q[c] = (uint8_t)r.channels[c].dq_id;
+    h.comp_sx[c] = (uint8_t)r.channels[c].samples_x;
+    h.comp_sy[c] = (uint8_t)r.channels[c].samples_y;
+    bpm += h.comp_sx[c] * h.comp_sy[c];
+  }
+  h.mcux = r.num_blocks_x;
+  h.mcuy = r.num_blocks_y;
+  h.width = r.width;
+  h.height = r.height;
+  h.hmax = r.block_size_x >> 3;
+  h.vmax = r.block_size_y >> 3;
+  int xs = 0, ys = 0;
+  if (r.num_channels == 3) {
+    while ((r.channels[1].width << xs) < r.width) xs++;
+    while ((r.channels[1].height << ys) < r.height) ys++;
+  }
+  h.xshift = (uint8_t)xs;
+  h.yshift = (uint8_t)ys;
+  h.restart_interval = r.restart_interval;
+  const int64_t mcus = (int64_t)h.mcux * h.mcuy;
+  h.nseg_expected = r.restart_interval ? (int)((mcus + r.restart_interval - 1) / r.restart_interval) : 1;
+  h.total_blocks = mcus * bpm;
+  if (h.comp_sx[0] != h.hmax || h.comp_sy[0] != h.vmax) return UNSUPPORTED_ERROR;
+  if (h.nch == 3 && ((h.comp_sx[1] << xs) != h.hmax || (h.comp_sy[1] << ys) != h.vmax))
+    return UNSUPPORTED_ERROR;
+  const int ch = h.nch == 3 ? 3 : 1;
+  const size_t out_bytes = (size_t)h.width * h.height * ch;
+  if (width) *width = h.width;
+  if (height) *height = h.height;
+  if (channels) *channels = ch;
+  if (out_capacity < out_bytes) return PROGRAMMER_ERROR;
+  const int64_t scan_off = (int64_t)(r.pos - jpeg), scan_len = (int64_t)(r.end - r.pos);
+  if ((uint64_t)scan_len > CJ_MAX_SCAN_BYTES) return UNSUPPORTED_ERROR;
+
+  // plan: one image, every buffer carved out of the static array
+  const int S = CJ_SUB_BITS_DEFAULT;
+  d.src_off = scan_off;
+  d.raw_len = scan_len;
+  d.data_off = 0;
+  d.tile0 = 0;
+  d.ntiles = (int)std::max<int64_t>(1, (scan_len + BT_TILE_BYTES - 1) / BT_TILE_BYTES);
+  d.mark0 = 0;
+  d.mark_cap = h.nseg_expected + 1;
+  d.seg0 = 0;
+  d.seg_cap = h.nseg_expected;
+  d.sub_bits = S;
+  d.sub0 = 0;
+  d.sub_cap = ((int)((scan_len * 8 + S - 1) / S) + h.nseg_expected + 1 + 31) & ~31;
+  d.T = cj_pix_tile_mcus(h.hmax, bpm);
+  d.ptile0 = 0;
+  d.nptiles = h.mcuy * ((h.mcux + d.T - 1) / d.T);
+  d.coef0 = 0;
+  d.out_off = 0;
+  const int nwarps = d.sub_cap / 32;
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    size_t o = off;
+    off = bt_align(off + bytes);
+    return o;
+  };
+  const size_t o_hdr = carve(sizeof(CJImageHeader)), o_desc = carve(sizeof(CJImageDesc));
+  const size_t o_prm = carve(sizeof(CJScanParams)), o_st = carve(sizeof(CJStatus));
+  const size_t o_ctl = carve(sizeof(CJBatchCtl));
+  const size_t o_blob = carve(size + 64), o_data = carve((size_t)scan_len + 64);
+  const size_t o_tk = carve((size_t)d.ntiles * 4), o_tm = carve((size_t)d.ntiles * 4);
+  const size_t o_mpos = carve((size_t)d.mark_cap * 4), o_mcode = carve((size_t)d.mark_cap);
+  const size_t o_segs = carve((size_t)d.seg_cap * sizeof(CJSegment));
+  const size_t o_recs = carve((size_t)d.sub_cap * sizeof(CJSubRec));
+  const size_t o_snap = carve((size_t)2 * nwarps * sizeof(uint64_t));
+  const size_t o_wagg = carve((size_t)nwarps * sizeof(CJWarpAgg));
+  const size_t o_carry = carve((size_t)nwarps * sizeof(CJWarpAgg));
+  const size_t o_coef = carve((size_t)h.total_blocks * 128 + 128);
+  if (off > CJ_NOALLOC_SCRATCH_BYTES) {
+    fprintf(stderr,
+            "libcudajpeg: cjDecodeNoAlloc: this image needs %zu bytes of working memory; the "
+            "static scratch holds %u (use openJPG or the batch decoder for larger images)\n",
+            off, CJ_NOALLOC_SCRATCH_BYTES);
+    return UNSUPPORTED_ERROR;
+  }
+  CJPixGeom g;
+  g.nch = h.nch;
+  g.bpm = bpm;
+  g.hmax = h.hmax;
+  g.vmax = h.vmax;
+  g.T = d.T;
+  const size_t smem = std::max(cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1]),
+                               (size_t)BT_THREADS * sizeof(CJAgg5));
+
+  cudaStream_t s = (cudaStream_t)stream;
+  CJ_CUDA_TRY(cudaMemcpyAsync(base + o_hdr, &h, sizeof(h), cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaMemcpyAsync(base + o_desc, &d, sizeof(d), cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaMemcpyAsync(base + o_blob, jpeg, size, cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaMemsetAsync(base + o_ctl, 0, sizeof(CJBatchCtl), s), CUDA_MEM_ERROR);
+  CJBatchArgs a;
+  a.hdr = (const CJImageHeader*)(base + o_hdr);
+  a.desc = (const CJImageDesc*)(base + o_desc);
+  a.prm = (CJScanParams*)(base + o_prm);
+  a.st = (CJStatus*)(base + o_st);
+  a.blob = base + o_blob;
+  a.data = base + o_data;
+  a.tile_keep = (int32_t*)(base + o_tk);
+  a.tile_mark = (int32_t*)(base + o_tm);
+  a.mpos = (uint32_t*)(base + o_mpos);
+  a.mcode = base + o_mcode;
+  a.segs = (CJSegment*)(base + o_segs);
+  a.recs = (CJSubRec*)(base + o_recs);
+  a.snap0 = (uint64_t*)(base + o_snap);
+  a.snap1 = a.snap0 + nwarps;
+  a.wagg = (CJWarpAgg*)(base + o_wagg);
+  a.carry = (CJWarpAgg*)(base + o_carry);
+  a.coef = (int16_t*)(base + o_coef);
+  a.out = d_out;
+  a.ctl = (CJBatchCtl*)(base + o_ctl);
+  a.n = 1;
+  a.ntiles = d.ntiles;
+  a.nwarps = nwarps;
+  a.nptiles = d.nptiles;
+  a.max_passes = nwarps + 2;
+  int sms = 0, per_sm = 0;
+  CJ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_decode_batch, BT_THREADS, smem),
+              CUDA_KERNEL_LAUNCH_ERROR);
+  if (per_sm < 1) return UNSUPPORTED_ERROR;
+  void* args[] = {&a};
+  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_decode_batch, dim3(per_sm * sms), dim3(BT_THREADS), args,
+                                          smem, s),
+              CUDA_KERNEL_LAUNCH_ERROR);
+  CJStatus st;
+  CJBatchCtl ctl;
+  CJ_CUDA_TRY(cudaMemcpyAsync(&st, base + o_st, sizeof(st), cudaMemcpyDeviceToHost, s), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaMemcpyAsync(&ctl, base + o_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, s), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaStreamSynchronize(s), CUDA_KERNEL_LAUNCH_ERROR);
+  if (ctl.timeout || ctl.passes > nwarps + 2) return PROGRAMMER_ERROR;
+  return cj_status_error(&st);
+}

@@ -128,6 +128,34 @@ float cjBatchKernelMs(const CJBatch *b);
  * warp-scan, write, pixel.  Returns the number of entries. */
 int cjBatchPhaseTimes(const CJBatch *b, float *ms);
 
+/* ---- Decoding without allocating: cjDecodeNoAlloc ----
+ *
+ * No counterpart in the reference.  Decodes one baseline JPEG held in host
+ * memory into a device buffer the caller owns, and allocates no device (or
+ * host) memory on the way: for callers that cannot call cudaMalloc while
+ * decoding -- a host application whose own caching allocator owns all of the
+ * GPU's memory, or a latency-critical loop where an allocation (and the
+ * device synchronisation a cudaFree implies) is not acceptable.
+ *
+ * All working memory (compressed and destuffed bytes, tables, decoder state,
+ * coefficient blocks) comes from one static device array of 24 MiB that every
+ * GPU which loads the library keeps until the process exits.  The working set
+ * is roughly 4-12 bytes per pixel depending on subsampling and compression, so
+ * images up to about 2-5 megapixels fit; a larger image is rejected with
+ * UNSUPPORTED_ERROR and a message on stderr naming the bytes it needs.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  Every call shares the array, so calls that
+ * overlap on the GPU (from different host threads or streams) race: run them
+ * one after another.  d_out receives RGB (width*height*3) or grey
+ * (width*height) bytes and out_capacity is its size in bytes (too small:
+ * PROGRAMMER_ERROR).  width/height/channels are filled once the header has
+ * been parsed.  The call waits for its own work on `stream` (NULL = the
+ * default stream) before returning 0 or a format.h error code. */
+int cjDecodeNoAlloc(const unsigned char *jpeg, size_t size, unsigned char *d_out,
+                    size_t out_capacity, int *width, int *height, int *channels, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
