@@ -78,6 +78,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=1.5,
+                    help="seconds of arrivals per rate for the serving measurement (0: skip)")
     return ap.parse_args()
 
 
@@ -297,6 +299,36 @@ def plain_path_value(cj, files) -> dict:
                    "per image, summed over the same files"}
 
 
+def serving_value(wl, seconds: float) -> dict:
+    """Open-loop Poisson request streams of the workload's files (one JPEG
+    per request) through the continuous-batching server at 2k, 8k and 32k
+    requests/s; latency = scheduled arrival -> the request's batch finished
+    on the GPU, outputs left on the device."""
+    import numpy as np
+
+    from cudajpeg_b200 import serve as sv
+    px = np.array([s.pixels for s in wl.samples], np.float64)
+    out = {"how": f"cjServerReplay, {seconds:g} s of Poisson arrivals per rate over the "
+                  f"{len(wl.files)} workload files (cycled), 3 engines, 8 GiB budget",
+           "rates": []}
+    with sv.Server(engines=3, hbm_budget_bytes=8 << 30, max_batch=256) as s:
+        # warm-up: bursts of the largest files grow every engine's buffers to
+        # steady-state size before any measured stream
+        sizes = np.array([len(f) for f in wl.files])
+        for idx in (np.argsort(-px)[:256], np.argsort(-sizes)[:256]):
+            big = [wl.files[i] for i in idx]
+            for _ in range(3):
+                s.replay(big, np.zeros(3 * len(big)))
+        s.replay(wl.files, sv.poisson_arrivals(8000.0, 4000, seed=99))
+        for rate in (2000.0, 8000.0, 32000.0):
+            n = int(rate * seconds)
+            run = s.replay(wl.files, sv.poisson_arrivals(rate, n, seed=7))
+            summ = sv.summarize(run, px, rate)
+            out["rates"].append({k: (round(v, 3) if isinstance(v, float) else v) for k, v in summ.items()})
+        out["server_stats"] = s.stats()
+    return out
+
+
 def run_batch(args, wl, world, rank, local, dist):
     import numpy as np
     import torch
@@ -382,8 +414,8 @@ def run_batch(args, wl, world, rank, local, dist):
                                                      / (total_ms / 1e3) / 1e6, 1),
                            passes=st["passes"], grid_ctas=st["grid"], warp_items=st["warp_items"]),
             "e2e": {"value": round(e2e_value, 2), "unit": "MPix/s",
-                    "h2d_bytes_per_step": int(len(blob)),
-                    "d2h_bytes_per_step": int(wl.out_bytes),
+                    "h2d_bytes_per_step": int(st["input_bytes"]),
+                    "d2h_bytes_per_step": int(st["output_bytes"]),
                     "latency_ms_p50": round(lat[len(lat) // 2], 3),
                     "latency_ms_p99": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 3)},
             "roofline": {"bound": "hbm", "kernel": "k_decode_batch", "achieved": round(achieved, 1),
@@ -395,6 +427,8 @@ def run_batch(args, wl, world, rank, local, dist):
     if rank == 0 and world == 1:
         line["plain_path"] = plain_path_value(cj, wl.files)
         line["plain_path"]["batched_over_plain"] = round(value / line["plain_path"]["value"], 2)
+        if args.serve_seconds > 0:
+            line["serving"] = serving_value(wl, args.serve_seconds)
     return line
 
 

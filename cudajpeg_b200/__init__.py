@@ -48,7 +48,9 @@ EXPORTED = [
     "cjBatchCreate", "cjBatchDestroy", "cjBatchSetSubsequenceBits", "cjBatchStage", "cjBatchRun",
     "cjBatchFetch", "cjBatchWait", "cjBatchDecode", "cjBatchImage", "cjBatchDeviceImage",
     "cjBatchStream", "cjBatchStats", "cjBatchKernelMs", "cjBatchPhaseTimes",
-    "cjDecodeNoAlloc",
+    "cjDecodeNoAlloc", "cjBatchImageGeometry",
+    "cjServerCreate", "cjServerDestroy", "cjServerSubmit", "cjServerWait", "cjServerCopyOut",
+    "cjServerRelease", "cjServerStats", "cjServerReplay",
 ]
 
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
@@ -132,6 +134,18 @@ def load(build_if_missing: bool = True):
     lib.cjBatchPhaseTimes.argtypes = [vp, C.POINTER(C.c_float)]
     ip = C.POINTER(C.c_int)
     lib.cjDecodeNoAlloc.argtypes = [vp, C.c_size_t, vp, C.c_size_t, ip, ip, ip, vp]
+    lib.cjBatchImageGeometry.argtypes = [vp, C.c_int, ip, ip, ip]
+    lib.cjServerCreate.restype = vp
+    lib.cjServerCreate.argtypes = [C.c_int, C.c_longlong, C.c_int]
+    lib.cjServerDestroy.argtypes = [vp]
+    lib.cjServerSubmit.restype = C.c_longlong
+    lib.cjServerSubmit.argtypes = [vp, vp, C.c_size_t]
+    lib.cjServerWait.argtypes = [vp, C.c_longlong, C.c_double, vp]
+    lib.cjServerCopyOut.argtypes = [vp, C.c_longlong, vp, C.c_size_t]
+    lib.cjServerRelease.argtypes = [vp, C.c_longlong]
+    lib.cjServerStats.argtypes = [vp, C.POINTER(C.c_longlong)]
+    lib.cjServerReplay.argtypes = [vp, vp, vp, vp, C.c_int, vp, C.c_int, vp, vp,
+                                   C.POINTER(C.c_double)]
     _lib = lib
     return lib
 

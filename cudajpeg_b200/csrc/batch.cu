@@ -72,6 +72,8 @@ struct CJBatchCtl {
   int timeout;
   int passes;
   int pad;
+  int next_sync, next_write, next_fix[3];  // dynamic work counters
+  int pad2[3];
   unsigned long long t[BT_NPHASE + 1];  // %globaltimer (ns) at each phase start (CTA 0)
 };
 
@@ -141,6 +143,29 @@ __device__ __forceinline__ void bt_grid_sync(CJBatchCtl* ctl, unsigned& gen) {
     gen = g + 1;
   }
   __syncthreads();
+}
+
+// L2-coherent loads of records another SM may have rewritten in this kernel.
+__device__ __forceinline__ CJSubRec bt_load_rec(const CJSubRec* p) {
+  CJSubRec r;
+  const int4* q = reinterpret_cast<const int4*>(p);
+  *reinterpret_cast<int4*>(&r) = __ldcg(q);
+  *(reinterpret_cast<int4*>(&r) + 1) = __ldcg(q + 1);
+  return r;
+}
+__device__ __forceinline__ CJWarpAgg bt_load_agg(const CJWarpAgg* p) {
+  CJWarpAgg r;
+  const int4* q = reinterpret_cast<const int4*>(p);
+  *reinterpret_cast<int4*>(&r) = __ldcg(q);
+  *(reinterpret_cast<int4*>(&r) + 1) = __ldcg(q + 1);
+  return r;
+}
+
+// Next warp item from a work counter (lane 0 takes it, the warp shares it).
+__device__ __forceinline__ int bt_next_item(int* counter) {
+  int w = 0;
+  if ((threadIdx.x & 31) == 0) w = atomicAdd(counter, 1);
+  return __shfl_sync(0xFFFFFFFFu, w, 0);
 }
 
 // Largest i with key(i) <= v over a sorted int32 field of the descriptors.
@@ -236,18 +261,16 @@ __device__ __forceinline__ uint32_t bt_smem_addr(const void* p) {
 
 __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ uint64_t bar;
+  __shared__ uint64_t bar2[2];
   __shared__ int2 sm2[33];
   __shared__ CJPixSmemParams P;
   unsigned gen = 0;
   if (threadIdx.x == 0) {
     gen = atomicAdd(&a.ctl->bar_gen, 0);
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bt_smem_addr(&bar)), "r"(1) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    cj_mbar_init(&bar2[0], 1);
+    cj_mbar_init(&bar2[1], 1);
   }
   const int lane = threadIdx.x & 31;
-  const int gwarp0 = blockIdx.x * BT_WARPS + (threadIdx.x >> 5);
-  const int gwarps = gridDim.x * BT_WARPS;
 
   bt_stamp(a.ctl, 0);
   // ---- phase 0: tables + status
@@ -397,8 +420,8 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   bt_grid_sync(a.ctl, gen);
 
   bt_stamp(a.ctl, 5);
-  // ---- phase 5: speculative decode + warp settle
-  for (int w = gwarp0; w < a.nwarps; w += gwarps) {
+  // ---- phase 5: speculative decode + warp settle (items handed out dynamically)
+  for (int w = bt_next_item(&a.ctl->next_sync); w < a.nwarps; w = bt_next_item(&a.ctl->next_sync)) {
     int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
     const CJImageDesc& d = a.desc[i];
     const int nsub = __ldcg(&a.st[i].nsub), nseg = __ldcg(&a.st[i].nseg);
@@ -430,8 +453,12 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
     const uint64_t* snap_in = (pass & 1) ? a.snap1 : a.snap0;
     uint64_t* snap_out = (pass & 1) ? a.snap0 : a.snap1;
     int* unstable = &a.ctl->unstable[pass % 3];
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->unstable[(pass + 1) % 3] = 0;
-    for (int w = gwarp0; w < a.nwarps; w += gwarps) {
+    int* next = &a.ctl->next_fix[pass % 3];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.ctl->unstable[(pass + 1) % 3] = 0;
+      a.ctl->next_fix[(pass + 1) % 3] = 0;
+    }
+    for (int w = bt_next_item(next); w < a.nwarps; w = bt_next_item(next)) {
       int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
       const CJImageDesc& d = a.desc[i];
       const int nsub = __ldcg(&a.st[i].nsub), nseg = __ldcg(&a.st[i].nseg);
@@ -448,7 +475,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
       const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
       CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
       CJSubRec r;
-      if (ln.active) r = a.recs[d.sub0 + j0 + lane];
+      if (ln.active) r = bt_load_rec(&a.recs[d.sub0 + j0 + lane]);
       else {
         r.start = r.exit = 0;
         r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
@@ -498,7 +525,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
     int lo = threadIdx.x * per, hi = min(nw, lo + per);
     CJAgg5 acc = {0, 0, 0, 0, 0};
     for (int w = lo; w < hi; w++) {
-      CJWarpAgg g = a.wagg[w];
+      CJWarpAgg g = bt_load_agg(&a.wagg[w]);
       acc = cj_op(acc, CJAgg5{g.has_head, g.nblocks, g.dc[0], g.dc[1], g.dc[2]});
     }
     sm[threadIdx.x] = acc;
@@ -520,15 +547,15 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
       o.dc[2] = run.c;
       o.pad[0] = o.pad[1] = o.pad[2] = 0;
       a.carry[w] = o;
-      CJWarpAgg g = a.wagg[w];
+      CJWarpAgg g = bt_load_agg(&a.wagg[w]);
       run = cj_op(run, CJAgg5{g.has_head, g.nblocks, g.dc[0], g.dc[1], g.dc[2]});
     }
   }
   bt_grid_sync(a.ctl, gen);
 
   bt_stamp(a.ctl, 8);
-  // ---- phase 8: coefficient write-out
-  for (int w = gwarp0; w < a.nwarps; w += gwarps) {
+  // ---- phase 8: coefficient write-out (items handed out dynamically)
+  for (int w = bt_next_item(&a.ctl->next_write); w < a.nwarps; w = bt_next_item(&a.ctl->next_write)) {
     int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
     const CJImageDesc& d = a.desc[i];
     CJStatus* st = &a.st[i];
@@ -539,7 +566,7 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
     const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
     CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
     CJSubRec r;
-    if (ln.active) r = a.recs[d.sub0 + j0 + lane];
+    if (ln.active) r = bt_load_rec(&a.recs[d.sub0 + j0 + lane]);
     else {
       r.start = r.exit = 0;
       r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
@@ -556,31 +583,72 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   bt_grid_sync(a.ctl, gen);
 
   bt_stamp(a.ctl, 9);
-  // ---- phase 9: pixel tiles
-  uint32_t parity = 0;
-  for (int t = blockIdx.x; t < a.nptiles; t += gridDim.x) {
-    int i = bt_find(a.n, t, [&](int k) { return a.desc[k].ptile0; });
-    const CJImageDesc& d = a.desc[i];
-    const CJScanParams& prm = a.prm[i];
+  // ---- phase 9: pixel tiles, double-buffered: the TMA copy of a CTA's next
+  // tile is in flight while it computes the current one
+  {
+    int t = blockIdx.x;
+    int buf = 0;
+    uint32_t par[2] = {0, 0};
     CJPixGeom g;
-    g.nch = prm.nch;
-    g.bpm = prm.bpm;
-    g.mcux = prm.mcux;
-    g.mcuy = prm.mcuy;
-    g.width = prm.width;
-    g.height = prm.height;
-    g.hmax = prm.hmax;
-    g.vmax = prm.vmax;
-    g.xs = prm.xshift;
-    g.ys = prm.yshift;
-    g.T = d.T;
-    cj_pix_layout(&g, prm.comp_sx[1], prm.comp_sy[1]);
-    const int gx = (g.mcux + g.T - 1) / g.T;
-    const int local = t - d.ptile0;
-    if (!cj_pixel_tile(prm, a.coef + d.coef0 * 64, a.out + d.out_off, &a.st[i], g, local / gx,
-                       (local % gx) * g.T, smem, &bar, parity, &P))
-      break;
-    parity ^= 1;
+    int cur_img = -1;
+    auto geom_of = [&](int tt, int* local, int* img) {
+      int i = bt_find(a.n, tt, [&](int k) { return a.desc[k].ptile0; });
+      const CJImageDesc& d = a.desc[i];
+      const CJScanParams& prm = a.prm[i];
+      CJPixGeom gg;
+      gg.nch = prm.nch;
+      gg.bpm = prm.bpm;
+      gg.mcux = prm.mcux;
+      gg.mcuy = prm.mcuy;
+      gg.width = prm.width;
+      gg.height = prm.height;
+      gg.hmax = prm.hmax;
+      gg.vmax = prm.vmax;
+      gg.xs = prm.xshift;
+      gg.ys = prm.yshift;
+      gg.T = d.T;
+      cj_pix_layout(&gg, prm.comp_sx[1], prm.comp_sy[1], 2);
+      *local = tt - d.ptile0;
+      *img = i;
+      return gg;
+    };
+    int local = 0;
+    if (t < a.nptiles) {
+      g = geom_of(t, &local, &cur_img);
+      if (threadIdx.x == 0) {
+        const int gx = (g.mcux + g.T - 1) / g.T;
+        cj_pixel_issue(a.coef + a.desc[cur_img].coef0 * 64, g, local / gx, (local % gx) * g.T,
+                       reinterpret_cast<int16_t*>(smem), &bar2[0]);
+      }
+    }
+    while (t < a.nptiles) {
+      const int nt = t + gridDim.x;
+      int nlocal = 0, nimg = -1;
+      CJPixGeom ng;
+      if (nt < a.nptiles) {
+        ng = geom_of(nt, &nlocal, &nimg);
+        if (threadIdx.x == 0) {
+          const int ngx = (ng.mcux + ng.T - 1) / ng.T;
+          int16_t* dst = reinterpret_cast<int16_t*>(smem + (buf ^ 1) * ng.sc1_off);
+          cj_pixel_issue(a.coef + a.desc[nimg].coef0 * 64, ng, nlocal / ngx, (nlocal % ngx) * ng.T, dst,
+                         &bar2[buf ^ 1]);
+        }
+      }
+      const int gx = (g.mcux + g.T - 1) / g.T;
+      const CJImageDesc& d = a.desc[cur_img];
+      const int16_t* sc = reinterpret_cast<const int16_t*>(smem + buf * g.sc1_off);
+      if (!cj_pixel_compute(a.prm[cur_img], a.out + d.out_off, &a.st[cur_img], g, local / gx,
+                            (local % gx) * g.T, sc, smem, &bar2[buf], par[buf], &P)) {
+        if (nt < a.nptiles) cj_mbar_wait(&bar2[buf ^ 1], par[buf ^ 1]);  // the prefetch in flight
+        break;
+      }
+      par[buf] ^= 1;
+      buf ^= 1;
+      t = nt;
+      g = ng;
+      local = nlocal;
+      cur_img = nimg;
+    }
   }
 }
 
@@ -610,6 +678,27 @@ struct CJBatch {
   int grid = 0;
   long long launches = 0;
 };
+
+// Grow-only device buffer in the batch's stream order: the old buffer is
+// freed and the new one allocated on b->stream (stream-ordered allocator),
+// so growing one batch's buffers never waits for work on other streams, as
+// cudaFree would.  50% headroom keeps regrowth rare.
+static int bt_ensure(CJBatch* b, CJDevBuf& d, size_t bytes) {
+  if (d.p && bytes <= d.cap) return 0;
+  if (d.p) cudaFreeAsync(d.p, b->stream);
+  d.p = nullptr;
+  d.cap = 0;
+  size_t cap = bytes + bytes / 2 + 256;
+  cudaError_t e = cudaMallocAsync(&d.p, cap, b->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fprintf(stderr, "libcudajpeg: cudaMallocAsync(%zu) failed: %s\n", cap, cudaGetErrorString(e));
+    d.p = nullptr;
+    return CUDA_MEM_ERROR;
+  }
+  d.cap = cap;
+  return 0;
+}
 
 static int bt_init(CJBatch* b) {
   if (b->ready) return 0;
@@ -777,14 +866,14 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
     blocks += h.total_blocks;
     d.out_off = out_total;
     int ch = h.nch == 3 ? 3 : 1;
-    out_total += (int64_t)h.width * h.height * ch;
+    out_total += ((int64_t)h.width * h.height * ch + 15) & ~(int64_t)15;  // 16-byte aligned starts
     CJPixGeom g;
     g.nch = h.nch;
     g.bpm = bpm;
     g.hmax = h.hmax;
     g.vmax = h.vmax;
     g.T = d.T;
-    smem = std::max(smem, cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1]));
+    smem = std::max(smem, cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1], 2));
     b->dev_of[i] = nd;
     b->dims.push_back(h.width);
     b->dims.push_back(h.height);
@@ -801,18 +890,18 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   b->smem = std::max(smem, (size_t)BT_THREADS * sizeof(CJAgg5));
   if (!nd) return 0;
   size_t nd_ = (size_t)nd;
-  if (cj_dev_ensure(b->hdr, nd_ * sizeof(CJImageHeader)) || cj_dev_ensure(b->desc, nd_ * sizeof(CJImageDesc)) ||
-      cj_dev_ensure(b->prm, nd_ * sizeof(CJScanParams)) || cj_dev_ensure(b->st, nd_ * sizeof(CJStatus)) ||
-      cj_dev_ensure(b->blob, (size_t)blob_bytes + 64) || cj_dev_ensure(b->data, (size_t)data_bytes + 64) ||
-      cj_dev_ensure(b->tile_keep, (size_t)ntiles * 4) || cj_dev_ensure(b->tile_mark, (size_t)ntiles * 4) ||
-      cj_dev_ensure(b->mpos, (size_t)nmark * 4) || cj_dev_ensure(b->mcode, (size_t)nmark) ||
-      cj_dev_ensure(b->segs, (size_t)nseg * sizeof(CJSegment)) ||
-      cj_dev_ensure(b->recs, (size_t)nsubw * 32 * sizeof(CJSubRec)) ||
-      cj_dev_ensure(b->snap, (size_t)2 * nsubw * sizeof(uint64_t)) ||
-      cj_dev_ensure(b->wagg, (size_t)nsubw * sizeof(CJWarpAgg)) ||
-      cj_dev_ensure(b->carry, (size_t)nsubw * sizeof(CJWarpAgg)) ||
-      cj_dev_ensure(b->coef, (size_t)blocks * 128 + 128) || cj_dev_ensure(b->out, (size_t)out_total + 64) ||
-      cj_dev_ensure(b->ctl, sizeof(CJBatchCtl)))
+  if (bt_ensure(b, b->hdr, nd_ * sizeof(CJImageHeader)) || bt_ensure(b, b->desc, nd_ * sizeof(CJImageDesc)) ||
+      bt_ensure(b, b->prm, nd_ * sizeof(CJScanParams)) || bt_ensure(b, b->st, nd_ * sizeof(CJStatus)) ||
+      bt_ensure(b, b->blob, (size_t)blob_bytes + 64) || bt_ensure(b, b->data, (size_t)data_bytes + 64) ||
+      bt_ensure(b, b->tile_keep, (size_t)ntiles * 4) || bt_ensure(b, b->tile_mark, (size_t)ntiles * 4) ||
+      bt_ensure(b, b->mpos, (size_t)nmark * 4) || bt_ensure(b, b->mcode, (size_t)nmark) ||
+      bt_ensure(b, b->segs, (size_t)nseg * sizeof(CJSegment)) ||
+      bt_ensure(b, b->recs, (size_t)nsubw * 32 * sizeof(CJSubRec)) ||
+      bt_ensure(b, b->snap, (size_t)2 * nsubw * sizeof(uint64_t)) ||
+      bt_ensure(b, b->wagg, (size_t)nsubw * sizeof(CJWarpAgg)) ||
+      bt_ensure(b, b->carry, (size_t)nsubw * sizeof(CJWarpAgg)) ||
+      bt_ensure(b, b->coef, (size_t)blocks * 128 + 128) || bt_ensure(b, b->out, (size_t)out_total + 64) ||
+      bt_ensure(b, b->ctl, sizeof(CJBatchCtl)))
     return CUDA_MEM_ERROR;
   if (cj_host_ensure(b->h_st, nd_ * sizeof(CJStatus)) || cj_host_ensure(b->h_ctl, sizeof(CJBatchCtl)))
     return OOM_ERROR;
@@ -920,6 +1009,15 @@ const unsigned char* cjBatchImage(const CJBatch* b, int i, int* w, int* h, int* 
   if (h) *h = b->dims[3 * k + 1];
   if (c) *c = b->dims[3 * k + 2];
   return (const unsigned char*)b->h_out.p + b->outoff[k];
+}
+
+int cjBatchImageGeometry(const CJBatch* b, int i, int* w, int* h, int* c) {
+  if (i < 0 || i >= b->n_in || b->dev_of[i] < 0) return PROGRAMMER_ERROR;
+  int k = b->dev_of[i];
+  if (w) *w = b->dims[3 * k];
+  if (h) *h = b->dims[3 * k + 1];
+  if (c) *c = b->dims[3 * k + 2];
+  return 0;
 }
 
 const unsigned char* cjBatchDeviceImage(const CJBatch* b, int i) {
@@ -1109,7 +1207,7 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   g.hmax = h.hmax;
   g.vmax = h.vmax;
   g.T = d.T;
-  const size_t smem = std::max(cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1]),
+  const size_t smem = std::max(cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1], 2),
                                (size_t)BT_THREADS * sizeof(CJAgg5));
 
   cudaStream_t s = (cudaStream_t)stream;

@@ -77,7 +77,7 @@ CJ_HD uint32_t cj_state_phase(uint64_t s) { return (uint32_t)(s & 0xFF); }
 
 // One speculative subsequence: where its decode started, where it left off,
 // how many blocks it began and the sum of its DC differences per component.
-struct CJSubRec {
+struct alignas(16) CJSubRec {
   uint64_t start;
   uint64_t exit;
   int32_t nblocks;
@@ -85,7 +85,7 @@ struct CJSubRec {
 };
 
 // Per-warp aggregate used by the segmented block/DC scan.
-struct CJWarpAgg {
+struct alignas(16) CJWarpAgg {
   int32_t has_head;  // a segment starts inside this warp
   int32_t nblocks;   // sums over the lanes after the last segment head
   int32_t dc[3];

@@ -53,9 +53,9 @@ __device__ __forceinline__ bool cj_mbar_wait(uint64_t* bar, uint32_t parity) {
 struct CJPixGeom {
   int nch, bpm, mcux, mcuy, width, height;
   int hmax, vmax, xs, ys;
-  int T;                 // MCUs per CTA (one MCU row)
+  int T;                  // MCUs per tile (one MCU row)
   int y_stride, c_stride; // tile plane strides (bytes)
-  int tmp_off, y_off, cb_off, cr_off;
+  int sc1_off, tmp_off, y_off, cb_off, cr_off;
 };
 
 struct CJPixSmemParams {
@@ -83,11 +83,21 @@ CJ_HD int cj_pix_check(const CJScanParams* hp) {
   return 0;
 }
 
-// Shared-memory layout of a tile; returns its size in bytes.
-CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy) {
+// Shared-memory layout of a tile; returns its size in bytes.  With nbuf = 2
+// the two coefficient buffers sit at fixed offsets 0 and 8 KiB (a tile holds
+// at most 64 blocks), so tiles of different geometry -- consecutive tiles of
+// a batch CTA may come from different images -- never overlap the current
+// tile's working space.
+CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy, int nbuf = 1) {
   g->y_stride = g->T * 8 * g->hmax;
   g->c_stride = g->nch == 3 ? g->T * 8 * csx : 0;
-  size_t off = (size_t)g->T * g->bpm * 128;
+  const size_t coef_bytes = (size_t)g->T * g->bpm * 128;
+  size_t off = coef_bytes;
+  g->sc1_off = 0;
+  if (nbuf == 2) {
+    g->sc1_off = 8192;
+    off = 16384;
+  }
   g->tmp_off = (int)off;
   off += (size_t)g->T * g->bpm * 256;
   g->y_off = (int)off;
@@ -101,29 +111,40 @@ CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy) {
   return (off + 15) & ~(size_t)15;
 }
 
-// One tile: MCU row `mrow`, MCUs [mc0, mc0 + T).  `bar` is an initialised
-// mbarrier; `parity` the phase this tile's copy completes.  Returns false if
-// the copy did not land within the wait bound (the error is recorded).
-__device__ __forceinline__ bool cj_pixel_tile(const CJScanParams& prmr, const int16_t* __restrict__ coef,
-                                              uint8_t* __restrict__ out, CJStatus* st,
-                                              const CJPixGeom& g, int mrow, int mc0, uint8_t* smem,
-                                              uint64_t* barp, uint32_t parity, CJPixSmemParams* Pp) {
+// Thread 0: start the TMA bulk copy of tile (mrow, mc0)'s coefficient blocks
+// (contiguous in MCU scan order) into `dst`, completing on `bar`.
+__device__ __forceinline__ void cj_pixel_issue(const int16_t* __restrict__ coef, const CJPixGeom& g,
+                                               int mrow, int mc0, int16_t* dst, uint64_t* bar) {
+  const int nm = min(g.T, g.mcux - mc0);
+  const int16_t* src = coef + ((int64_t)mrow * g.mcux + mc0) * g.bpm * 64;
+  // earlier generic reads of `dst` are ordered before the async-proxy write
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  cj_bulk_load(dst, src, (uint32_t)(nm * g.bpm) * 128u, bar);
+}
+
+__device__ __forceinline__ uint32_t cj_rgb_pack(int yy, int cb, int cr, int k) {
+  // byte k of the pixel's R, G, B (JFIF integer transform, CPUonly/src/pixelTransformCPU.c:152-154)
+  return k == 0 ? cj_clip8((yy + 359 * cr + 128) >> 8)
+                : (k == 1 ? cj_clip8((yy - 88 * cb - 183 * cr + 128) >> 8) : cj_clip8((yy + 454 * cb + 128) >> 8));
+}
+
+// One tile, MCU row `mrow`, MCUs [mc0, mc0 + T), whose coefficients arrive
+// in `sc` on phase `parity` of `bar`: dequantise + integer iDCT into plane
+// tiles, then nearest upsampling + YCbCr->RGB (or a grey copy) into `out`.
+// Returns false if the copy did not land within the wait bound (recorded).
+// Ends with a barrier, so `sc` and the plane tiles are free afterwards.
+__device__ __forceinline__ bool cj_pixel_compute(const CJScanParams& prmr, uint8_t* __restrict__ out,
+                                                 CJStatus* st, const CJPixGeom& g, int mrow, int mc0,
+                                                 const int16_t* sc, uint8_t* smem, uint64_t* barp,
+                                                 uint32_t parity, CJPixSmemParams* Pp) {
   const CJScanParams* prm = &prmr;
   CJPixSmemParams& P = *Pp;
-  uint64_t& bar = *barp;
-  __syncthreads();  // the previous tile is done with shared memory
   const int nm = min(g.T, g.mcux - mc0);
   const int nblk = nm * g.bpm;
-  int16_t* sc = reinterpret_cast<int16_t*>(smem);
   int* tmp = reinterpret_cast<int*>(smem + g.tmp_off);
   uint8_t* py = smem + g.y_off;
   uint8_t* pcb = smem + g.cb_off;
   uint8_t* pcr = smem + g.cr_off;
-
-  if (threadIdx.x == 0) {
-    const int16_t* src = coef + ((int64_t)mrow * g.mcux + mc0) * g.bpm * 64;
-    cj_bulk_load(sc, src, (uint32_t)nblk * 128u, &bar);
-  }
   for (int k = threadIdx.x; k < 4 * 64; k += blockDim.x) P.q[k >> 6][k & 63] = prm->qnat[k >> 6][k & 63];
   if (threadIdx.x < CJ_MAX_BPM) {
     P.pc[threadIdx.x] = prm->phase_comp[threadIdx.x];
@@ -134,7 +155,7 @@ __device__ __forceinline__ bool cj_pixel_tile(const CJScanParams& prmr, const in
     P.csx[threadIdx.x] = prm->comp_sx[threadIdx.x];
     P.csy[threadIdx.x] = prm->comp_sy[threadIdx.x];
   }
-  bool ok = cj_mbar_wait(&bar, parity);
+  bool ok = cj_mbar_wait(barp, parity);
   if (!__syncthreads_and(ok)) {
     if (threadIdx.x == 0) atomicMax(&st->dec_err_key, ~((unsigned long long)CJ_DEV_CAPACITY));
     return false;
@@ -178,23 +199,53 @@ __device__ __forceinline__ bool cj_pixel_tile(const CJScanParams& prmr, const in
   const int X0 = mc0 * 8 * g.hmax, Y0 = mrow * 8 * g.vmax;
   const int w = min(nm * 8 * g.hmax, g.width - X0);
   const int h = min(8 * g.vmax, g.height - Y0);
-  if (w <= 0 || h <= 0) return true;
-  if (g.nch == 3) {
-    for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
-      int y = t / w, x = t - y * w;
-      int yy = py[y * g.y_stride + x] << 8;
-      int ci = (y >> g.ys) * g.c_stride + (x >> g.xs);
-      int cb = (int)pcb[ci] - 128, cr = (int)pcr[ci] - 128;
-      uint8_t* o = out + ((int64_t)(Y0 + y) * g.width + X0 + x) * 3;
-      o[0] = (uint8_t)cj_clip8((yy + 359 * cr + 128) >> 8);
-      o[1] = (uint8_t)cj_clip8((yy - 88 * cb - 183 * cr + 128) >> 8);
-      o[2] = (uint8_t)cj_clip8((yy + 454 * cb + 128) >> 8);
-    }
-  } else {
-    for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
-      int y = t / w, x = t - y * w;
-      out[(int64_t)(Y0 + y) * g.width + X0 + x] = py[y * g.y_stride + x];
+  if (w > 0 && h > 0) {
+    if ((g.width & 7) == 0 && (((uintptr_t)out) & 7) == 0) {
+      // 8 pixels per item: 24 (or 8) bytes, 8-byte aligned stores
+      const int per_row = w >> 3;
+      for (int t = threadIdx.x; t < h * per_row; t += blockDim.x) {
+        int y = t / per_row, x0 = (t - y * per_row) * 8;
+        uint2 yv = *reinterpret_cast<const uint2*>(py + y * g.y_stride + x0);
+        if (g.nch == 3) {
+          uint32_t wds[6] = {0, 0, 0, 0, 0, 0};
+          const uint8_t* crow_b = pcb + (y >> g.ys) * g.c_stride;
+          const uint8_t* crow_r = pcr + (y >> g.ys) * g.c_stride;
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            int yy = (int)(((k < 4 ? yv.x : yv.y) >> (8 * (k & 3))) & 0xFF) << 8;
+            int cb = (int)crow_b[(x0 + k) >> g.xs] - 128, cr = (int)crow_r[(x0 + k) >> g.xs] - 128;
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) {
+              int byte = 3 * k + cc;
+              wds[byte >> 2] |= cj_rgb_pack(yy, cb, cr, cc) << (8 * (byte & 3));
+            }
+          }
+          uint2* o = reinterpret_cast<uint2*>(out + ((int64_t)(Y0 + y) * g.width + X0 + x0) * 3);
+          o[0] = make_uint2(wds[0], wds[1]);
+          o[1] = make_uint2(wds[2], wds[3]);
+          o[2] = make_uint2(wds[4], wds[5]);
+        } else {
+          *reinterpret_cast<uint2*>(out + (int64_t)(Y0 + y) * g.width + X0 + x0) = yv;
+        }
+      }
+    } else if (g.nch == 3) {
+      for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
+        int y = t / w, x = t - y * w;
+        int yy = py[y * g.y_stride + x] << 8;
+        int ci = (y >> g.ys) * g.c_stride + (x >> g.xs);
+        int cb = (int)pcb[ci] - 128, cr = (int)pcr[ci] - 128;
+        uint8_t* o = out + ((int64_t)(Y0 + y) * g.width + X0 + x) * 3;
+        o[0] = (uint8_t)cj_rgb_pack(yy, cb, cr, 0);
+        o[1] = (uint8_t)cj_rgb_pack(yy, cb, cr, 1);
+        o[2] = (uint8_t)cj_rgb_pack(yy, cb, cr, 2);
+      }
+    } else {
+      for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
+        int y = t / w, x = t - y * w;
+        out[(int64_t)(Y0 + y) * g.width + X0 + x] = py[y * g.y_stride + x];
+      }
     }
   }
+  __syncthreads();
   return true;
 }

@@ -28,9 +28,13 @@ k_pixel(const CJScanParams* __restrict__ prm, const int16_t* __restrict__ coef,
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ uint64_t bar;
   __shared__ CJPixSmemParams P;
-  if (threadIdx.x == 0) cj_mbar_init(&bar, 1);
+  if (threadIdx.x == 0) {
+    cj_mbar_init(&bar, 1);
+    cj_pixel_issue(coef, g, blockIdx.y, blockIdx.x * g.T, reinterpret_cast<int16_t*>(smem), &bar);
+  }
   __syncthreads();
-  cj_pixel_tile(*prm, coef, out, st, g, blockIdx.y, blockIdx.x * g.T, smem, &bar, 0, &P);
+  cj_pixel_compute(*prm, out, st, g, blockIdx.y, blockIdx.x * g.T, reinterpret_cast<int16_t*>(smem), smem,
+                   &bar, 0, &P);
 }
 
 // Dequantised int32 coefficients in the reference's per-channel layout

@@ -116,6 +116,9 @@ int cjBatchDecode(CJBatch *b, int n, const unsigned char *blob, const int64_t *o
  * was rejected by the host parse. */
 const unsigned char *cjBatchImage(const CJBatch *b, int i, int *width, int *height, int *channels);
 const unsigned char *cjBatchDeviceImage(const CJBatch *b, int i);
+/* Width, height and channels of image i of the staged batch (known after
+ * cjBatchStage); PROGRAMMER_ERROR if image i was rejected by the host parse. */
+int cjBatchImageGeometry(const CJBatch *b, int i, int *width, int *height, int *channels);
 void *cjBatchStream(const CJBatch *b);
 /* stats[0..10]: images submitted, images on the device, grid CTAs, warp
  * items, destuff tiles, pixel tiles, fix-up passes of the last run, input
@@ -155,6 +158,53 @@ int cjBatchPhaseTimes(const CJBatch *b, float *ms);
  * default stream) before returning 0 or a format.h error code. */
 int cjDecodeNoAlloc(const unsigned char *jpeg, size_t size, unsigned char *d_out,
                     size_t out_capacity, int *width, int *height, int *channels, void *stream);
+
+/* ---- Decode server: continuous batching of single-image requests ----
+ *
+ * No counterpart in the reference (its driver decodes one file per process,
+ * src/main.cu).  Any host thread submits one JPEG per request; a worker
+ * thread groups waiting requests into batches for `engines` batch decoders
+ * (each with its own stream, so one batch's copies and host parse overlap
+ * another's kernel), admitting a request only while the projected device
+ * bytes of all batches in flight stay within `hbm_budget_bytes` (a lone
+ * request is always admitted).  Results stay in the engine's device buffer
+ * until released; an engine is reused once all of its results are released.
+ * Each result is byte-identical to decoding the same file alone. */
+typedef struct CJServer CJServer;
+typedef struct CJServerResult {
+  int error;                           /* format.h code of this request */
+  int width, height, channels;
+  const unsigned char *device_pixels;  /* valid until cjServerRelease */
+  double latency_ms;                   /* submit -> batch finished on the GPU */
+} CJServerResult;
+
+/* engines <= 0: 2; hbm_budget_bytes <= 0: 8 GiB; max_batch_images <= 0: 256.
+ * NULL if no CUDA device is available.  Uses the current device. */
+CJServer *cjServerCreate(int engines, long long hbm_budget_bytes, int max_batch_images);
+void cjServerDestroy(CJServer *s);
+/* Copies the file; returns a ticket >= 0 or a negative value on a fatal
+ * server error. */
+long long cjServerSubmit(CJServer *s, const unsigned char *jpeg, size_t size);
+/* Waits up to timeout_s seconds: 0 = done (result in *out), 1 = still
+ * waiting, else PROGRAMMER_ERROR (unknown ticket). */
+int cjServerWait(CJServer *s, long long ticket, double timeout_s, CJServerResult *out);
+/* Copies a finished request's pixels to host memory. */
+int cjServerCopyOut(CJServer *s, long long ticket, unsigned char *host_dst, size_t capacity);
+/* Ends a finished request; its device pixels may be reused afterwards. */
+void cjServerRelease(CJServer *s, long long ticket);
+/* stats[0..5]: batches launched, images admitted, most batches in flight at
+ * once, largest batch, requests waiting, projected bytes in flight. */
+void cjServerStats(CJServer *s, long long *stats);
+/* Open-loop load replay (for measuring the server): request k is file
+ * k % nfiles of `blob` (offsets/sizes as for cjBatchStage; the blob must stay
+ * valid, it is not copied), submitted at arrival_s[k] seconds after the
+ * start.  A collector thread waits for each request in order, writes
+ * latency_ms[k] (scheduled arrival -> its batch finished on the GPU) and
+ * errors[k] (may be NULL), and releases it.  *wall_s (may be NULL) gets start
+ * -> last completion.  Returns 0 or the server's fatal error. */
+int cjServerReplay(CJServer *s, const unsigned char *blob, const int64_t *offsets,
+                   const int64_t *sizes, int nfiles, const double *arrival_s, int nreq,
+                   double *latency_ms, int *errors, double *wall_s);
 
 #ifdef __cplusplus
 }
