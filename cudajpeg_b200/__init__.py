@@ -301,7 +301,7 @@ class Batch:
     batch of JPEGs of any size / subsampling / restart structure."""
 
     STAT_KEYS = ["submitted", "on_device", "grid", "warp_items", "destuff_tiles", "pixel_tiles",
-                 "passes", "input_bytes", "output_bytes", "smem", "launches"]
+                 "passes", "input_bytes", "output_bytes", "smem", "launches", "pixel_grid"]
 
     def __init__(self, sub_bits: int = 0):
         self.lib = load()
@@ -388,7 +388,7 @@ class Batch:
         return [self.image(i) if not e else None for i, e in enumerate(errs)], errs
 
     def stats(self) -> dict:
-        a = (C.c_int64 * 11)()
+        a = (C.c_int64 * 12)()
         self.lib.cjBatchStats(self.ptr, a)
         return dict(zip(self.STAT_KEYS, [int(v) for v in a]))
 

@@ -1,8 +1,9 @@
 // batch.cu -- persistent, cooperative batch decoder: many JPEGs of uneven
 // size, subsampling and restart structure decoded by ONE kernel launch.
 //
-// The whole decode path of scan.cu + pixel.cu runs as phases of a single
-// cooperative kernel (every CTA co-resident), separated by a grid barrier:
+// The whole decode path of scan.cu + pixel.cu runs as phases 0-8 of a single
+// cooperative kernel (every CTA co-resident), separated by a grid barrier,
+// followed on the same stream by the pixel kernel (phase 9):
 //
 //   0 tables     build each image's canonical Huffman tables and geometry on
 //                the device from its raw DHT/DQT bytes
@@ -14,9 +15,11 @@
 //   7 scan       segmented block / DC prefix over warps
 //   8 write      coefficient write-out
 //   9 pixel      TMA-staged integer iDCT + upsample + colour per MCU tile
+//                (k_pixel_batch, its own launch)
 //
-// Work items are grid-strided, so a warp item is always handled by the same
-// persistent warp in phases 5, 6 and 8.  Data one CTA writes and another
+// Warp items of phases 5, 6 and 8 are handed out through global work
+// counters, so slow items (long synchronisation tails) do not hold up the
+// warps behind them.  Data one CTA writes and another
 // reads inside the kernel is read with L2-coherent loads (__ldcg).  Errors
 // are kept per image: a corrupt image fails alone.
 #include <stdio.h>
@@ -261,15 +264,9 @@ __device__ __forceinline__ uint32_t bt_smem_addr(const void* p) {
 
 __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ uint64_t bar2[2];
   __shared__ int2 sm2[33];
-  __shared__ CJPixSmemParams P;
   unsigned gen = 0;
-  if (threadIdx.x == 0) {
-    gen = atomicAdd(&a.ctl->bar_gen, 0);
-    cj_mbar_init(&bar2[0], 1);
-    cj_mbar_init(&bar2[1], 1);
-  }
+  if (threadIdx.x == 0) gen = atomicAdd(&a.ctl->bar_gen, 0);
   const int lane = threadIdx.x & 31;
 
   bt_stamp(a.ctl, 0);
@@ -580,75 +577,84 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
     cj_write_lane(sp, words, ln, seg, r, b + seg.first_block, dc0, dc1, dc2,
                   a.coef + d.coef0 * 64, st);
   }
-  bt_grid_sync(a.ctl, gen);
+}
 
+// Phase 9 runs as its own kernel, launched right after k_decode_batch on the
+// same stream: the pixel work needs no grid barrier, and on its own it runs
+// at the occupancy of its 32-40 registers per thread instead of the entropy
+// phases' 64.  Pixel tiles, double-buffered: the TMA copy of a CTA's next
+// tile is in flight while it computes the current one.
+__global__ void __launch_bounds__(CJ_PIX_THREADS, 6) k_pixel_batch(CJBatchArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ uint64_t bar2[2];
+  __shared__ CJPixSmemParams P;
+  if (threadIdx.x == 0) {
+    cj_mbar_init(&bar2[0], 1);
+    cj_mbar_init(&bar2[1], 1);
+  }
   bt_stamp(a.ctl, 9);
-  // ---- phase 9: pixel tiles, double-buffered: the TMA copy of a CTA's next
-  // tile is in flight while it computes the current one
-  {
-    int t = blockIdx.x;
-    int buf = 0;
-    uint32_t par[2] = {0, 0};
-    CJPixGeom g;
-    int cur_img = -1;
-    auto geom_of = [&](int tt, int* local, int* img) {
-      int i = bt_find(a.n, tt, [&](int k) { return a.desc[k].ptile0; });
-      const CJImageDesc& d = a.desc[i];
-      const CJScanParams& prm = a.prm[i];
-      CJPixGeom gg;
-      gg.nch = prm.nch;
-      gg.bpm = prm.bpm;
-      gg.mcux = prm.mcux;
-      gg.mcuy = prm.mcuy;
-      gg.width = prm.width;
-      gg.height = prm.height;
-      gg.hmax = prm.hmax;
-      gg.vmax = prm.vmax;
-      gg.xs = prm.xshift;
-      gg.ys = prm.yshift;
-      gg.T = d.T;
-      cj_pix_layout(&gg, prm.comp_sx[1], prm.comp_sy[1], 2);
-      *local = tt - d.ptile0;
-      *img = i;
-      return gg;
-    };
-    int local = 0;
-    if (t < a.nptiles) {
-      g = geom_of(t, &local, &cur_img);
-      if (threadIdx.x == 0) {
-        const int gx = (g.mcux + g.T - 1) / g.T;
-        cj_pixel_issue(a.coef + a.desc[cur_img].coef0 * 64, g, local / gx, (local % gx) * g.T,
-                       reinterpret_cast<int16_t*>(smem), &bar2[0]);
-      }
+  __syncthreads();
+  // Each CTA takes a contiguous run of tiles, so consecutive tiles mostly
+  // belong to one image: the image index only ever moves forward and the
+  // tile geometry is rebuilt only when it changes.
+  const int per = (a.nptiles + gridDim.x - 1) / gridDim.x;
+  const int t0 = blockIdx.x * per, t1 = min(t0 + per, a.nptiles);
+  auto advance = [&](int tt, int i) {
+    while (tt >= a.desc[i].ptile0 + a.desc[i].nptiles) i++;
+    return i;
+  };
+  auto geom_of = [&](int i) {
+    const CJScanParams& prm = a.prm[i];
+    CJPixGeom gg;
+    gg.nch = prm.nch;
+    gg.bpm = prm.bpm;
+    gg.mcux = prm.mcux;
+    gg.mcuy = prm.mcuy;
+    gg.width = prm.width;
+    gg.height = prm.height;
+    gg.hmax = prm.hmax;
+    gg.vmax = prm.vmax;
+    gg.xs = prm.xshift;
+    gg.ys = prm.yshift;
+    gg.T = a.desc[i].T;
+    cj_pix_layout(&gg, prm.comp_sx[1], prm.comp_sy[1], 2);
+    return gg;
+  };
+  // thread 0 issues each tile's copy one tile ahead of the compute
+  auto issue = [&](int tt, int i, int which) {
+    const CJPixGeom gg = geom_of(i);
+    const int local = tt - a.desc[i].ptile0, gx = (gg.mcux + gg.T - 1) / gg.T;
+    cj_pixel_issue(a.coef + a.desc[i].coef0 * 64, gg, local / gx, (local % gx) * gg.T,
+                   reinterpret_cast<int16_t*>(smem + which * gg.sc1_off), &bar2[which]);
+  };
+  if (t0 >= t1) return;
+  int img = bt_find(a.n, t0, [&](int k) { return a.desc[k].ptile0; });
+  int pimg = img;  // image of the tile being prefetched (thread 0)
+  if (threadIdx.x == 0) issue(t0, img, 0);
+  CJPixGeom g = geom_of(img);
+  int gimg = img;
+  int buf = 0;
+  uint32_t par[2] = {0, 0};
+  for (int t = t0; t < t1; t++) {
+    if (t + 1 < t1 && threadIdx.x == 0) {
+      pimg = advance(t + 1, pimg);
+      issue(t + 1, pimg, buf ^ 1);
     }
-    while (t < a.nptiles) {
-      const int nt = t + gridDim.x;
-      int nlocal = 0, nimg = -1;
-      CJPixGeom ng;
-      if (nt < a.nptiles) {
-        ng = geom_of(nt, &nlocal, &nimg);
-        if (threadIdx.x == 0) {
-          const int ngx = (ng.mcux + ng.T - 1) / ng.T;
-          int16_t* dst = reinterpret_cast<int16_t*>(smem + (buf ^ 1) * ng.sc1_off);
-          cj_pixel_issue(a.coef + a.desc[nimg].coef0 * 64, ng, nlocal / ngx, (nlocal % ngx) * ng.T, dst,
-                         &bar2[buf ^ 1]);
-        }
-      }
-      const int gx = (g.mcux + g.T - 1) / g.T;
-      const CJImageDesc& d = a.desc[cur_img];
-      const int16_t* sc = reinterpret_cast<const int16_t*>(smem + buf * g.sc1_off);
-      if (!cj_pixel_compute(a.prm[cur_img], a.out + d.out_off, &a.st[cur_img], g, local / gx,
-                            (local % gx) * g.T, sc, smem, &bar2[buf], par[buf], &P)) {
-        if (nt < a.nptiles) cj_mbar_wait(&bar2[buf ^ 1], par[buf ^ 1]);  // the prefetch in flight
-        break;
-      }
-      par[buf] ^= 1;
-      buf ^= 1;
-      t = nt;
-      g = ng;
-      local = nlocal;
-      cur_img = nimg;
+    img = advance(t, img);
+    if (img != gimg) {
+      g = geom_of(img);
+      gimg = img;
     }
+    const CJImageDesc& d = a.desc[img];
+    const int local = t - d.ptile0, gx = (g.mcux + g.T - 1) / g.T;
+    const int16_t* sc = reinterpret_cast<const int16_t*>(smem + buf * g.sc1_off);
+    if (!cj_pixel_compute(a.prm[img], a.out + d.out_off, &a.st[img], g, local / gx, (local % gx) * g.T, sc,
+                          smem, &bar2[buf], par[buf], &P)) {
+      if (t + 1 < t1) cj_mbar_wait(&bar2[buf ^ 1], par[buf ^ 1]);  // the prefetch in flight
+      break;
+    }
+    par[buf] ^= 1;
+    buf ^= 1;
   }
 }
 
@@ -674,8 +680,8 @@ struct CJBatch {
   std::vector<int64_t> outoff; // output offset per device slot
   int ntiles = 0, nwarps = 0, nptiles = 0;
   int64_t blob_bytes = 0, out_total = 0;
-  size_t smem = 0;
-  int grid = 0;
+  size_t smem = 0, smem_pix = 0;
+  int grid = 0, grid_pix = 0;
   long long launches = 0;
 };
 
@@ -718,6 +724,8 @@ static int bt_init(CJBatch* b) {
   CJ_CUDA_TRY(cudaEventCreate(&b->ev0), CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaEventCreate(&b->ev1), CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaFuncSetAttribute(k_decode_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
+              CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaFuncSetAttribute(k_pixel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
               CUDA_MEM_ERROR);
   b->parser = newJPGReader();
   if (!b->parser) return OOM_ERROR;
@@ -825,7 +833,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   CJImageDesc* dd = (CJImageDesc*)b->h_desc.p;
   int nd = 0, ntiles = 0, nsubw = 0, nptiles = 0, nmark = 0, nseg = 0;
   int64_t data_bytes = 0, blocks = 0, out_total = 0;
-  size_t smem = 8192;
+  size_t smem = 0;
   for (int i = 0; i < n; i++) {
     int64_t so = 0, sl = 0;
     int e = bt_parse(b, blob + offsets[i], (size_t)sizes[i], &hh[nd], &so, &sl);
@@ -887,7 +895,8 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   b->nptiles = nptiles;
   b->blob_bytes = blob_bytes;
   b->out_total = out_total;
-  b->smem = std::max(smem, (size_t)BT_THREADS * sizeof(CJAgg5));
+  b->smem = (size_t)BT_THREADS * sizeof(CJAgg5);
+  b->smem_pix = smem;
   if (!nd) return 0;
   size_t nd_ = (size_t)nd;
   if (bt_ensure(b, b->hdr, nd_ * sizeof(CJImageHeader)) || bt_ensure(b, b->desc, nd_ * sizeof(CJImageDesc)) ||
@@ -917,6 +926,10 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
               CUDA_KERNEL_LAUNCH_ERROR);
   if (per_sm < 1) return UNSUPPORTED_ERROR;
   b->grid = per_sm * b->sm_count;
+  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pixel_batch, CJ_PIX_THREADS, b->smem_pix),
+              CUDA_KERNEL_LAUNCH_ERROR);
+  if (per_sm < 1) return UNSUPPORTED_ERROR;
+  b->grid_pix = std::min(nptiles, per_sm * b->sm_count);
   return 0;
 }
 
@@ -956,6 +969,11 @@ int cjBatchRun(CJBatch* b) {
                                           b->smem, s),
               CUDA_KERNEL_LAUNCH_ERROR);
   b->launches++;
+  if (b->grid_pix > 0) {
+    k_pixel_batch<<<b->grid_pix, CJ_PIX_THREADS, b->smem_pix, s>>>(a);
+    CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
+    b->launches++;
+  }
   CJ_CUDA_TRY(cudaEventRecord(b->ev1, s), CUDA_KERNEL_LAUNCH_ERROR);
   return 0;
 }
@@ -1049,8 +1067,9 @@ void cjBatchStats(const CJBatch* b, int64_t* s) {
   s[6] = ctl ? ctl->passes : 0;
   s[7] = b->blob_bytes;
   s[8] = b->out_total;
-  s[9] = (int64_t)b->smem;
+  s[9] = (int64_t)b->smem_pix;
   s[10] = b->launches;
+  s[11] = b->grid_pix;
 }
 
 float cjBatchKernelMs(const CJBatch* b) {
@@ -1095,6 +1114,8 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
       return CUDA_MEM_ERROR;
     }
     CJ_CUDA_TRY(cudaFuncSetAttribute(k_decode_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
+                CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaFuncSetAttribute(k_pixel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
                 CUDA_MEM_ERROR);
     g_noalloc_ptr[dev] = (unsigned char*)p;
   }
@@ -1207,8 +1228,8 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   g.hmax = h.hmax;
   g.vmax = h.vmax;
   g.T = d.T;
-  const size_t smem = std::max(cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1], 2),
-                               (size_t)BT_THREADS * sizeof(CJAgg5));
+  const size_t smem_pix = cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1], 2);
+  const size_t smem = (size_t)BT_THREADS * sizeof(CJAgg5);
 
   cudaStream_t s = (cudaStream_t)stream;
   CJ_CUDA_TRY(cudaMemcpyAsync(base + o_hdr, &h, sizeof(h), cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
@@ -1249,6 +1270,11 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   CJ_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_decode_batch, dim3(per_sm * sms), dim3(BT_THREADS), args,
                                           smem, s),
               CUDA_KERNEL_LAUNCH_ERROR);
+  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pixel_batch, CJ_PIX_THREADS, smem_pix),
+              CUDA_KERNEL_LAUNCH_ERROR);
+  if (per_sm < 1) return UNSUPPORTED_ERROR;
+  k_pixel_batch<<<std::min(d.nptiles, per_sm * sms), CJ_PIX_THREADS, smem_pix, s>>>(a);
+  CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
   CJStatus st;
   CJBatchCtl ctl;
   CJ_CUDA_TRY(cudaMemcpyAsync(&st, base + o_st, sizeof(st), cudaMemcpyDeviceToHost, s), CUDA_MEM_ERROR);

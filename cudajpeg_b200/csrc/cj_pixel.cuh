@@ -55,13 +55,19 @@ struct CJPixGeom {
   int hmax, vmax, xs, ys;
   int T;                  // MCUs per tile (one MCU row)
   int y_stride, c_stride; // tile plane strides (bytes)
+  int ipr_shift;          // log2 of 8-pixel items per tile row (T * hmax)
   int sc1_off, tmp_off, y_off, cb_off, cr_off;
 };
 
-struct CJPixSmemParams {
-  int16_t q[4][64];
-  uint8_t pc[CJ_MAX_BPM], pb[CJ_MAX_BPM];
-  uint8_t cq[4], csx[4], csy[4];
+// Row-pass results of one block: 8 rows of 8 int32, padded to 72 words so
+// that the column pass (lanes = 4 blocks x 8 columns) reads 32 distinct banks.
+#define CJ_TMP_STRIDE 72
+
+struct alignas(16) CJPixSmemParams {
+  int16_t q[4][64];       // dequantisation tables, natural order
+  uint16_t boff[64];      // per block of the tile: smem offset of its 8x8 destination
+  uint8_t bc[64];         // per block of the tile: component
+  uint8_t bq[64];         // per block of the tile: quantisation table
 };
 
 // MCUs per tile: 128 output pixels across, at most 64 blocks of coefficients.
@@ -91,6 +97,8 @@ CJ_HD int cj_pix_check(const CJScanParams* hp) {
 CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy, int nbuf = 1) {
   g->y_stride = g->T * 8 * g->hmax;
   g->c_stride = g->nch == 3 ? g->T * 8 * csx : 0;
+  g->ipr_shift = 0;
+  while ((1 << g->ipr_shift) < g->T * g->hmax) g->ipr_shift++;
   const size_t coef_bytes = (size_t)g->T * g->bpm * 128;
   size_t off = coef_bytes;
   g->sc1_off = 0;
@@ -99,7 +107,7 @@ CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy, int nbuf = 1) {
     off = 16384;
   }
   g->tmp_off = (int)off;
-  off += (size_t)g->T * g->bpm * 256;
+  off += (size_t)g->T * g->bpm * CJ_TMP_STRIDE * 4;
   g->y_off = (int)off;
   off += (size_t)g->y_stride * 8 * g->vmax;
   off = (off + 15) & ~(size_t)15;
@@ -128,6 +136,34 @@ __device__ __forceinline__ uint32_t cj_rgb_pack(int yy, int cb, int cr, int k) {
                 : (k == 1 ? cj_clip8((yy - 88 * cb - 183 * cr + 128) >> 8) : cj_clip8((yy + 454 * cb + 128) >> 8));
 }
 
+// The same transform split per chroma sample: with yy = Y << 8 a multiple of
+// 256, (yy + t) >> 8 == Y + (t >> 8) for every t (arithmetic shift = floor),
+// so R = clip(Y + dR) etc. with the d terms computed once per chroma sample
+// and shared by the 1, 2 or 4 pixels it covers.
+struct CJChromaTerms {
+  int r, g, b;
+};
+__device__ __forceinline__ CJChromaTerms cj_chroma_terms(int cb_byte, int cr_byte) {
+  const int cb = cb_byte - 128, cr = cr_byte - 128;
+  return {(359 * cr + 128) >> 8, (-88 * cb - 183 * cr + 128) >> 8, (454 * cb + 128) >> 8};
+}
+
+// 8 pixels of one row (Y bytes in yv) -> 24 RGB bytes in six words.
+__device__ __forceinline__ void cj_rgb8(uint2 yv, const CJChromaTerms* d, int dshift, uint32_t* wds) {
+  uint32_t bytes[24];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const int Y = (int)(((k < 4 ? yv.x : yv.y) >> (8 * (k & 3))) & 0xFF);
+    const CJChromaTerms t = d[k >> dshift];
+    bytes[3 * k] = cj_clip8(Y + t.r);
+    bytes[3 * k + 1] = cj_clip8(Y + t.g);
+    bytes[3 * k + 2] = cj_clip8(Y + t.b);
+  }
+#pragma unroll
+  for (int w = 0; w < 6; w++)
+    wds[w] = bytes[4 * w] | (bytes[4 * w + 1] << 8) | (bytes[4 * w + 2] << 16) | (bytes[4 * w + 3] << 24);
+}
+
 // One tile, MCU row `mrow`, MCUs [mc0, mc0 + T), whose coefficients arrive
 // in `sc` on phase `parity` of `bar`: dequantise + integer iDCT into plane
 // tiles, then nearest upsampling + YCbCr->RGB (or a grey copy) into `out`.
@@ -146,14 +182,16 @@ __device__ __forceinline__ bool cj_pixel_compute(const CJScanParams& prmr, uint8
   uint8_t* pcb = smem + g.cb_off;
   uint8_t* pcr = smem + g.cr_off;
   for (int k = threadIdx.x; k < 4 * 64; k += blockDim.x) P.q[k >> 6][k & 63] = prm->qnat[k >> 6][k & 63];
-  if (threadIdx.x < CJ_MAX_BPM) {
-    P.pc[threadIdx.x] = prm->phase_comp[threadIdx.x];
-    P.pb[threadIdx.x] = prm->phase_blk[threadIdx.x];
-  }
-  if (threadIdx.x < 3) {
-    P.cq[threadIdx.x] = prm->comp_q[threadIdx.x];
-    P.csx[threadIdx.x] = prm->comp_sx[threadIdx.x];
-    P.csy[threadIdx.x] = prm->comp_sy[threadIdx.x];
+  // per-block destination table (one division per block, not per row)
+  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
+    const int mi = k / g.bpm, ph = k - mi * g.bpm;
+    const int c = prm->phase_comp[ph], bl = prm->phase_blk[ph], sxc = prm->comp_sx[c];
+    const int bx = mi * sxc + bl % sxc, by = bl / sxc;
+    const int base = c == 0 ? g.y_off : (c == 1 ? g.cb_off : g.cr_off);
+    const int ps = c == 0 ? g.y_stride : g.c_stride;
+    P.boff[k] = (uint16_t)(base + by * 8 * ps + bx * 8);
+    P.bc[k] = (uint8_t)c;
+    P.bq[k] = prm->comp_q[c];
   }
   bool ok = cj_mbar_wait(barp, parity);
   if (!__syncthreads_and(ok)) {
@@ -163,14 +201,14 @@ __device__ __forceinline__ bool cj_pixel_compute(const CJScanParams& prmr, uint8
 
   // Row pass: one thread per (block, row); dequantise on load.
   for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
-    int k = t >> 3, r = t & 7;
-    int c = P.pc[k % g.bpm];
-    const int16_t* q = &P.q[P.cq[c]][r * 8];
+    const int k = t >> 3, r = t & 7;
+    const uint4 qv = *reinterpret_cast<const uint4*>(&P.q[P.bq[k]][r * 8]);
+    const int16_t* q = reinterpret_cast<const int16_t*>(&qv);
     uint4 raw = *reinterpret_cast<const uint4*>(sc + k * 64 + r * 8);
     int v[8];
     cj_unpack_dequant(raw, q, v);
     cj_idct_row(v);
-    int4* o = reinterpret_cast<int4*>(tmp + k * 64 + r * 8);
+    int4* o = reinterpret_cast<int4*>(tmp + k * CJ_TMP_STRIDE + r * 8);
     o[0] = make_int4(v[0], v[1], v[2], v[3]);
     o[1] = make_int4(v[4], v[5], v[6], v[7]);
   }
@@ -178,18 +216,14 @@ __device__ __forceinline__ bool cj_pixel_compute(const CJScanParams& prmr, uint8
 
   // Column pass: one thread per (block, column); 8 samples into the plane tile.
   for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
-    int k = t >> 3, col = t & 7;
+    const int k = t >> 3, col = t & 7;
     int d[8];
 #pragma unroll
-    for (int j = 0; j < 8; j++) d[j] = tmp[k * 64 + j * 8 + col];
+    for (int j = 0; j < 8; j++) d[j] = tmp[k * CJ_TMP_STRIDE + j * 8 + col];
     uint32_t o[8];
     cj_idct_col(d, o);
-    int mi = k / g.bpm, ph = k - mi * g.bpm;
-    int c = P.pc[ph], bl = P.pb[ph], sxc = P.csx[c];
-    int bx = mi * sxc + bl % sxc, by = bl / sxc;
-    uint8_t* plane = c == 0 ? py : (c == 1 ? pcb : pcr);
-    int ps = c == 0 ? g.y_stride : g.c_stride;
-    uint8_t* dst = plane + (by * 8) * ps + bx * 8 + col;
+    const int ps = P.bc[k] == 0 ? g.y_stride : g.c_stride;
+    uint8_t* dst = smem + P.boff[k] + col;
 #pragma unroll
     for (int j = 0; j < 8; j++) dst[j * ps] = (uint8_t)o[j];
   }
@@ -201,25 +235,41 @@ __device__ __forceinline__ bool cj_pixel_compute(const CJScanParams& prmr, uint8
   const int h = min(8 * g.vmax, g.height - Y0);
   if (w > 0 && h > 0) {
     if ((g.width & 7) == 0 && (((uintptr_t)out) & 7) == 0) {
-      // 8 pixels per item: 24 (or 8) bytes, 8-byte aligned stores
-      const int per_row = w >> 3;
-      for (int t = threadIdx.x; t < h * per_row; t += blockDim.x) {
-        int y = t / per_row, x0 = (t - y * per_row) * 8;
-        uint2 yv = *reinterpret_cast<const uint2*>(py + y * g.y_stride + x0);
+      // 8 pixels per item, items laid out (row, 8-pixel column) with a
+      // power-of-two number of items per tile row; 8-byte aligned stores
+      const int ipr = 1 << g.ipr_shift, per_row = w >> 3;
+      for (int t = threadIdx.x; t < (h << g.ipr_shift); t += blockDim.x) {
+        const int y = t >> g.ipr_shift, xi = t & (ipr - 1);
+        if (xi >= per_row) continue;
+        const int x0 = xi * 8;
+        const uint2 yv = *reinterpret_cast<const uint2*>(py + y * g.y_stride + x0);
         if (g.nch == 3) {
-          uint32_t wds[6] = {0, 0, 0, 0, 0, 0};
           const uint8_t* crow_b = pcb + (y >> g.ys) * g.c_stride;
           const uint8_t* crow_r = pcr + (y >> g.ys) * g.c_stride;
+          CJChromaTerms d[8];
+          int dshift;
+          if (g.xs == 1) {  // 4 chroma samples, 4-byte aligned (x0 / 2 is a multiple of 4)
+            const uint32_t b4 = *reinterpret_cast<const uint32_t*>(crow_b + (x0 >> 1));
+            const uint32_t r4 = *reinterpret_cast<const uint32_t*>(crow_r + (x0 >> 1));
 #pragma unroll
-          for (int k = 0; k < 8; k++) {
-            int yy = (int)(((k < 4 ? yv.x : yv.y) >> (8 * (k & 3))) & 0xFF) << 8;
-            int cb = (int)crow_b[(x0 + k) >> g.xs] - 128, cr = (int)crow_r[(x0 + k) >> g.xs] - 128;
+            for (int j = 0; j < 4; j++) d[j] = cj_chroma_terms((b4 >> (8 * j)) & 0xFF, (r4 >> (8 * j)) & 0xFF);
+            dshift = 1;
+          } else if (g.xs == 0) {  // 8 chroma samples, 8-byte aligned
+            const uint2 b8 = *reinterpret_cast<const uint2*>(crow_b + x0);
+            const uint2 r8 = *reinterpret_cast<const uint2*>(crow_r + x0);
 #pragma unroll
-            for (int cc = 0; cc < 3; cc++) {
-              int byte = 3 * k + cc;
-              wds[byte >> 2] |= cj_rgb_pack(yy, cb, cr, cc) << (8 * (byte & 3));
-            }
+            for (int j = 0; j < 8; j++)
+              d[j] = cj_chroma_terms(((j < 4 ? b8.x : b8.y) >> (8 * (j & 3))) & 0xFF,
+                                     ((j < 4 ? r8.x : r8.y) >> (8 * (j & 3))) & 0xFF);
+            dshift = 0;
+          } else {  // wider chroma subsampling: per pixel
+#pragma unroll
+            for (int j = 0; j < 8; j++) d[j] = cj_chroma_terms(crow_b[(x0 + j) >> g.xs], crow_r[(x0 + j) >> g.xs]);
+            dshift = 0;
           }
+          uint32_t wds[6];
+          if (dshift) cj_rgb8(yv, d, 1, wds);
+          else cj_rgb8(yv, d, 0, wds);
           uint2* o = reinterpret_cast<uint2*>(out + ((int64_t)(Y0 + y) * g.width + X0 + x0) * 3);
           o[0] = make_uint2(wds[0], wds[1]);
           o[1] = make_uint2(wds[2], wds[3]);

@@ -120,9 +120,10 @@ const unsigned char *cjBatchDeviceImage(const CJBatch *b, int i);
  * cjBatchStage); PROGRAMMER_ERROR if image i was rejected by the host parse. */
 int cjBatchImageGeometry(const CJBatch *b, int i, int *width, int *height, int *channels);
 void *cjBatchStream(const CJBatch *b);
-/* stats[0..10]: images submitted, images on the device, grid CTAs, warp
- * items, destuff tiles, pixel tiles, fix-up passes of the last run, input
- * bytes, output bytes, dynamic shared memory, kernel launches so far. */
+/* stats[0..11]: images submitted, images on the device, decode-kernel CTAs,
+ * warp items, destuff tiles, pixel tiles, fix-up passes of the last run,
+ * input bytes, output bytes, pixel-kernel dynamic shared memory, kernel
+ * launches so far, pixel-kernel CTAs. */
 void cjBatchStats(const CJBatch *b, int64_t *stats);
 /* Device time of the last cjBatchRun, in milliseconds. */
 float cjBatchKernelMs(const CJBatch *b);
