@@ -78,6 +78,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default batch tuning")
     ap.add_argument("--serve-seconds", type=float, default=1.5,
                     help="seconds of arrivals per rate for the serving measurement (0: skip)")
     return ap.parse_args()
@@ -309,7 +310,8 @@ def serving_value(wl, seconds: float) -> dict:
     from cudajpeg_b200 import serve as sv
     px = np.array([s.pixels for s in wl.samples], np.float64)
     out = {"how": f"cjServerReplay, {seconds:g} s of Poisson arrivals per rate over the "
-                  f"{len(wl.files)} workload files (cycled), 3 engines, 8 GiB budget",
+                  f"{len(wl.files)} workload files (cycled), 3 engines, 8 GiB budget, server "
+                  "default tuning (512-bit subsequences)",
            "rates": []}
     with sv.Server(engines=3, hbm_budget_bytes=8 << 30, max_batch=256) as s:
         # warm-up: bursts of the largest files grow every engine's buffers to
@@ -345,6 +347,12 @@ def run_batch(args, wl, world, rank, local, dist):
     errs = b.wait()
     if any(errs):
         raise RuntimeError(f"batch decode errors: {sum(1 for e in errs if e)}")
+    # untimed: the autotuner picks subsequence size, decode-kernel occupancy
+    # and pixel tile width for this batch (cjBatchAutotune)
+    tune = b.autotune(src.data_ptr(), offsets, sizes, reps=3) if not args.no_autotune else b.tuning()
+    b.run()
+    if any(b.wait()):
+        raise RuntimeError("batch decode errors under the tuned configuration")
     ext = torch.cuda.ExternalStream(b.stream())
     for _ in range(args.warmup):
         b.run()
@@ -412,7 +420,13 @@ def run_batch(args, wl, world, rank, local, dist):
                            l2="working set ~1.6 GB per step, larger than L2 (126 MB)",
                            compressed_MB_per_s=round(world * wl.file_bytes * args.steps
                                                      / (total_ms / 1e3) / 1e6, 1),
-                           passes=st["passes"], grid_ctas=st["grid"], warp_items=st["warp_items"]),
+                           passes=st["passes"], grid_ctas=st["grid"], warp_items=st["warp_items"],
+                           pixel_ctas=st["pixel_grid"],
+                           tuning={k: tune[k] for k in ("sub_bits", "decode_ctas_per_sm", "pixel_tile_cap")},
+                           autotune=({"best_ms": tune["best_ms"], "trials_ms": tune["trials_ms"],
+                                      "order": "sub_bits {512,1024,2048,4096} x ctas {3,4,5}, "
+                                               "then tile cap {8,4,2}"}
+                                     if "best_ms" in tune else None)),
             "e2e": {"value": round(e2e_value, 2), "unit": "MPix/s",
                     "h2d_bytes_per_step": int(st["input_bytes"]),
                     "d2h_bytes_per_step": int(st["output_bytes"]),

@@ -50,7 +50,8 @@ EXPORTED = [
     "cjBatchStream", "cjBatchStats", "cjBatchKernelMs", "cjBatchPhaseTimes",
     "cjDecodeNoAlloc", "cjBatchImageGeometry",
     "cjServerCreate", "cjServerDestroy", "cjServerSubmit", "cjServerWait", "cjServerCopyOut",
-    "cjServerRelease", "cjServerStats", "cjServerReplay",
+    "cjServerRelease", "cjServerStats", "cjServerReplay", "cjServerSetTuning",
+    "cjBatchSetTuning", "cjBatchGetTuning", "cjBatchAutotune",
 ]
 
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
@@ -135,6 +136,11 @@ def load(build_if_missing: bool = True):
     ip = C.POINTER(C.c_int)
     lib.cjDecodeNoAlloc.argtypes = [vp, C.c_size_t, vp, C.c_size_t, ip, ip, ip, vp]
     lib.cjBatchImageGeometry.argtypes = [vp, C.c_int, ip, ip, ip]
+    lib.cjBatchSetTuning.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+    lib.cjBatchGetTuning.argtypes = [vp, ip, ip, ip]
+    lib.cjBatchAutotune.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float), C.c_int]
+    lib.cjServerSetTuning.argtypes = [vp, C.c_int, C.c_int, C.c_int]
     lib.cjServerCreate.restype = vp
     lib.cjServerCreate.argtypes = [C.c_int, C.c_longlong, C.c_int]
     lib.cjServerDestroy.argtypes = [vp]
@@ -301,7 +307,8 @@ class Batch:
     batch of JPEGs of any size / subsampling / restart structure."""
 
     STAT_KEYS = ["submitted", "on_device", "grid", "warp_items", "destuff_tiles", "pixel_tiles",
-                 "passes", "input_bytes", "output_bytes", "smem", "launches", "pixel_grid"]
+                 "passes", "input_bytes", "output_bytes", "smem", "launches", "pixel_grid",
+                 "graph_runs", "graph_failures"]
 
     def __init__(self, sub_bits: int = 0):
         self.lib = load()
@@ -388,7 +395,7 @@ class Batch:
         return [self.image(i) if not e else None for i, e in enumerate(errs)], errs
 
     def stats(self) -> dict:
-        a = (C.c_int64 * 12)()
+        a = (C.c_int64 * 14)()
         self.lib.cjBatchStats(self.ptr, a)
         return dict(zip(self.STAT_KEYS, [int(v) for v in a]))
 
@@ -402,6 +409,34 @@ class Batch:
 
     def stream(self) -> int:
         return self.lib.cjBatchStream(self.ptr)
+
+    def set_tuning(self, sub_bits: int = 0, decode_ctas_per_sm: int = 0, pixel_tile_cap: int = 0):
+        err = self.lib.cjBatchSetTuning(self.ptr, sub_bits, decode_ctas_per_sm, pixel_tile_cap)
+        if err:
+            raise ValueError(f"bad tuning {(sub_bits, decode_ctas_per_sm, pixel_tile_cap)}")
+
+    def tuning(self) -> dict:
+        a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
+        self.lib.cjBatchGetTuning(self.ptr, C.byref(a), C.byref(b), C.byref(c))
+        return {"sub_bits": a.value, "decode_ctas_per_sm": b.value, "pixel_tile_cap": c.value}
+
+    def autotune(self, blob_ptr: int, offsets: np.ndarray, sizes: np.ndarray, reps: int = 3) -> dict:
+        """Time the batch under every candidate tuning (cjBatchAutotune) and
+        keep the fastest; the batch is left staged under it."""
+        offsets = np.ascontiguousarray(offsets, np.int64)
+        sizes = np.ascontiguousarray(sizes, np.int64)
+        self._keep = (offsets, sizes)
+        self.n = len(sizes)
+        best = C.c_float(0.0)
+        trials = (C.c_float * 32)()
+        err = self.lib.cjBatchAutotune(self.ptr, self.n, C.c_void_p(blob_ptr), offsets.ctypes.data,
+                                       sizes.ctypes.data, reps, C.byref(best), trials, 32)
+        if err:
+            raise DecodeError(err, "cjBatchAutotune")
+        out = self.tuning()
+        out["best_ms"] = round(best.value, 4)
+        out["trials_ms"] = [round(trials[k], 4) for k in range(15)]
+        return out
 
 
 # ---- JPGReader field access for the few fields ctypes needs (layout of

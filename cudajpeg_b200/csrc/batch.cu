@@ -183,6 +183,8 @@ __device__ __forceinline__ int bt_find(int n, int v, F key) {
   return lo;
 }
 
+__constant__ uint8_t c_bt_zz[64] = CJ_ZIGZAG_INIT;  // zig-zag -> natural index
+
 // Phase 0: one CTA builds one image's CJScanParams (the device twin of
 // cj_build_huff + cj_fill_params).
 __device__ void bt_build_params(const CJImageHeader& h, CJScanParams& p) {
@@ -221,9 +223,8 @@ __device__ void bt_build_params(const CJImageHeader& h, CJScanParams& p) {
     p.huff[slot].maxcode[17] = -1;
     p.huff[slot].valoff[17] = 0;
   }
-  const uint8_t zz[64] = CJ_ZIGZAG_INIT;
-  for (int e = threadIdx.x; e < 4 * 64; e += blockDim.x) p.qnat[e >> 6][zz[e & 63]] = h.dq[e >> 6][e & 63];
-  if (threadIdx.x < 64) p.zz[threadIdx.x] = zz[threadIdx.x];
+  for (int e = threadIdx.x; e < 4 * 64; e += blockDim.x) p.qnat[e >> 6][c_bt_zz[e & 63]] = h.dq[e >> 6][e & 63];
+  if (threadIdx.x < 64) p.zz[threadIdx.x] = c_bt_zz[threadIdx.x];
   if (threadIdx.x == 0) {
     int k = 0;
     for (int c = 0; c < h.nch; c++)
@@ -262,11 +263,16 @@ __device__ __forceinline__ uint32_t bt_smem_addr(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
+// MINB = CTAs per SM the register allocation is sized for (64 registers at
+// 4); the autotuner picks among the compiled variants.
+template <int MINB>
+__global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ int2 sm2[33];
+  __shared__ uint8_t s_zz[64];
   unsigned gen = 0;
   if (threadIdx.x == 0) gen = atomicAdd(&a.ctl->bar_gen, 0);
+  if (threadIdx.x < 64) s_zz[threadIdx.x] = c_bt_zz[threadIdx.x];
   const int lane = threadIdx.x & 31;
 
   bt_stamp(a.ctl, 0);
@@ -575,7 +581,17 @@ __global__ void __launch_bounds__(BT_THREADS) k_decode_batch(CJBatchArgs a) {
     if (!ln.active) continue;
     const CJSegment seg = a.segs[d.seg0 + ln.seg];
     cj_write_lane(sp, words, ln, seg, r, b + seg.first_block, dc0, dc1, dc2,
-                  a.coef + d.coef0 * 64, st);
+                  a.coef + d.coef0 * 64, st, s_zz);
+  }
+}
+
+typedef void (*bt_decode_fn)(CJBatchArgs);
+#define BT_DECODE_CTAS_DEFAULT 4
+static bt_decode_fn bt_decode_kernel(int ctas_per_sm) {
+  switch (ctas_per_sm) {
+    case 3: return k_decode_batch<3>;
+    case 5: return k_decode_batch<5>;
+    default: return k_decode_batch<4>;
   }
 }
 
@@ -665,7 +681,10 @@ struct CJBatch {
   int device = 0, sm_count = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // tuning (cjBatchSetTuning / cjBatchAutotune)
   int sub_bits = CJ_SUB_BITS_DEFAULT;
+  int decode_ctas = BT_DECODE_CTAS_DEFAULT;  // decode-kernel CTAs per SM (3, 4 or 5)
+  int tile_cap = 0;                          // max MCUs per pixel tile (0 = layout maximum)
   JPGReader* parser = nullptr;  // host marker parse, one image at a time
   // device buffers (grow-only)
   CJDevBuf hdr, desc, prm, st, blob, data, tile_keep, tile_mark, mpos, mcode, segs, recs, snap,
@@ -683,6 +702,10 @@ struct CJBatch {
   size_t smem = 0, smem_pix = 0;
   int grid = 0, grid_pix = 0;
   long long launches = 0;
+  // the run as a CUDA graph (rebuilt after each stage)
+  bool use_graph = true, graph_stale = true;
+  cudaGraphExec_t gexec = nullptr;
+  long long graph_launches = 0, graph_failures = 0;
 };
 
 // Grow-only device buffer in the batch's stream order: the old buffer is
@@ -723,8 +746,6 @@ static int bt_init(CJBatch* b) {
   CJ_CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaEventCreate(&b->ev0), CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaEventCreate(&b->ev1), CUDA_MEM_ERROR);
-  CJ_CUDA_TRY(cudaFuncSetAttribute(k_decode_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
-              CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaFuncSetAttribute(k_pixel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
               CUDA_MEM_ERROR);
   b->parser = newJPGReader();
@@ -799,6 +820,7 @@ void cjBatchDestroy(CJBatch* b) {
     CJHostBuf* hb[] = {&b->h_hdr, &b->h_desc, &b->h_out, &b->h_st, &b->h_ctl};
     for (CJHostBuf* h : hb)
       if (h->p) cudaFreeHost(h->p);
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
     cudaEventDestroy(b->ev0);
     cudaEventDestroy(b->ev1);
     cudaStreamDestroy(b->stream);
@@ -814,12 +836,31 @@ int cjBatchSetSubsequenceBits(CJBatch* b, int bits) {
   return 0;
 }
 
+int cjBatchSetTuning(CJBatch* b, int sub_bits, int decode_ctas_per_sm, int pixel_tile_cap) {
+  if (!b) return PROGRAMMER_ERROR;
+  if (decode_ctas_per_sm == 0) decode_ctas_per_sm = BT_DECODE_CTAS_DEFAULT;
+  if (decode_ctas_per_sm < 3 || decode_ctas_per_sm > 5) return PROGRAMMER_ERROR;
+  if (pixel_tile_cap < 0 || (pixel_tile_cap & (pixel_tile_cap - 1))) return PROGRAMMER_ERROR;
+  int e = cjBatchSetSubsequenceBits(b, sub_bits);
+  if (e) return e;
+  b->decode_ctas = decode_ctas_per_sm;
+  b->tile_cap = pixel_tile_cap;
+  return 0;
+}
+
+void cjBatchGetTuning(const CJBatch* b, int* sub_bits, int* decode_ctas_per_sm, int* pixel_tile_cap) {
+  if (sub_bits) *sub_bits = b->sub_bits;
+  if (decode_ctas_per_sm) *decode_ctas_per_sm = b->decode_ctas;
+  if (pixel_tile_cap) *pixel_tile_cap = b->tile_cap;
+}
+
 int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* offsets,
                  const int64_t* sizes) {
   int err = bt_init(b);
   if (err) return err;
   if (n < 0) return PROGRAMMER_ERROR;
   b->n_in = n;
+  b->graph_stale = true;
   b->dev_of.assign(n, -1);
   b->host_err.assign(n, 0);
   b->dims.clear();
@@ -867,6 +908,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
     nsubw += sub_cap / 32;
     int bpm = (int)(h.total_blocks / ((int64_t)h.mcux * h.mcuy));
     d.T = cj_pix_tile_mcus(h.hmax, bpm);
+    while (b->tile_cap > 0 && d.T > b->tile_cap && d.T > 1) d.T >>= 1;
     d.ptile0 = nptiles;
     d.nptiles = h.mcuy * ((h.mcux + d.T - 1) / d.T);
     nptiles += d.nptiles;
@@ -922,10 +964,11 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   CJ_CUDA_TRY(cudaMemcpyAsync(b->blob.p, blob, (size_t)blob_bytes, cudaMemcpyHostToDevice, s),
               CUDA_MEM_ERROR);
   int per_sm = 0;
-  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_decode_batch, BT_THREADS, b->smem),
+  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)bt_decode_kernel(b->decode_ctas),
+                                                            BT_THREADS, b->smem),
               CUDA_KERNEL_LAUNCH_ERROR);
   if (per_sm < 1) return UNSUPPORTED_ERROR;
-  b->grid = per_sm * b->sm_count;
+  b->grid = std::min(per_sm, b->decode_ctas) * b->sm_count;
   CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pixel_batch, CJ_PIX_THREADS, b->smem_pix),
               CUDA_KERNEL_LAUNCH_ERROR);
   if (per_sm < 1) return UNSUPPORTED_ERROR;
@@ -933,9 +976,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   return 0;
 }
 
-int cjBatchRun(CJBatch* b) {
-  if (!b->ready) return PROGRAMMER_ERROR;
-  if (!b->n_dev) return 0;
+static CJBatchArgs bt_args(const CJBatch* b) {
   CJBatchArgs a;
   a.hdr = (const CJImageHeader*)b->hdr.p;
   a.desc = (const CJImageDesc*)b->desc.p;
@@ -961,12 +1002,102 @@ int cjBatchRun(CJBatch* b) {
   a.nwarps = b->nwarps;
   a.nptiles = b->nptiles;
   a.max_passes = b->nwarps + 2;
+  return a;
+}
+
+// The run of a staged batch as one CUDA graph: clear the control block, the
+// cooperative decode kernel (graph kernel node with the cooperative launch
+// attribute), the pixel kernel.  Buffers, counts and the decode-kernel
+// variant are baked into the nodes, so after every stage the graph is
+// rebuilt and the executable graph updated in place (instantiated again only
+// when that update is refused).
+static void bt_drop_graph(CJBatch* b) {
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  b->gexec = nullptr;
+}
+
+static bool bt_build_graph(CJBatch* b) {
+  const CJBatchArgs a = bt_args(b);
+  cudaGraph_t g = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  bool ok = true;
+  cudaGraphNode_t n_mem = nullptr, n_dec = nullptr, n_pix = nullptr;
+  cudaMemsetParams mp;
+  memset(&mp, 0, sizeof(mp));
+  mp.dst = b->ctl.p;
+  mp.value = 0;
+  mp.elementSize = 1;
+  mp.width = sizeof(CJBatchCtl);
+  mp.height = 1;
+  mp.pitch = 0;
+  ok = ok && cudaGraphAddMemsetNode(&n_mem, g, nullptr, 0, &mp) == cudaSuccess;
+  CJBatchArgs a1 = a;
+  void* args[] = {&a1};
+  cudaKernelNodeParams kp;
+  memset(&kp, 0, sizeof(kp));
+  kp.func = (void*)bt_decode_kernel(b->decode_ctas);
+  kp.gridDim = dim3(b->grid);
+  kp.blockDim = dim3(BT_THREADS);
+  kp.sharedMemBytes = (unsigned)b->smem;
+  kp.kernelParams = args;
+  ok = ok && cudaGraphAddKernelNode(&n_dec, g, &n_mem, 1, &kp) == cudaSuccess;
+  if (ok) {
+    cudaLaunchAttributeValue v;
+    memset(&v, 0, sizeof(v));
+    v.cooperative = 1;
+    ok = cudaGraphKernelNodeSetAttribute(n_dec, cudaLaunchAttributeCooperative, &v) == cudaSuccess;
+  }
+  if (ok && b->grid_pix > 0) {
+    cudaKernelNodeParams pp = kp;
+    pp.func = (void*)k_pixel_batch;
+    pp.gridDim = dim3(b->grid_pix);
+    pp.blockDim = dim3(CJ_PIX_THREADS);
+    pp.sharedMemBytes = (unsigned)b->smem_pix;
+    ok = cudaGraphAddKernelNode(&n_pix, g, &n_dec, 1, &pp) == cudaSuccess;
+  }
+  if (ok && b->gexec) {
+    // same topology as the instantiated graph: update its nodes in place
+    // (much cheaper than instantiating; batches are staged back to back)
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(b->gexec, g, &info) != cudaSuccess) {
+      cudaGetLastError();
+      bt_drop_graph(b);
+    }
+  }
+  if (ok && !b->gexec) ok = cudaGraphInstantiate(&b->gexec, g, 0) == cudaSuccess;
+  cudaGraphDestroy(g);
+  if (!ok) {
+    cudaGetLastError();
+    bt_drop_graph(b);
+  }
+  return ok;
+}
+
+int cjBatchRun(CJBatch* b) {
+  if (!b->ready) return PROGRAMMER_ERROR;
+  if (!b->n_dev) return 0;
   cudaStream_t s = b->stream;
+  if (b->use_graph && b->graph_stale) {
+    b->graph_stale = false;
+    if (!bt_build_graph(b)) b->graph_failures++;
+  }
+  if (b->use_graph && b->gexec) {
+    CJ_CUDA_TRY(cudaEventRecord(b->ev0, s), CUDA_KERNEL_LAUNCH_ERROR);
+    CJ_CUDA_TRY(cudaGraphLaunch(b->gexec, s), CUDA_KERNEL_LAUNCH_ERROR);
+    CJ_CUDA_TRY(cudaEventRecord(b->ev1, s), CUDA_KERNEL_LAUNCH_ERROR);
+    b->launches += b->grid_pix > 0 ? 2 : 1;
+    b->graph_launches++;
+    return 0;
+  }
+  CJBatchArgs a = bt_args(b);
   CJ_CUDA_TRY(cudaMemsetAsync(b->ctl.p, 0, sizeof(CJBatchCtl), s), CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaEventRecord(b->ev0, s), CUDA_KERNEL_LAUNCH_ERROR);
   void* args[] = {&a};
-  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_decode_batch, dim3(b->grid), dim3(BT_THREADS), args,
-                                          b->smem, s),
+  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bt_decode_kernel(b->decode_ctas), dim3(b->grid),
+                                          dim3(BT_THREADS), args, b->smem, s),
               CUDA_KERNEL_LAUNCH_ERROR);
   b->launches++;
   if (b->grid_pix > 0) {
@@ -1070,12 +1201,82 @@ void cjBatchStats(const CJBatch* b, int64_t* s) {
   s[9] = (int64_t)b->smem_pix;
   s[10] = b->launches;
   s[11] = b->grid_pix;
+  s[12] = b->graph_launches;
+  s[13] = b->graph_failures;
 }
 
 float cjBatchKernelMs(const CJBatch* b) {
   float ms = 0.f;
   if (b->ready) cudaEventElapsedTime(&ms, b->ev0, b->ev1);
   return ms;
+}
+
+// Device time of the staged batch under the current tuning: median of
+// `reps` runs after one warm-up run.
+static int bt_time_config(CJBatch* b, int n, const unsigned char* blob, const int64_t* offsets,
+                          const int64_t* sizes, int reps, float* ms) {
+  int e = cjBatchStage(b, n, blob, offsets, sizes);
+  if (!e) e = cjBatchRun(b);
+  if (!e) e = cjBatchWait(b, NULL);
+  std::vector<float> t;
+  for (int r = 0; r < reps && !e; r++) {
+    e = cjBatchRun(b);
+    if (!e) e = cjBatchWait(b, NULL);
+    t.push_back(cjBatchKernelMs(b));
+  }
+  if (e) return e;
+  std::sort(t.begin(), t.end());
+  *ms = t[t.size() / 2];
+  return 0;
+}
+
+int cjBatchAutotune(CJBatch* b, int n, const unsigned char* blob, const int64_t* offsets,
+                    const int64_t* sizes, int reps, float* best_ms, float* trials_ms, int max_trials) {
+  if (!b || n <= 0 || !blob) return PROGRAMMER_ERROR;
+  if (reps < 1) reps = 3;
+  static const int subs[] = {512, 1024, 2048, 4096};
+  static const int ctas[] = {3, 4, 5};
+  int best_s = b->sub_bits, best_c = b->decode_ctas, best_t = 0;
+  float best = 1e30f;
+  int trial = 0;
+  auto record = [&](float ms) {
+    if (trials_ms && trial < max_trials) trials_ms[trial] = ms;
+    trial++;
+  };
+  // 1. subsequence size x decode-kernel occupancy
+  for (int sb : subs)
+    for (int c : ctas) {
+      b->sub_bits = sb;
+      b->decode_ctas = c;
+      b->tile_cap = 0;
+      float ms = 0.f;
+      int e = bt_time_config(b, n, blob, offsets, sizes, reps, &ms);
+      if (e) return e;
+      record(ms);
+      if (ms < best) {
+        best = ms;
+        best_s = sb;
+        best_c = c;
+      }
+    }
+  // 2. pixel tile width at the best entropy configuration
+  b->sub_bits = best_s;
+  b->decode_ctas = best_c;
+  for (int cap : {8, 4, 2}) {
+    b->tile_cap = cap;
+    float ms = 0.f;
+    int e = bt_time_config(b, n, blob, offsets, sizes, reps, &ms);
+    if (e) return e;
+    record(ms);
+    if (ms < best) {
+      best = ms;
+      best_t = cap;
+    }
+  }
+  b->tile_cap = best_t;
+  if (best_ms) *best_ms = best;
+  // leave the batch staged under the chosen tuning
+  return cjBatchStage(b, n, blob, offsets, sizes);
 }
 
 }  // extern "C"
@@ -1113,8 +1314,6 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
       cj_note_cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
       return CUDA_MEM_ERROR;
     }
-    CJ_CUDA_TRY(cudaFuncSetAttribute(k_decode_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
-                CUDA_MEM_ERROR);
     CJ_CUDA_TRY(cudaFuncSetAttribute(k_pixel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
                 CUDA_MEM_ERROR);
     g_noalloc_ptr[dev] = (unsigned char*)p;
@@ -1263,11 +1462,13 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   a.max_passes = nwarps + 2;
   int sms = 0, per_sm = 0;
   CJ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), CUDA_MEM_ERROR);
-  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_decode_batch, BT_THREADS, smem),
+  const bt_decode_fn dk = bt_decode_kernel(BT_DECODE_CTAS_DEFAULT);
+  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)dk, BT_THREADS, smem),
               CUDA_KERNEL_LAUNCH_ERROR);
   if (per_sm < 1) return UNSUPPORTED_ERROR;
+  per_sm = std::min(per_sm, BT_DECODE_CTAS_DEFAULT);
   void* args[] = {&a};
-  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_decode_batch, dim3(per_sm * sms), dim3(BT_THREADS), args,
+  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)dk, dim3(per_sm * sms), dim3(BT_THREADS), args,
                                           smem, s),
               CUDA_KERNEL_LAUNCH_ERROR);
   CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pixel_batch, CJ_PIX_THREADS, smem_pix),

@@ -163,27 +163,32 @@ CJ_HD int32_t cj_extend(uint32_t bits, uint32_t size) {
 // MSB-first bit reader over the destuffed buffer with a 64-bit register
 // window and one word of prefetch, so the load feeding the next refill is in
 // flight while the current symbols decode.  Bytes at or past `end_byte` read
-// as 0xFF (the padding the reference's bit reader supplies).
+// as 0xFF (the padding the reference's bit reader supplies).  Word indices are
+// 32-bit (a scan is at most CJ_MAX_SCAN_BYTES); the bit position is not kept
+// but derived: pos() = 32 * w - n.
 struct CJBits {
   const uint32_t* words;
-  uint64_t end_byte;
-  uint64_t buf;   // unread bits, MSB-aligned
-  uint64_t pos;   // absolute bit position of buf's MSB
-  uint64_t w;     // next word to append
-  uint32_t nxt;   // that word, already loaded
-  int n;          // valid bits in buf (32..63 after a refill)
+  uint64_t buf;        // unread bits, MSB-aligned
+  uint32_t w;          // index of the word in `nxt`
+  uint32_t wfull;      // words below this index lie wholly before end_byte
+  uint32_t end_byte;
+  uint32_t nxt;        // the next word to append, already loaded
+  int n;               // valid bits in buf (32..63 after a refill)
 
+  CJ_HD uint32_t word(uint32_t i) const {
+    if (i < wfull) return cj_bswap(words[i]);
+    return cj_word(words, i, end_byte);  // the partial last word, or past the end
+  }
   CJ_HD void init(const uint32_t* wd, uint64_t eb, uint64_t p) {
     words = wd;
-    end_byte = eb;
-    pos = p;
-    w = p >> 5;
-    uint32_t first = cj_word(words, w, end_byte);
+    end_byte = (uint32_t)eb;
+    wfull = (uint32_t)(eb >> 2);
+    uint32_t w0 = (uint32_t)(p >> 5);
     uint32_t s = (uint32_t)(p & 31);
-    buf = ((uint64_t)first << 32) << s;
+    buf = ((uint64_t)word(w0) << 32) << s;
     n = 32 - (int)s;
-    w++;
-    nxt = cj_word(words, w, end_byte);
+    w = w0 + 1;
+    nxt = word(w);
     refill();
   }
   CJ_HD void refill() {
@@ -191,14 +196,14 @@ struct CJBits {
       buf |= (uint64_t)nxt << (32 - n);
       n += 32;
       w++;
-      nxt = cj_word(words, w, end_byte);
+      nxt = word(w);
     }
   }
+  CJ_HD uint64_t pos() const { return ((uint64_t)w << 5) - (uint64_t)n; }
   CJ_HD uint32_t peek32() const { return (uint32_t)(buf >> 32); }
   CJ_HD void skip(uint32_t k) {
     buf <<= k;
     n -= (int)k;
-    pos += k;
     refill();
   }
 };
@@ -261,7 +266,7 @@ CJ_HD uint64_t cj_decode_block(const uint32_t* words, uint64_t end_byte, uint64_
   br.init(words, end_byte, p);
   *err = cj_block(br, dc, ac, zz, dc_diff, sink);
   *last_sym = p;
-  return br.pos;
+  return br.pos();
 }
 
 struct CJNullSink {

@@ -105,7 +105,7 @@ __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const
   uint32_t m = cj_state_phase(start);
   int nb = 0, d0 = 0, d1 = 0, d2 = 0;
   CJNullSink ns;
-  while (br.pos < ln.end) {
+  while (br.pos() < ln.end) {
     int c = sp.phase_comp[m];
     int32_t dd;
     cj_block(br, sp.huff[sp.comp_dc[c]], sp.huff[sp.comp_ac[c]], sp.zz, &dd, ns);
@@ -117,7 +117,7 @@ __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const
   }
   CJSubRec r;
   r.start = start;
-  r.exit = cj_state(br.pos, m);
+  r.exit = cj_state(br.pos(), m);
   r.nblocks = nb;
   r.dc[0] = d0;
   r.dc[1] = d1;
@@ -216,12 +216,13 @@ __device__ __forceinline__ void cj_warp_prefix(const CJSubRec& r, const CJLane& 
 
 // Final decode of one lane from its settled start: writes quantised int16
 // coefficients (natural order) of its blocks, DC predicted per component,
-// and records structural errors of its restart interval.
+// and records structural errors of its restart interval.  `zz` is the
+// zig-zag -> natural index table (64 entries, in shared memory).
 __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint32_t* words,
                                               const CJLane& ln, const CJSegment& seg,
                                               const CJSubRec& r, int64_t first_block, int dc0,
                                               int dc1, int dc2, int16_t* __restrict__ coef,
-                                              CJStatus* st) {
+                                              CJStatus* st, const uint8_t* zz) {
   int64_t b = first_block;
   const int64_t bend = seg.first_block + seg.nblocks;
   CJBits br;
@@ -229,7 +230,7 @@ __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint
   uint32_t m = cj_state_phase(r.start);
   const uint64_t seg_end = seg.bit_end;
   for (;;) {
-    const uint64_t p = br.pos;
+    const uint64_t p = br.pos();
     if (!ln.last && p >= ln.end) break;
     if (b >= bend) {
       if (!ln.last) cj_raise_dec(st, b, CJ_DEV_EXTRA);
@@ -251,12 +252,12 @@ __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint
     for (int k = 0; k < 8; k++) reinterpret_cast<uint4*>(blk)[k] = z;
     CJCoefSink sink{blk};
     int32_t dd;
-    int err = cj_block(br, sp.huff[sp.comp_dc[c]], sp.huff[sp.comp_ac[c]], sp.zz, &dd, sink);
+    int err = cj_block(br, sp.huff[sp.comp_dc[c]], sp.huff[sp.comp_ac[c]], zz, &dd, sink);
     if (err) {
       cj_raise_dec(st, b, err);
       break;
     }
-    if (seg.marker_follows && br.pos > seg_end) {
+    if (seg.marker_follows && br.pos() > seg_end) {
       cj_raise_dec(st, b, CJ_DEV_OVERRUN);
       break;
     }

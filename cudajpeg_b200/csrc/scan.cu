@@ -425,7 +425,7 @@ k_decode_write(const CJScanParams* __restrict__ prm, const CJSegment* __restrict
   cj_warp_prefix(r, ln, cw.nblocks, cw.dc[0], cw.dc[1], cw.dc[2], &e0, &e1, &e2, &e3);
   if (!ln.active) return;
   const CJSegment seg = segs[ln.seg];
-  cj_write_lane(sp, words, ln, seg, r, seg.first_block + e0, e1, e2, e3, coef, st);
+  cj_write_lane(sp, words, ln, seg, r, seg.first_block + e0, e1, e2, e3, coef, st, sp.zz);
 }
 
 // ---------------------------------------------------------------- host side

@@ -68,6 +68,9 @@ struct CJServer {
   int64_t batches = 0, images = 0, max_running = 0, max_batch_seen = 0;
   bool stop = false;
   int fatal = 0;
+  // applied to each engine before it stages; serving batches are small at low
+  // load, where short subsequences give the lowest latency
+  int tune_sub = 512, tune_ctas = 0, tune_cap = 0;
   std::thread worker;
 };
 
@@ -177,6 +180,7 @@ static void cj_server_loop(CJServer* s) {
       if (en.tickets.empty()) break;  // the budget is full: wait for a completion
       en.footprint = fp;
       s->inflight_bytes += fp;
+      cjBatchSetTuning(en.batch, s->tune_sub, s->tune_ctas, s->tune_cap);
       const int n = (int)en.tickets.size();
       // packing, host parse, H2D and launch happen outside the lock
       lk.unlock();
@@ -311,6 +315,21 @@ void cjServerRelease(CJServer* s, long long ticket) {
   if (e >= 0) s->engines[e].held--;
   s->reqs.erase(it);
   s->cv_work.notify_one();
+}
+
+int cjServerSetTuning(CJServer* s, int sub_bits, int decode_ctas_per_sm, int pixel_tile_cap) {
+  if (!s) return PROGRAMMER_ERROR;
+  // validate on a scratch batch object (no device work)
+  CJBatch* probe = cjBatchCreate();
+  if (!probe) return OOM_ERROR;
+  int e = cjBatchSetTuning(probe, sub_bits, decode_ctas_per_sm, pixel_tile_cap);
+  cjBatchDestroy(probe);
+  if (e) return e;
+  std::lock_guard<std::mutex> g(s->mu);
+  s->tune_sub = sub_bits;
+  s->tune_ctas = decode_ctas_per_sm;
+  s->tune_cap = pixel_tile_cap;
+  return 0;
 }
 
 void cjServerStats(CJServer* s, long long* st) {

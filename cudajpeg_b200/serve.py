@@ -85,6 +85,11 @@ class Server:
             raise DecodeError(rc, f"cjServerCopyOut({ticket})")
         return out
 
+    def set_tuning(self, sub_bits: int = 0, decode_ctas_per_sm: int = 0, pixel_tile_cap: int = 0):
+        err = self.lib.cjServerSetTuning(self.ptr, sub_bits, decode_ctas_per_sm, pixel_tile_cap)
+        if err:
+            raise ValueError(f"bad tuning {(sub_bits, decode_ctas_per_sm, pixel_tile_cap)}")
+
     def release(self, ticket: int):
         self.lib.cjServerRelease(self.ptr, ticket)
 

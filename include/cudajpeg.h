@@ -98,11 +98,29 @@ CJBatch *cjBatchCreate(void);
 void cjBatchDestroy(CJBatch *b);
 int cjBatchSetSubsequenceBits(CJBatch *b, int bits);
 
+/* Tuning of later stages/runs: bits per speculative subsequence (0 =
+ * default; multiple of 32, 128..65536), decode-kernel CTAs per SM (3, 4 or 5,
+ * 0 = 4: the register budget per thread of the entropy kernel, 80/64/48), and
+ * the largest pixel tile in MCUs (power of two, 0 = the layout maximum:
+ * 128 pixels across). */
+int cjBatchSetTuning(CJBatch *b, int sub_bits, int decode_ctas_per_sm, int pixel_tile_cap);
+void cjBatchGetTuning(const CJBatch *b, int *sub_bits, int *decode_ctas_per_sm, int *pixel_tile_cap);
+/* Autotuner: times the given batch (device time, median of `reps` runs)
+ * under every subsequence size in {512, 1024, 2048, 4096} x decode CTAs per
+ * SM in {3, 4, 5}, then pixel tile caps {8, 4, 2} at the best of those, and
+ * keeps the fastest tuning in `b`.  The batch is left staged under it.
+ * trials_ms (may be NULL) receives up to max_trials timings in that order;
+ * *best_ms (may be NULL) the best. */
+int cjBatchAutotune(CJBatch *b, int n, const unsigned char *blob, const int64_t *offsets,
+                    const int64_t *sizes, int reps, float *best_ms, float *trials_ms, int max_trials);
+
 /* Parse, plan and queue the host->device copy of a batch (asynchronous). */
 int cjBatchStage(CJBatch *b, int n, const unsigned char *blob, const int64_t *offsets,
                  const int64_t *sizes);
-/* Queue the decode kernel over the staged batch (inputs already on the
- * device; may be re-run to re-decode them). */
+/* Queue the decode over the staged batch (inputs already on the device; may
+ * be re-run to re-decode them): one CUDA graph launch -- clear the control
+ * block, the cooperative decode kernel, the pixel kernel -- built once per
+ * stage. */
 int cjBatchRun(CJBatch *b);
 /* Queue the device->host copy of all outputs into the batch's pinned buffer. */
 int cjBatchFetch(CJBatch *b);
@@ -120,10 +138,11 @@ const unsigned char *cjBatchDeviceImage(const CJBatch *b, int i);
  * cjBatchStage); PROGRAMMER_ERROR if image i was rejected by the host parse. */
 int cjBatchImageGeometry(const CJBatch *b, int i, int *width, int *height, int *channels);
 void *cjBatchStream(const CJBatch *b);
-/* stats[0..11]: images submitted, images on the device, decode-kernel CTAs,
+/* stats[0..13]: images submitted, images on the device, decode-kernel CTAs,
  * warp items, destuff tiles, pixel tiles, fix-up passes of the last run,
  * input bytes, output bytes, pixel-kernel dynamic shared memory, kernel
- * launches so far, pixel-kernel CTAs. */
+ * launches so far, pixel-kernel CTAs, runs launched as a CUDA graph, graph
+ * builds that failed (those runs used plain launches). */
 void cjBatchStats(const CJBatch *b, int64_t *stats);
 /* Device time of the last cjBatchRun, in milliseconds. */
 float cjBatchKernelMs(const CJBatch *b);
@@ -193,6 +212,10 @@ int cjServerWait(CJServer *s, long long ticket, double timeout_s, CJServerResult
 int cjServerCopyOut(CJServer *s, long long ticket, unsigned char *host_dst, size_t capacity);
 /* Ends a finished request; its device pixels may be reused afterwards. */
 void cjServerRelease(CJServer *s, long long ticket);
+/* Batch tuning (as cjBatchSetTuning) for the batches staged from now on.
+ * The server's default is 512-bit subsequences (the lowest latency for the
+ * small batches of light load), 4 decode CTAs per SM, full pixel tiles. */
+int cjServerSetTuning(CJServer *s, int sub_bits, int decode_ctas_per_sm, int pixel_tile_cap);
 /* stats[0..5]: batches launched, images admitted, most batches in flight at
  * once, largest batch, requests waiting, projected bytes in flight. */
 void cjServerStats(CJServer *s, long long *stats);

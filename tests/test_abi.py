@@ -115,3 +115,15 @@ def test_huffman_tables_match_reference_lut(cj):
         ref = _reference_lut(counts, s)
         got = np.array([lib.cjDebugHuffDecode(c, s.ctypes.data, w) for w in range(0, 65536, 7)])
         assert np.array_equal(got, ref[::7])
+
+
+def test_batch_tuning_validation_without_gpu(cj):
+    """cjBatchSetTuning checks its arguments on the host (no device work)."""
+    with cj.Batch() as b:
+        assert b.tuning() == {"sub_bits": 1024, "decode_ctas_per_sm": 4, "pixel_tile_cap": 0}
+        b.set_tuning(2048, 5, 4)
+        assert b.tuning() == {"sub_bits": 2048, "decode_ctas_per_sm": 5, "pixel_tile_cap": 4}
+        for bad in [(100, 4, 0), (1000, 4, 0), (1024, 7, 0), (1024, 2, 0), (1024, 4, 3), (1024, 4, -2)]:
+            with pytest.raises(ValueError):
+                b.set_tuning(*bad)
+        assert b.tuning()["sub_bits"] == 2048  # a rejected call changes nothing

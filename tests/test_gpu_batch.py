@@ -25,6 +25,7 @@ def test_mixed_batch_matches_oracle(cj, oracle_mod):
     files = [s.data for s in W.mixed_batch(n=40, seed=21, max_side=700)]
     stats = check_batch(cj, oracle_mod, files)
     assert stats["on_device"] == 40 and stats["launches"] == 2  # decode kernel + pixel kernel
+    assert stats["graph_runs"] == 1 and stats["graph_failures"] == 0  # launched as one CUDA graph
 
 
 def test_golden_cases_in_one_batch(cj, golden, oracle_mod):
@@ -77,3 +78,39 @@ def test_batch_all_rejected_on_host(cj):
     with cj.Batch() as b:
         imgs, errs = b.decode([b"\xff\xd8\xff\xd9", b"not a jpeg at all"])
     assert errs == [1, 5] and imgs == [None, None]
+
+
+@pytest.mark.parametrize("sub_bits,ctas,cap", [(512, 3, 0), (1024, 4, 0), (2048, 5, 4), (4096, 4, 2),
+                                               (1024, 5, 8)])
+def test_tuning_variants_identical(cj, oracle_mod, sub_bits, ctas, cap):
+    """Every tuning the autotuner can pick decodes bit-identically."""
+    files = [s.data for s in W.mixed_batch(n=16, seed=12, max_side=800)]
+    with cj.Batch() as b:
+        b.set_tuning(sub_bits, ctas, cap)
+        imgs, errs = b.decode(files)
+        assert b.tuning() == {"sub_bits": sub_bits, "decode_ctas_per_sm": ctas, "pixel_tile_cap": cap}
+    for k, data in enumerate(files):
+        ref = oracle_mod.decode(data)
+        assert errs[k] == ref.error, k
+        if ref.error == 0:
+            assert np.array_equal(imgs[k], ref.pixels), k
+
+
+def test_autotune_keeps_results(cj, oracle_mod):
+    files = [s.data for s in W.mixed_batch(n=24, seed=13, max_side=600)]
+    blob, offsets, sizes = cj.Batch.pack(files)
+    with cj.Batch() as b:
+        res = b.autotune(blob.ctypes.data, offsets, sizes, reps=1)
+        assert res["sub_bits"] in (512, 1024, 2048, 4096)
+        assert res["decode_ctas_per_sm"] in (3, 4, 5)
+        assert res["best_ms"] > 0 and min(t for t in res["trials_ms"] if t > 0) == pytest.approx(res["best_ms"])
+        b.run()
+        b.fetch()
+        errs = b.wait()
+        for k, data in enumerate(files):
+            ref = oracle_mod.decode(data)
+            assert errs[k] == ref.error
+            if ref.error == 0:
+                assert np.array_equal(b.image(k), ref.pixels), k
+
+
