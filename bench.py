@@ -2,14 +2,17 @@
 """bench.py -- decoded MPix/s of the baseline-JPEG decode path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cudajpeg|reference]
-                    [--workload mixed_batch|single_4096|single_1024]
+                    [--workload mixed_batch|single_4096|single_1024|precision_8192]
 
 Default workload (the batching configuration): one batch of 1024 seeded
 synthetic baseline JPEGs, W and H log-uniform in [64, 2048], 4:2:0 / 4:2:2 /
 4:4:4 / grey with p = .6/.2/.1/.1, quality U[50, 95], 30% with restart
 intervals of 16-64 MCUs (about 320 MPix, 58 MB of JPEG).  One step = one
-decode of the whole batch by the persistent batch kernel (cjBatchRun).
-The single_* workloads time the plain per-image path (openJPG) instead.
+decode of the whole batch: one CUDA-graph launch of the persistent
+cooperative decode kernel and the pixel kernel (cjBatchRun), under the
+tuning the autotuner (cjBatchAutotune) picks in the untimed warm-up.
+The single_* workloads time the plain per-image path (openJPG) instead;
+precision_8192 is the iDCT precision A/B (run_precision).
 
 * ``value``   device-resident throughput: the compressed bytes are already in
   HBM when the timed region starts; each step is timed with CUDA events on
@@ -20,10 +23,14 @@ The single_* workloads time the plain per-image path (openJPG) instead.
 * ``e2e``     the same metric through the public C API: per step the host
   parse, the host->device copy of the files from pinned memory, the decode,
   and the device->host copy of every decoded image into pinned memory.
-* ``roofline`` the dominant kernel's algorithmic bytes (entropy-coded bytes
-  read + output pixels written) / its mean duration, against the measured
-  HBM copy bandwidth in MEASURED_PEAKS.json.
+* ``roofline`` the dominant kernel (k_decode_batch): its algorithmic bytes
+  (compressed scans read, destuffed copy written and read twice, int16
+  coefficient blocks written) / its duration (in-kernel %globaltimer phase
+  stamps), against the measured HBM copy bandwidth in MEASURED_PEAKS.json;
+  ``roofline_pixel`` the same for k_pixel_batch (blocks read, pixels written).
 * ``plain_path`` (batch workload) the per-image path over the same images.
+* ``serving`` open-loop Poisson request streams through the continuous-
+  batching server (cudajpeg_b200.serve): p50/p99/p99.9 latency, MPix/s.
 * ``cpu_baseline`` the reference's own CPUonly decoder (compiled from its
   sources into oracle/_ref) on the host cores, on a bounded sample.
 
@@ -73,12 +80,16 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="cudajpeg", choices=["cudajpeg", "reference"])
     ap.add_argument("--workload", default="mixed_batch",
-                    choices=["mixed_batch", "single_4096", "single_1024"])
+                    choices=["mixed_batch", "single_4096", "single_1024", "precision_8192"])
+    ap.add_argument("--precision-size", type=int, default=8192,
+                    help="image side of the precision workload (8192 as specified)")
     ap.add_argument("--batch-size", type=int, default=1024)
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default batch tuning")
+    ap.add_argument("--tuning", default="",
+                    help="fixed batch tuning SUB_BITS,CTAS_PER_SM,TILE_CAP instead of the autotuner")
     ap.add_argument("--serve-seconds", type=float, default=1.5,
                     help="seconds of arrivals per rate for the serving measurement (0: skip)")
     return ap.parse_args()
@@ -349,7 +360,14 @@ def run_batch(args, wl, world, rank, local, dist):
         raise RuntimeError(f"batch decode errors: {sum(1 for e in errs if e)}")
     # untimed: the autotuner picks subsequence size, decode-kernel occupancy
     # and pixel tile width for this batch (cjBatchAutotune)
-    tune = b.autotune(src.data_ptr(), offsets, sizes, reps=3) if not args.no_autotune else b.tuning()
+    if args.tuning:
+        b.set_tuning(*[int(x) for x in args.tuning.split(",")])
+        b.stage(src.data_ptr(), offsets, sizes)
+        tune = b.tuning()
+    elif args.no_autotune:
+        tune = b.tuning()
+    else:
+        tune = b.autotune(src.data_ptr(), offsets, sizes, reps=3)
     b.run()
     if any(b.wait()):
         raise RuntimeError("batch decode errors under the tuned configuration")
@@ -374,7 +392,8 @@ def run_batch(args, wl, world, rank, local, dist):
             for name, ms in b.phase_ms().items():
                 phases.setdefault(name, []).append(ms)
         torch.cuda.synchronize()
-    launches = b.stats()["launches"] - launches0
+    st_run = b.stats()
+    launches = st_run["launches"] - launches0
     if dist:
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
@@ -408,9 +427,20 @@ def run_batch(args, wl, world, rank, local, dist):
 
     peaks = read_peaks()
     mean_ms = total_ms / args.steps
-    alg = wl.file_bytes + wl.out_bytes
-    achieved = alg / (mean_ms / 1e3) / 1e9
     pm = {k: round(statistics.mean(v), 4) for k, v in phases.items()}
+    # per-kernel rooflines from the in-kernel phase stamps (CUDA-event total
+    # split by %globaltimer stamps at each phase start and the pixel kernel's end)
+    decode_ms = sum(pm[k] for k in cj.BATCH_PHASES[:9])
+    pixel_ms = pm["pixel"]
+    coef_bytes = st_run["blocks"] * 128
+    # k_decode_batch must read the compressed scans, write the destuffed
+    # copy, read it at least twice (speculative sync + write-out) and write
+    # the int16 coefficient blocks; k_pixel_batch reads the blocks and
+    # writes the interleaved output
+    alg_decode = st_run["input_bytes"] + 3 * st_run["scan_bytes"] + coef_bytes
+    alg_pixel = coef_bytes + st_run["output_bytes"]
+    ach_decode = alg_decode / (decode_ms / 1e3) / 1e9
+    ach_pixel = alg_pixel / (pixel_ms / 1e3) / 1e9
     lat = sorted(e2e_ms)
     line = {"metric": METRIC, "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean_ms, 4),
@@ -432,11 +462,18 @@ def run_batch(args, wl, world, rank, local, dist):
                     "d2h_bytes_per_step": int(st["output_bytes"]),
                     "latency_ms_p50": round(lat[len(lat) // 2], 3),
                     "latency_ms_p99": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 3)},
-            "roofline": {"bound": "hbm", "kernel": "k_decode_batch", "achieved": round(achieved, 1),
+            "roofline": {"bound": "hbm", "kernel": "k_decode_batch", "achieved": round(ach_decode, 1),
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": round(achieved / peaks["hbm_gbs"], 4),
+                         "frac": round(ach_decode / peaks["hbm_gbs"], 4),
                          "traffic": read_traffic("k_decode_batch", args.workload),
-                         "algorithmic_bytes": int(alg), "peak_source": peaks["source"]},
+                         "algorithmic_bytes": int(alg_decode), "kernel_ms": round(decode_ms, 4),
+                         "peak_source": peaks["source"]},
+            "roofline_pixel": {"bound": "hbm", "kernel": "k_pixel_batch", "achieved": round(ach_pixel, 1),
+                               "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                               "frac": round(ach_pixel / peaks["hbm_gbs"], 4),
+                               "traffic": read_traffic("k_pixel_batch", args.workload),
+                               "algorithmic_bytes": int(alg_pixel), "kernel_ms": round(pixel_ms, 4),
+                               "peak_source": peaks["source"]},
             "phase_ms": pm, "gpu_launches": int(launches), "clocks": clocks.summary()}
     if rank == 0 and world == 1:
         line["plain_path"] = plain_path_value(cj, wl.files)
@@ -545,6 +582,112 @@ def run_single(args, wl, world, rank, local, dist):
             "gpu_launches": int(launches), "clocks": clocks.summary()}
 
 
+def idct_basis_f64():
+    """C[u, x] = c(u)/2 cos((2x+1) u pi / 16), c(0) = 1/sqrt(2): the 8-point
+    inverse DCT of T.81 A.3.3, in float64."""
+    import numpy as np
+    u = np.arange(8)[:, None]
+    x = np.arange(8)[None, :]
+    cu = np.where(u == 0, 1 / np.sqrt(2), 1.0)
+    return cu / 2 * np.cos((2 * x + 1) * u * np.pi / 16)
+
+
+def run_precision(args):
+    """Precision form: plane iDCT of 8192x8192 q95 images (4:4:4, 4:2:2,
+    grey; 50/50 uniform noise and gradient) in the three arithmetic forms of
+    cjIDCTPlane -- the bit-exact fixed-point iDCT, FP32 on CUDA cores, FP16
+    hi+lo basis on tensor cores with FP32 accumulation -- timed with CUDA
+    events, with the raw FP32 outputs (cjIDCTBlocksRaw) compared against a
+    float64 iDCT of the same dequantised coefficients."""
+    import numpy as np
+    import torch
+
+    import cudajpeg_b200 as cj
+    from cudajpeg_b200 import workloads as W
+    samples = [W.precision_8192(m, size=args.precision_size) for m in ("444", "422", "gray")]
+    torch.cuda.set_device(0)
+    basis = torch.from_numpy(idct_basis_f64()).cuda()
+    peaks = read_peaks()
+    modes = {"int": cj.IDCT_INT, "f32": cj.IDCT_F32, "tc": cj.IDCT_TC}
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    rows = []
+    tot = {m: [0.0, 0] for m in modes}
+    for smp in samples:
+        with cj.Reader(host_coefficients=True) as r:
+            r.open_bytes(smp.data)
+            coefs = r.coefficients()  # dequantised int32 per component, reference layout
+            for c in range(len(coefs)):
+                g = r.plane_geometry(c)
+                nblk = coefs[c].shape[0]
+                planes, ms = {}, {}
+                for name, mode in modes.items():
+                    out = torch.zeros((g["rows"], g["stride"]), dtype=torch.uint8, device="cuda")
+                    stream = torch.cuda.current_stream()
+                    for _ in range(args.warmup):
+                        r.plane_launch(g, out.data_ptr(), mode, stream.cuda_stream)
+                    ts = []
+                    for _ in range(args.steps):
+                        flush.zero_()  # coefficients (128 B/block) start outside L2
+                        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        s0.record(stream)
+                        r.plane_launch(g, out.data_ptr(), mode, stream.cuda_stream)
+                        s1.record(stream)
+                        s1.synchronize()
+                        ts.append(s0.elapsed_time(s1))
+                    ms[name] = float(np.median(ts))
+                    planes[name] = out
+                    tot[name][0] += ms[name]
+                    tot[name][1] += nblk * 64
+                ref = planes["int"].to(torch.int16)
+                match = {}
+                for name in ("f32", "tc"):
+                    d = (planes[name].to(torch.int16) - ref).abs()
+                    match[name] = {"exact": round(float((d == 0).double().mean()), 6),
+                                   "within_1": round(float((d <= 1).double().mean()), 6),
+                                   "max_abs": int(d.max())}
+                # raw (pre-rounding) error against float64, in chunks
+                err = {}
+                deq = coefs[c]
+                if np.abs(deq).max() > 32767:
+                    raise RuntimeError("dequantised coefficient outside int16")
+                ones = np.ones(64, np.int16)
+                for name in ("f32", "tc"):
+                    mx, sm = 0.0, 0.0
+                    for k0 in range(0, nblk, 1 << 18):
+                        blk = deq[k0:k0 + (1 << 18)]
+                        raw = torch.from_numpy(cj.idct_blocks_raw(blk.astype(np.int16), ones, modes[name])).cuda()
+                        x = torch.from_numpy(blk).cuda().double().view(-1, 8, 8)
+                        want = (basis.t() @ x @ basis).reshape(-1, 64)   # out[x][y] = sum_uv C[u,x] C[v,y] F[u,v]
+                        e = (raw.double() - want).abs()
+                        mx = max(mx, float(e.max()))
+                        sm += float(e.sum())
+                    err[name] = {"max_abs_vs_f64": round(mx, 6), "mean_abs_vs_f64": round(sm / (nblk * 64), 8)}
+                mpix = {k: round(nblk * 64 / (v / 1e3) / 1e6, 1) for k, v in ms.items()}
+                gbs = {k: round(nblk * 192 / (v / 1e3) / 1e9, 1) for k, v in ms.items()}
+                rows.append({"image": f"{smp.mode}_{smp.width}x{smp.height}_q{smp.quality}", "component": c,
+                             "blocks": nblk, "ms": {k: round(v, 4) for k, v in ms.items()},
+                             "MPix_per_s": mpix, "GB_per_s": gbs, "match_vs_int": match, "raw_error": err})
+    tc_mpix = tot["tc"][1] / (tot["tc"][0] / 1e3) / 1e6
+    tc_gbs = tot["tc"][1] * 3 / (tot["tc"][0] / 1e3) / 1e9   # 2 B coefficient in + 1 B sample out per pixel
+    worst_tc = max(r_["raw_error"]["tc"]["max_abs_vs_f64"] for r_ in rows)
+    line = {"metric": "plane iDCT MPix/s (tensor-core FP16 hi/lo, FP32 accumulate)", "value": round(tc_mpix, 1),
+            "unit": "MPix/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(tot["tc"][0] / max(1, len(rows)), 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp16 hi/lo in, fp32 accumulate",
+            "data": "synthetic",
+            "config": {"workload": f"precision_{args.precision_size}", "images": "444, 422, grey at q95",
+                       "content": "50/50 uniform noise and gradient (cudajpeg_b200/workloads.py)",
+                       "l2": "L2 flushed (256 MB write) before every timed launch"},
+            "per_mode_MPix_per_s": {k: round(v[1] / (v[0] / 1e3) / 1e6, 1) for k, v in tot.items()},
+            "tc_max_abs_error_vs_f64": worst_tc, "tc_error_below_0_5": worst_tc < 0.5,
+            "roofline": {"bound": "hbm", "kernel": "k_idct_tc", "achieved": round(tc_gbs, 1),
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(tc_gbs / peaks["hbm_gbs"], 4),
+                         "traffic": read_traffic("k_idct_tc", f"precision_{args.precision_size}"),
+                         "peak_source": peaks["source"]},
+            "rows": rows}
+    print(json.dumps(line), flush=True)
+
+
 def run_gpu(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -576,6 +719,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload.startswith("precision"):
+        run_precision(args)
     else:
         run_gpu(args)
 

@@ -55,7 +55,7 @@ EXPORTED = [
 ]
 
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
-                "fixup", "warp_scan", "write", "pixel"]
+                "fixup", "warp_scan", "write", "pixel", "launch"]
 
 KERNEL_NAMES = ["k_destuff_count", "k_scan_tiles", "k_destuff_scatter", "k_build_segments",
                 "k_sync_intra", "k_sync_inter", "k_scan_warps", "k_decode_write", "k_pixel"]
@@ -276,23 +276,34 @@ class Reader:
     def launch_count(self) -> int:
         return int(self.lib.cjReaderLaunchCount(self.ptr))
 
+    def plane_geometry(self, c: int) -> dict:
+        """Arguments of cjIDCTPlane for component c of the last decode."""
+        fields = _Reader.from_address(self.ptr)
+        ch = fields.channels[c]
+        first = sum(fields.channels[k].samples_x * fields.channels[k].samples_y for k in range(c))
+        coef, _ = self.device_coefficients()
+        return {"coef": coef, "bpm": self.info()["bpm"], "first": first, "sx": ch.samples_x,
+                "sy": ch.samples_y, "mcux": fields.num_blocks_x, "mcuy": fields.num_blocks_y,
+                "q": self.lib.cjReaderDeviceQuantTable(self.ptr, ch.dq_id), "rows": ch.block_stride,
+                "stride": ch.stride}
+
+    def plane_launch(self, geom: dict, out_ptr: int, mode: int, stream: int = 0):
+        """Queue cjIDCTPlane for a plane_geometry() on `stream` (no sync)."""
+        g = geom
+        err = self.lib.cjIDCTPlane(C.c_void_p(g["coef"]), g["bpm"], g["first"], g["sx"], g["sy"],
+                                   g["mcux"], g["mcuy"], C.c_void_p(g["q"]), C.c_void_p(out_ptr),
+                                   g["stride"], mode, C.c_void_p(stream) if stream else None)
+        if err:
+            raise DecodeError(err, "cjIDCTPlane")
+
     def plane(self, c: int, mode: int = 0):
         """iDCT of component c of the last decode through cjIDCTPlane into a
         padded uint8 plane [rows, stride] (mode: IDCT_INT / IDCT_F32 / IDCT_TC)."""
         import torch
-        fields = _Reader.from_address(self.ptr)
-        ch = fields.channels[c]
-        bpm = self.info()["bpm"]
-        first = sum(fields.channels[k].samples_x * fields.channels[k].samples_y for k in range(c))
-        plane = torch.zeros((ch.block_stride, ch.stride), dtype=torch.uint8, device="cuda")
-        coef, _ = self.device_coefficients()
-        q = self.lib.cjReaderDeviceQuantTable(self.ptr, ch.dq_id)
+        g = self.plane_geometry(c)
+        plane = torch.zeros((g["rows"], g["stride"]), dtype=torch.uint8, device="cuda")
         torch.cuda.synchronize()
-        err = self.lib.cjIDCTPlane(C.c_void_p(coef), bpm, first, ch.samples_x, ch.samples_y,
-                                   fields.num_blocks_x, fields.num_blocks_y, C.c_void_p(q),
-                                   C.c_void_p(plane.data_ptr()), ch.stride, mode, None)
-        if err:
-            raise DecodeError(err, "cjIDCTPlane")
+        self.plane_launch(g, plane.data_ptr(), mode)
         torch.cuda.synchronize()
         return plane.cpu().numpy()
 
@@ -308,7 +319,7 @@ class Batch:
 
     STAT_KEYS = ["submitted", "on_device", "grid", "warp_items", "destuff_tiles", "pixel_tiles",
                  "passes", "input_bytes", "output_bytes", "smem", "launches", "pixel_grid",
-                 "graph_runs", "graph_failures"]
+                 "graph_runs", "graph_failures", "blocks", "scan_bytes"]
 
     def __init__(self, sub_bits: int = 0):
         self.lib = load()
@@ -395,7 +406,7 @@ class Batch:
         return [self.image(i) if not e else None for i, e in enumerate(errs)], errs
 
     def stats(self) -> dict:
-        a = (C.c_int64 * 14)()
+        a = (C.c_int64 * 16)()
         self.lib.cjBatchStats(self.ptr, a)
         return dict(zip(self.STAT_KEYS, [int(v) for v in a]))
 

@@ -76,9 +76,18 @@ struct CJBatchCtl {
   int passes;
   int pad;
   int next_sync, next_write, next_fix[3];  // dynamic work counters
-  int pad2[3];
-  unsigned long long t[BT_NPHASE + 1];  // %globaltimer (ns) at each phase start (CTA 0)
+  unsigned pix_done;                      // pixel-kernel CTAs finished
+  int pad2[2];
+  // %globaltimer (ns) at each phase start (CTA 0); t[BT_NPHASE] = end of the
+  // pixel kernel (its last CTA)
+  unsigned long long t[BT_NPHASE + 1];
 };
+
+__device__ __forceinline__ void bt_stamp_any(CJBatchCtl* ctl, int k) {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  ctl->t[k] = t;
+}
 
 __device__ __forceinline__ void bt_stamp(CJBatchCtl* ctl, int k) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -595,6 +604,9 @@ static bt_decode_fn bt_decode_kernel(int ctas_per_sm) {
   }
 }
 
+__device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int t1, uint8_t* smem,
+                                               uint64_t* bar2, CJPixSmemParams* Pp);
+
 // Phase 9 runs as its own kernel, launched right after k_decode_batch on the
 // same stream: the pixel work needs no grid barrier, and on its own it runs
 // at the occupancy of its 32-40 registers per thread instead of the entropy
@@ -615,6 +627,15 @@ __global__ void __launch_bounds__(CJ_PIX_THREADS, 6) k_pixel_batch(CJBatchArgs a
   // tile geometry is rebuilt only when it changes.
   const int per = (a.nptiles + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(t0 + per, a.nptiles);
+  if (t0 < t1) bt_pixel_tiles(a, t0, t1, smem, bar2, &P);
+  __syncthreads();
+  if (threadIdx.x == 0 && atomicAdd(&a.ctl->pix_done, 1) == gridDim.x - 1) bt_stamp_any(a.ctl, BT_NPHASE);
+}
+
+// Tiles [t0, t1) of one pixel-kernel CTA.
+__device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int t1, uint8_t* smem,
+                                               uint64_t* bar2, CJPixSmemParams* Pp) {
+  CJPixSmemParams& P = *Pp;
   auto advance = [&](int tt, int i) {
     while (tt >= a.desc[i].ptile0 + a.desc[i].nptiles) i++;
     return i;
@@ -643,7 +664,6 @@ __global__ void __launch_bounds__(CJ_PIX_THREADS, 6) k_pixel_batch(CJBatchArgs a
     cj_pixel_issue(a.coef + a.desc[i].coef0 * 64, gg, local / gx, (local % gx) * gg.T,
                    reinterpret_cast<int16_t*>(smem + which * gg.sc1_off), &bar2[which]);
   };
-  if (t0 >= t1) return;
   int img = bt_find(a.n, t0, [&](int k) { return a.desc[k].ptile0; });
   int pimg = img;  // image of the tile being prefetched (thread 0)
   if (threadIdx.x == 0) issue(t0, img, 0);
@@ -698,7 +718,7 @@ struct CJBatch {
   std::vector<int> dims;       // width, height, channels per device slot
   std::vector<int64_t> outoff; // output offset per device slot
   int ntiles = 0, nwarps = 0, nptiles = 0;
-  int64_t blob_bytes = 0, out_total = 0;
+  int64_t blob_bytes = 0, out_total = 0, blocks = 0, scan_bytes = 0;
   size_t smem = 0, smem_pix = 0;
   int grid = 0, grid_pix = 0;
   long long launches = 0;
@@ -937,6 +957,8 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   b->nptiles = nptiles;
   b->blob_bytes = blob_bytes;
   b->out_total = out_total;
+  b->blocks = blocks;
+  b->scan_bytes = data_bytes;
   b->smem = (size_t)BT_THREADS * sizeof(CJAgg5);
   b->smem_pix = smem;
   if (!nd) return 0;
@@ -1179,12 +1201,11 @@ void* cjBatchStream(const CJBatch* b) { return (void*)b->stream; }
 int cjBatchPhaseTimes(const CJBatch* b, float* ms) {
   const CJBatchCtl* ctl = (const CJBatchCtl*)b->h_ctl.p;
   if (!ctl) return 0;
-  float total = cjBatchKernelMs(b);
-  for (int k = 0; k < BT_NPHASE; k++) {
-    if (k + 1 < BT_NPHASE) ms[k] = (float)((ctl->t[k + 1] - ctl->t[k]) * 1e-6);
-    else ms[k] = total - (float)((ctl->t[k] - ctl->t[0]) * 1e-6);
-  }
-  return BT_NPHASE;
+  const float total = cjBatchKernelMs(b);
+  for (int k = 0; k < BT_NPHASE; k++) ms[k] = (float)((ctl->t[k + 1] - ctl->t[k]) * 1e-6);
+  // the rest of the run: graph launch, control-block clear, kernel boundaries
+  ms[BT_NPHASE] = total - (float)((ctl->t[BT_NPHASE] - ctl->t[0]) * 1e-6);
+  return BT_NPHASE + 1;
 }
 
 void cjBatchStats(const CJBatch* b, int64_t* s) {
@@ -1203,6 +1224,8 @@ void cjBatchStats(const CJBatch* b, int64_t* s) {
   s[11] = b->grid_pix;
   s[12] = b->graph_launches;
   s[13] = b->graph_failures;
+  s[14] = b->blocks;
+  s[15] = b->scan_bytes;
 }
 
 float cjBatchKernelMs(const CJBatch* b) {

@@ -138,17 +138,20 @@ const unsigned char *cjBatchDeviceImage(const CJBatch *b, int i);
  * cjBatchStage); PROGRAMMER_ERROR if image i was rejected by the host parse. */
 int cjBatchImageGeometry(const CJBatch *b, int i, int *width, int *height, int *channels);
 void *cjBatchStream(const CJBatch *b);
-/* stats[0..13]: images submitted, images on the device, decode-kernel CTAs,
+/* stats[0..15]: images submitted, images on the device, decode-kernel CTAs,
  * warp items, destuff tiles, pixel tiles, fix-up passes of the last run,
  * input bytes, output bytes, pixel-kernel dynamic shared memory, kernel
  * launches so far, pixel-kernel CTAs, runs launched as a CUDA graph, graph
- * builds that failed (those runs used plain launches). */
+ * builds that failed (those runs used plain launches), coefficient blocks,
+ * entropy-coded bytes on the device (16-byte padded per image). */
 void cjBatchStats(const CJBatch *b, int64_t *stats);
 /* Device time of the last cjBatchRun, in milliseconds. */
 float cjBatchKernelMs(const CJBatch *b);
-/* Split of the last run (after cjBatchWait) into its 10 phases, in ms:
+/* Split of the last run (after cjBatchWait), in ms: its 10 phases --
  * tables, destuff-count, tile-scan, destuff-scatter, segments, sync, fix-up,
- * warp-scan, write, pixel.  Returns the number of entries. */
+ * warp-scan, write (the decode kernel), pixel (the pixel kernel) -- and the
+ * remainder of the run (graph launch, control-block clear, the boundary
+ * between the kernels).  Returns the number of entries (11). */
 int cjBatchPhaseTimes(const CJBatch *b, float *ms);
 
 /* ---- Decoding without allocating: cjDecodeNoAlloc ----
