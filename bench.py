@@ -87,6 +87,9 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--split", action="store_true",
+                    help="under torchrun: partition one batch across ranks (strong scaling) "
+                         "instead of one batch per rank (weak scaling)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default batch tuning")
     ap.add_argument("--tuning", default="",
                     help="fixed batch tuning SUB_BITS,CTAS_PER_SM,TILE_CAP instead of the autotuner")
@@ -96,13 +99,21 @@ def parse_args():
 
 
 class Workload:
-    """The files of one step, their pixel count and the JSON `config`."""
+    """The files of one step, their pixel count and the JSON `config`.
+    Under torchrun the mixed batch is per rank: its own seed (weak scaling)
+    or its share of one batch (strong scaling, --split)."""
 
-    def __init__(self, name: str, batch_size: int):
+    def __init__(self, name: str, batch_size: int, rank: int = 0, world: int = 1, split: bool = False):
+        from cudajpeg_b200 import replicas as R
         from cudajpeg_b200 import workloads as W
         self.name = name
         if name == "mixed_batch":
-            samples = W.mixed_batch(n=batch_size, workers=min(32, os.cpu_count() or 1))
+            workers = max(1, min(32, (os.cpu_count() or 1) // world))
+            seed = 4 if split else R.rank_seed(4, rank)
+            samples = W.mixed_batch(n=batch_size, seed=seed, workers=workers)
+            if split and world > 1:
+                share = R.partition([s.pixels for s in samples], world)[rank]
+                samples = [samples[i] for i in share]
             self.config = {"workload": f"mixed_batch_{batch_size}", "images": batch_size,
                            "sides": "log-uniform [64, 2048], multiples of 8",
                            "subsampling": "4:2:0/4:2:2/4:4:4/grey p=.6/.2/.1/.1",
@@ -347,6 +358,7 @@ def run_batch(args, wl, world, rank, local, dist):
     import torch
 
     import cudajpeg_b200 as cj
+    from cudajpeg_b200 import replicas as R
 
     blob, offsets, sizes = cj.Batch.pack(wl.files)
     src = torch.empty(len(blob), dtype=torch.uint8, pin_memory=True)
@@ -397,12 +409,11 @@ def run_batch(args, wl, world, rank, local, dist):
     if dist:
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * wl.pixels * args.steps / (total_ms / 1e3) / 1e6
+    # whole job: pixels of all ranks / the slowest rank's device time
+    total_ms = R.max_over_ranks(sum(step_ms), dist, "cuda")
+    job_pixels = R.sum_over_ranks(wl.pixels, dist, "cuda")
+    job_file_bytes = R.sum_over_ranks(wl.file_bytes, dist, "cuda")
+    value = job_pixels * args.steps / (total_ms / 1e3) / 1e6
 
     # end to end: host parse + H2D of the pinned blob + decode + D2H of all images
     e2e_ms = []
@@ -416,12 +427,8 @@ def run_batch(args, wl, world, rank, local, dist):
         if any(b.wait()):
             raise RuntimeError("batch decode errors")
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
-    e2e_total = sum(e2e_ms)
-    if dist:
-        t = torch.tensor([e2e_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * wl.pixels * args.steps / (e2e_total / 1e3) / 1e6
+    e2e_total = R.max_over_ranks(sum(e2e_ms), dist, "cuda")
+    e2e_value = job_pixels * args.steps / (e2e_total / 1e3) / 1e6
     st = b.stats()
     b.close()
 
@@ -444,11 +451,14 @@ def run_batch(args, wl, world, rank, local, dist):
     lat = sorted(e2e_ms)
     line = {"metric": METRIC, "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean_ms, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u8/int16/int32", "data": "synthetic",
-            "config": dict(wl.config, parallelism=f"replicas{world}",
+            "higher_is_better": True, "scaling": "strong" if args.split else "weak",
+            "vs_baseline": None, "dtype": "u8/int16/int32", "data": "synthetic",
+            "config": dict(wl.config,
+                           parallelism=(f"split{world}: one batch partitioned by pixels" if args.split
+                                        else f"shards{world}: one batch per rank, seed 4 + rank"),
                            l2="working set ~1.6 GB per step, larger than L2 (126 MB)",
-                           compressed_MB_per_s=round(world * wl.file_bytes * args.steps
+                           job_MPix=round(job_pixels / 1e6, 3),
+                           compressed_MB_per_s=round(job_file_bytes * args.steps
                                                      / (total_ms / 1e3) / 1e6, 1),
                            passes=st["passes"], grid_ctas=st["grid"], warp_items=st["warp_items"],
                            pixel_ctas=st["pixel_grid"],
@@ -488,6 +498,7 @@ def run_single(args, wl, world, rank, local, dist):
     import torch
 
     import cudajpeg_b200 as cj
+    from cudajpeg_b200 import replicas as R
 
     sample = wl.samples[0]
     n = len(sample.data)
@@ -532,11 +543,9 @@ def run_single(args, wl, world, rank, local, dist):
         raise RuntimeError("device decode reported an error")
     reader.set_profile(False)
     total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * wl.pixels * args.steps / (total_ms / 1e3) / 1e6
+    total_ms = R.max_over_ranks(total_ms, dist, "cuda")
+    job_pixels = R.sum_over_ranks(wl.pixels, dist, "cuda")  # each rank decodes its own copy
+    value = job_pixels * args.steps / (total_ms / 1e3) / 1e6
     e2e_ms = []
     if dist:
         dist.barrier()
@@ -548,11 +557,8 @@ def run_single(args, wl, world, rank, local, dist):
         reader.open_bytes((src.data_ptr(), n))
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e_total = sum(e2e_ms)
-    if dist:
-        t = torch.tensor([e2e_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * wl.pixels * args.steps / (e2e_total / 1e3) / 1e6
+    e2e_total = R.max_over_ranks(e2e_total, dist, "cuda")
+    e2e_value = job_pixels * args.steps / (e2e_total / 1e3) / 1e6
     lat = sorted(e2e_ms)
     means = {k: statistics.mean(v) for k, v in kern_ms.items()}
     dom = max(means, key=means.get)
@@ -690,11 +696,11 @@ def run_precision(args):
 
 def run_gpu(args):
     import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from cudajpeg_b200 import replicas as R
+    rank, local, world = R.rank_env()
     # the workload is generated in a spawn-started pool before CUDA starts
-    wl = Workload(args.workload, args.batch_size)
+    wl = Workload(args.workload, args.batch_size, rank, world, args.split)
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
