@@ -51,7 +51,7 @@ EXPORTED = [
     "cjDecodeNoAlloc", "cjBatchImageGeometry",
     "cjServerCreate", "cjServerDestroy", "cjServerSubmit", "cjServerWait", "cjServerCopyOut",
     "cjServerRelease", "cjServerStats", "cjServerReplay", "cjServerSetTuning",
-    "cjBatchSetTuning", "cjBatchGetTuning", "cjBatchAutotune",
+    "cjBatchSetTuning", "cjBatchGetTuning", "cjBatchAutotune", "cjDebugStepTable",
 ]
 
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
@@ -106,6 +106,7 @@ def load(build_if_missing: bool = True):
                                 C.c_int, C.c_int, vp]
     lib.cjIDCTBlocksRaw.argtypes = [vp, C.c_longlong, vp, vp, C.c_int, vp]
     lib.cjDebugHuffDecode.argtypes = [vp, vp, C.c_uint]
+    lib.cjDebugStepTable.argtypes = [vp, vp, C.c_int, vp]
     lib.cjReaderRedecodeDevice.argtypes = [vp]
     lib.cjReaderSync.argtypes = [vp]
     lib.cjReaderDevicePixels.restype = vp

@@ -3,6 +3,7 @@
 
 #include "../../include/cudajpeg.h"
 #include "cj_internal.h"
+#include <new>
 #include "cj_tables.h"
 
 extern "C" {
@@ -108,6 +109,22 @@ int cjDebugHuffDecode(const unsigned char counts[16], const unsigned char* symbo
   CJHuff t;
   cj_build_huff(counts, symbols, &t);
   return (int)cj_huff_decode(t, win16 & 0xFFFF);
+}
+
+int cjDebugStepTable(const unsigned char counts[16], const unsigned char* symbols, int ac,
+                     unsigned short* out) {
+  CJScanParams* sp = new (std::nothrow) CJScanParams;
+  if (!sp || !out) {
+    delete sp;
+    return PROGRAMMER_ERROR;
+  }
+  memset(sp, 0, sizeof(*sp));
+  const int slot = ac ? 2 : 0;
+  cj_build_huff(counts, symbols, &sp->huff[slot]);
+  cj_build_steps(sp->huff[slot], counts, true, slot, &sp->steps);
+  for (uint32_t w = 0; w < 65536; w++) out[w] = (unsigned short)cj_step(*sp, slot, w << 16);
+  delete sp;
+  return 0;
 }
 
 }  // extern "C"

@@ -232,6 +232,23 @@ __device__ void bt_build_params(const CJImageHeader& h, CJScanParams& p) {
     p.huff[slot].maxcode[17] = -1;
     p.huff[slot].valoff[17] = 0;
   }
+  // decode steps from the finished canonical tables (cj_build_steps)
+  __syncthreads();
+  for (int e = threadIdx.x; e < 4 * (1 << CJ_FAST_BITS); e += blockDim.x) {
+    const int slot = e >> CJ_FAST_BITS, f = e & ((1 << CJ_FAST_BITS) - 1);
+    int pmin = 1 << CJ_FAST_BITS, pmax = -1;
+    const bool defined = (h.huff_mask & (1 << slot)) != 0;
+    if (defined) cj_long_prefixes(h.counts[slot], &pmin, &pmax);
+    p.steps.pri[slot][f] = defined ? cj_step_primary(p.huff[slot], pmin, pmax, f, slot >= 2) : (uint16_t)CJ_STEP_BAD;
+  }
+  for (int e = threadIdx.x; e < 4 * CJ_STEP_SUBS * 64; e += blockDim.x) {
+    const int slot = e / (CJ_STEP_SUBS * 64), i = (e >> 6) % CJ_STEP_SUBS, j = e & 63;
+    int pmin = 1 << CJ_FAST_BITS, pmax = -1;
+    const bool defined = (h.huff_mask & (1 << slot)) != 0;
+    if (defined) cj_long_prefixes(h.counts[slot], &pmin, &pmax);
+    p.steps.sub[slot][i][j] =
+        defined && pmin + i <= pmax ? cj_step_sub(p.huff[slot], pmin, i, j, slot >= 2) : (uint16_t)CJ_STEP_BAD;
+  }
   for (int e = threadIdx.x; e < 4 * 64; e += blockDim.x) p.qnat[e >> 6][c_bt_zz[e & 63]] = h.dq[e >> 6][e & 63];
   if (threadIdx.x < 64) p.zz[threadIdx.x] = c_bt_zz[threadIdx.x];
   if (threadIdx.x == 0) {

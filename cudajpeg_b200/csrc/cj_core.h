@@ -39,9 +39,33 @@ struct CJHuff {
   uint8_t vals[256];
 };
 
+// Decode steps: the per-symbol work of the entropy decoder, tabulated.
+// Entry for a Huffman table slot and the next 10 bits of the stream:
+//   bits 0-4   bits the symbol consumes: code length + magnitude size
+//   bits 5-11  advance of the zig-zag position: DC 1 (from -1 to 0), AC
+//              run + 1, ZRL 16, EOB 64, invalid AC symbol 96, no code 97
+//   bits 12-15 magnitude size (extra bits that carry the value)
+// An entry consuming 0 bits is a pointer: bits 5-15 index a 64-entry
+// subtable for the following 6 bits (codes of 11-16 bits), or are
+// CJ_STEP_SEARCH when the table has more long-code prefixes than subtables
+// (the canonical search then decodes the code).  Long codes of a canonical
+// table are the last codes of the code space, so their 10-bit prefixes form
+// one contiguous range [pmin, pmax]: subtable i serves prefix pmin + i.
+#define CJ_STEP_SUBS 16
+#define CJ_STEP_SEARCH 0x7FFu
+#define CJ_STEP_EOB 64u
+#define CJ_STEP_BAD_AC 96u
+#define CJ_STEP_NO_CODE 97u
+#define CJ_STEP_BAD (1u | (CJ_STEP_NO_CODE << 5))  // consume 1 bit, end the block
+struct CJSteps {
+  uint16_t pri[4][1 << CJ_FAST_BITS];
+  uint16_t sub[4][CJ_STEP_SUBS][64];
+};
+
 // Per-scan parameters, built on the host after SOS and copied once.
 struct alignas(16) CJScanParams {
   CJHuff huff[4];                 // DC0, DC1, AC0, AC1
+  CJSteps steps;                  // the same four tables as decode steps
   int16_t qnat[4][64];            // quantisation tables, natural order
   uint8_t phase_comp[CJ_MAX_BPM]; // component of the k-th block of an MCU
   uint8_t phase_blk[CJ_MAX_BPM];  // index of that block inside its component's MCU part
@@ -139,15 +163,73 @@ CJ_HD uint32_t cj_peek32(const uint32_t* words, uint64_t p, uint64_t end_byte) {
 
 // Decode one Huffman code from a left-aligned 16-bit window.  Returns
 // (len << 8) | symbol, or 0 when no code of length 1..16 matches.
-CJ_HD uint32_t cj_huff_decode(const CJHuff& t, uint32_t win16) {
-  uint32_t e = t.fast[win16 >> (16 - CJ_FAST_BITS)];
-  if (e) return e;
+// Codes longer than CJ_FAST_BITS: canonical search by length.
+CJ_HD uint32_t cj_huff_slow(const CJHuff& t, uint32_t win16) {
   for (int l = CJ_FAST_BITS + 1; l <= 16; l++) {
     int32_t code = (int32_t)(win16 >> (16 - l));
     if (code <= t.maxcode[l]) return ((uint32_t)l << 8) | t.vals[(t.valoff[l] + code) & 255];
   }
   return 0;
 }
+
+CJ_HD uint32_t cj_huff_decode(const CJHuff& t, uint32_t win16) {
+  uint32_t e = t.fast[win16 >> (16 - CJ_FAST_BITS)];
+  if (e) return e;
+  return cj_huff_slow(t, win16);
+}
+
+// Decode step of a decoded (len << 8 | symbol) from a DC (ac = false) or AC table.
+CJ_HD uint32_t cj_step_of(uint32_t e, bool ac) {
+  if (!e) return CJ_STEP_BAD;
+  const uint32_t len = e >> 8, sym = e & 255, size = sym & 15, run = sym >> 4;
+  const uint32_t dk = !ac ? 1u : (size ? run + 1 : (sym == 0 ? CJ_STEP_EOB : (sym == 0xF0 ? 16u : CJ_STEP_BAD_AC)));
+  return (len + size) | (dk << 5) | (size << 12);
+}
+
+// 10-bit prefixes of the codes longer than 10 bits, from the DHT counts
+// (canonical assignment, T.81 Annex C); *pmin > *pmax when there are none.
+CJ_HD void cj_long_prefixes(const uint8_t counts[16], int* pmin, int* pmax) {
+  int code = 0;
+  *pmin = 1 << CJ_FAST_BITS;
+  *pmax = -1;
+  for (int l = 1; l <= 16; l++) {
+    const int n = counts[l - 1];
+    if (l > CJ_FAST_BITS && n) {
+      const int a = code >> (l - CJ_FAST_BITS), b = (code + n - 1) >> (l - CJ_FAST_BITS);
+      if (a < *pmin) *pmin = a;
+      if (b > *pmax) *pmax = b;
+    }
+    code = (code + n) << 1;
+  }
+}
+
+// Primary step entry for prefix p of table t (its fast table already built).
+CJ_HD uint16_t cj_step_primary(const CJHuff& t, int pmin, int pmax, int p, bool ac) {
+  const uint32_t e = t.fast[p];
+  if (e) return (uint16_t)cj_step_of(e, ac);
+  if (p < pmin || p > pmax) return (uint16_t)CJ_STEP_BAD;
+  const uint32_t i = (uint32_t)(p - pmin);
+  return (uint16_t)((i < CJ_STEP_SUBS ? i : CJ_STEP_SEARCH) << 5);
+}
+
+// Entry j of subtable s (prefix pmin + s) of table t.
+CJ_HD uint16_t cj_step_sub(const CJHuff& t, int pmin, int s, int j, bool ac) {
+  const uint32_t win = ((uint32_t)(pmin + s) << 6) | (uint32_t)j;
+  if (pmin + s >= (1 << CJ_FAST_BITS)) return (uint16_t)CJ_STEP_BAD;
+  return (uint16_t)cj_step_of(cj_huff_slow(t, win), ac);
+}
+
+// The decode step for the 32-bit window v (MSB = next bit) of table `slot`.
+CJ_HD uint32_t cj_step(const CJScanParams& sp, uint32_t slot, uint32_t v) {
+  uint32_t st = sp.steps.pri[slot][v >> (32 - CJ_FAST_BITS)];
+  if (!(st & 31)) {
+    const uint32_t i = st >> 5;
+    st = i != CJ_STEP_SEARCH ? sp.steps.sub[slot][i][(v >> 16) & 63]
+                             : cj_step_of(cj_huff_slow(sp.huff[slot], v >> 16), slot >= 2);
+  }
+  return st;
+}
+
 
 // Sign extension of a `size`-bit magnitude category value (T.81 F.2.2.1).
 CJ_HD int32_t cj_extend(uint32_t bits, uint32_t size) {

@@ -96,24 +96,88 @@ __device__ __forceinline__ CJLane cj_lane(const CJSegment* segs, int nseg, int n
   return l;
 }
 
+// Bit reader of the decode loops: the current and the next big-endian word
+// and a bit offset; a 32-bit window is one funnel shift, and a word boundary
+// is crossed at most once per symbol (a symbol consumes at most 31 bits).
+// Bytes at or past `end_byte` read as 0xFF, as in CJBits.
+struct CJFBits {
+  const uint32_t* words;
+  uint32_t wfull, end_byte, cur, nxt, wi, off;
+
+  __device__ __forceinline__ uint32_t word(uint32_t i) const {
+    return i < wfull ? cj_bswap(words[i]) : cj_word(words, i, end_byte);
+  }
+  __device__ __forceinline__ void init(const uint32_t* w, uint64_t eb, uint64_t p) {
+    words = w;
+    end_byte = (uint32_t)eb;
+    wfull = (uint32_t)(eb >> 2);
+    const uint32_t w0 = (uint32_t)(p >> 5);
+    off = (uint32_t)(p & 31);
+    cur = word(w0);
+    wi = w0 + 1;
+    nxt = word(wi);
+  }
+  __device__ __forceinline__ uint32_t peek() const { return __funnelshift_l(nxt, cur, off); }
+  __device__ __forceinline__ void skip(uint32_t u) {
+    off += u;
+    if (off >= 32) {
+      off -= 32;
+      cur = nxt;
+      wi++;
+      nxt = word(wi);
+    }
+  }
+  __device__ __forceinline__ uint64_t pos() const { return ((uint64_t)(wi - 1) << 5) + off; }
+};
+
 // Speculative decode of one subsequence from `start`: blocks beginning
 // before the subsequence's end, their DC sums, and the state after them.
+// One Huffman symbol per iteration through the decode-step tables (CJSteps):
+// bits consumed, zig-zag advance and magnitude size come from one lookup, so
+// DC and AC symbols of all lanes take the same instructions; a block ends
+// when the position passes 62 (EOB and invalid symbols advance by >= 64).
+// The DC symbol's window is kept and its difference added when the block
+// ends.  Symbol for symbol this is cj_block: a failing block is counted and
+// decoding goes on after the bits the failing symbol consumed.
 __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const uint32_t* words,
                                                    const CJLane& ln, uint64_t start) {
-  CJBits br;
+  CJFBits br;
   br.init(words, ln.end_byte, cj_state_bit(start));
   uint32_t m = cj_state_phase(start);
-  int nb = 0, d0 = 0, d1 = 0, d2 = 0;
-  CJNullSink ns;
-  while (br.pos() < ln.end) {
-    int c = sp.phase_comp[m];
-    int32_t dd;
-    cj_block(br, sp.huff[sp.comp_dc[c]], sp.huff[sp.comp_ac[c]], sp.zz, &dd, ns);
-    d0 += (c == 0) ? dd : 0;
-    d1 += (c == 1) ? dd : 0;
-    d2 += (c == 2) ? dd : 0;
-    nb++;
-    m = (m + 1 == (uint32_t)sp.bpm) ? 0 : m + 1;
+  int c = sp.phase_comp[m];
+  uint32_t aslot = sp.comp_ac[c], slot = sp.comp_dc[c];
+  int k = -1, nb = 0, d0 = 0, d1 = 0, d2 = 0;
+  uint32_t dcv = 0, dcst = 0;
+  int rem = (int)((int64_t)ln.end - (int64_t)cj_state_bit(start));
+  if (rem > 0) {
+    for (;;) {
+      const uint32_t v = br.peek();
+      const uint32_t st = cj_step(sp, slot, v);
+      const int kn = k + (int)((st >> 5) & 127);
+      const uint32_t used = (st & 31) - (kn > 63 ? (st >> 12) : 0u);
+      const bool isdc = k < 0;
+      dcv = isdc ? v : dcv;
+      dcst = isdc ? st : dcst;
+      br.skip(used);
+      rem -= (int)used;
+      slot = aslot;
+      if (kn >= 63) {
+        const uint32_t size = dcst >> 12, len = (dcst & 31) - size;
+        const int dd = size ? cj_extend((dcv << len) >> (32 - size), size) : 0;
+        if (c == 0) d0 += dd;
+        else if (c == 1) d1 += dd;
+        else d2 += dd;
+        k = -1;
+        nb++;
+        m = (m + 1 == (uint32_t)sp.bpm) ? 0 : m + 1;
+        c = sp.phase_comp[m];
+        aslot = sp.comp_ac[c];
+        slot = sp.comp_dc[c];
+        if (rem <= 0) break;
+      } else {
+        k = kn;
+      }
+    }
   }
   CJSubRec r;
   r.start = start;
@@ -225,13 +289,19 @@ __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint
                                               CJStatus* st, const uint8_t* zz) {
   int64_t b = first_block;
   const int64_t bend = seg.first_block + seg.nblocks;
-  CJBits br;
+  const uint64_t seg_end = seg.bit_end;
+  CJFBits br;
   br.init(words, ln.end_byte, cj_state_bit(r.start));
   uint32_t m = cj_state_phase(r.start);
-  const uint64_t seg_end = seg.bit_end;
-  for (;;) {
+  int c = sp.phase_comp[m];
+  uint32_t aslot = sp.comp_ac[c], slot = sp.comp_dc[c];
+  int k = -1;
+  int32_t dd = 0;
+  int16_t* blk = coef;
+  // the structural checks made before every block; false = stop here
+  auto block_start = [&]() -> bool {
     const uint64_t p = br.pos();
-    if (!ln.last && p >= ln.end) break;
+    if (!ln.last && p >= ln.end) return false;
     if (b >= bend) {
       if (!ln.last) cj_raise_dec(st, b, CJ_DEV_EXTRA);
       else if (seg.marker_follows) {
@@ -239,38 +309,58 @@ __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint
       } else if (ln.end_byte > ((p + 7) >> 3) + 2) {
         cj_raise_dec(st, b, CJ_DEV_TRAILING);
       }
-      break;
+      return false;
     }
     if (seg.marker_follows && p >= seg_end) {
       cj_raise_dec(st, b, CJ_DEV_OVERRUN);
-      break;
+      return false;
     }
-    int c = sp.phase_comp[m];
-    int16_t* blk = coef + b * 64;
-    uint4 z = make_uint4(0, 0, 0, 0);
+    blk = coef + b * 64;
+    const uint4 z = make_uint4(0, 0, 0, 0);
 #pragma unroll
-    for (int k = 0; k < 8; k++) reinterpret_cast<uint4*>(blk)[k] = z;
-    CJCoefSink sink{blk};
-    int32_t dd;
-    int err = cj_block(br, sp.huff[sp.comp_dc[c]], sp.huff[sp.comp_ac[c]], zz, &dd, sink);
-    if (err) {
-      cj_raise_dec(st, b, err);
-      break;
+    for (int q = 0; q < 8; q++) reinterpret_cast<uint4*>(blk)[q] = z;
+    return true;
+  };
+  if (!block_start()) return;
+  for (;;) {
+    const uint32_t v = br.peek();
+    const uint32_t stp = cj_step(sp, slot, v);
+    const uint32_t dk = (stp >> 5) & 127, size = stp >> 12, total = stp & 31;
+    const int kn = k + (int)dk;
+    const uint32_t len = total - size;
+    const int32_t val = size ? cj_extend((v << len) >> (32 - size), size) : 0;
+    if (k < 0) dd = val;
+    else if (size && kn <= 63) blk[zz[kn]] = (int16_t)val;
+    br.skip(total - (kn > 63 ? size : 0u));
+    slot = aslot;
+    if (kn < 63) {
+      k = kn;
+      continue;
     }
+    if (kn > 63 && dk != CJ_STEP_EOB) {  // failing symbol: the block is cut here
+      cj_raise_dec(st, b, dk == CJ_STEP_NO_CODE ? CJ_DEV_BAD_CODE : CJ_DEV_BAD_AC);
+      return;
+    }
+    // block complete
     if (seg.marker_follows && br.pos() > seg_end) {
       cj_raise_dec(st, b, CJ_DEV_OVERRUN);
-      break;
+      return;
     }
-    int v;
-    if (c == 0) v = dc0 += dd;
-    else if (c == 1) v = dc1 += dd;
-    else v = dc2 += dd;
-    if (v < -32768 || v > 32767) {
+    int dcv;
+    if (c == 0) dcv = dc0 += dd;
+    else if (c == 1) dcv = dc1 += dd;
+    else dcv = dc2 += dd;
+    if (dcv < -32768 || dcv > 32767) {
       cj_raise_dec(st, b, CJ_DEV_DC_RANGE);
-      break;
+      return;
     }
-    blk[0] = (int16_t)v;
+    blk[0] = (int16_t)dcv;
     b++;
     m = (m + 1 == (uint32_t)sp.bpm) ? 0 : m + 1;
+    c = sp.phase_comp[m];
+    aslot = sp.comp_ac[c];
+    slot = sp.comp_dc[c];
+    k = -1;
+    if (!block_start()) return;
   }
 }

@@ -34,3 +34,16 @@ inline void cj_build_huff(const uint8_t counts[16], const uint8_t* symbols, CJHu
   t->maxcode[17] = -1;
   t->valoff[17] = 0;
 }
+
+// Decode-step tables (CJSteps) of slot `slot` from its canonical table `t`
+// (already built) and DHT counts; an undefined slot decodes nothing.
+inline void cj_build_steps(const CJHuff& t, const uint8_t counts[16], bool defined, int slot, CJSteps* st) {
+  const bool ac = slot >= 2;
+  int pmin = 1 << CJ_FAST_BITS, pmax = -1;
+  if (defined) cj_long_prefixes(counts, &pmin, &pmax);
+  for (int p = 0; p < (1 << CJ_FAST_BITS); p++)
+    st->pri[slot][p] = defined ? cj_step_primary(t, pmin, pmax, p, ac) : (uint16_t)CJ_STEP_BAD;
+  for (int i = 0; i < CJ_STEP_SUBS; i++)
+    for (int j = 0; j < 64; j++)
+      st->sub[slot][i][j] = defined && pmin + i <= pmax ? cj_step_sub(t, pmin, i, j, ac) : (uint16_t)CJ_STEP_BAD;
+}

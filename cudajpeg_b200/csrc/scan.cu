@@ -433,8 +433,11 @@ k_decode_write(const CJScanParams* __restrict__ prm, const CJSegment* __restrict
 static void cj_fill_params(JPGReader* jpg, CJScanParams* hp) {
   CJReaderDevice* d = jpg->dev;
   memset(hp, 0, sizeof(*hp));
-  for (int s = 0; s < 4; s++)
-    if (jpg->huff_defined & (1 << s)) cj_build_huff(d->huff[s].counts, d->huff[s].symbols, &hp->huff[s]);
+  for (int s = 0; s < 4; s++) {
+    const bool defined = (jpg->huff_defined & (1 << s)) != 0;
+    if (defined) cj_build_huff(d->huff[s].counts, d->huff[s].symbols, &hp->huff[s]);
+    cj_build_steps(hp->huff[s], d->huff[s].counts, defined, s, &hp->steps);
+  }
   static const uint8_t zz[64] = CJ_ZIGZAG_INIT;
   memcpy(hp->zz, zz, 64);
   for (int t = 0; t < 4; t++)

@@ -81,6 +81,14 @@ long long cjReaderLaunchCount(const JPGReader *r);
 int cjDebugHuffDecode(const unsigned char counts[16], const unsigned char *symbols,
                       unsigned int win16);
 
+/* Host check of the decode-step tables the entropy kernels use: for every
+ * 16-bit window w, out[w] = the step entry for a DC (ac = 0) or AC table built
+ * from the DHT counts and symbols -- bits consumed (code + magnitude) in bits
+ * 0-4, zig-zag advance in bits 5-11 (DC 1, AC run + 1, ZRL 16, EOB 64,
+ * invalid symbol 96, no code 97), magnitude size in bits 12-15. */
+int cjDebugStepTable(const unsigned char counts[16], const unsigned char *symbols, int ac,
+                     unsigned short *out);
+
 /* ---- Batched decoder: many JPEGs in one persistent, cooperative kernel ----
  *
  * The files of a batch lie back to back in one host buffer `blob` (pinned

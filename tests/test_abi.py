@@ -117,6 +117,45 @@ def test_huffman_tables_match_reference_lut(cj):
         assert np.array_equal(got, ref[::7])
 
 
+def _step_of(e, ac):
+    """Decode-step entry of a (len << 8 | symbol) table entry."""
+    if not e:
+        return 1 | (97 << 5)
+    ln, sym = e >> 8, e & 255
+    size, run = sym & 15, sym >> 4
+    if not ac:
+        dk = 1
+    elif size:
+        dk = run + 1
+    else:
+        dk = 64 if sym == 0 else (16 if sym == 0xF0 else 96)
+    return (ln + size) | (dk << 5) | (size << 12)
+
+
+def test_decode_steps_match_reference_lut(cj):
+    """The two-level decode-step tables give, for every 16-bit window, the
+    bits consumed / zig-zag advance / magnitude size of the reference's 64K
+    table entry -- including tables with more long-code prefixes than
+    subtables, which fall back to the canonical search."""
+    lib = cj.load()
+    rng = np.random.default_rng(1)
+    annex_k_ac_luma = [0, 2, 1, 3, 3, 2, 4, 3, 5, 5, 4, 4, 0, 0, 1, 0x7D]
+    annex_k_dc_chroma = [0, 3, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0]
+    many_long = [0, 1, 1, 1, 1, 1, 1, 1, 1, 1, 120, 0, 0, 0, 0, 0]  # 120 codes of 11 bits: 60 prefixes
+    tables = [(annex_k_ac_luma, np.arange(162, dtype=np.uint8), True),
+              (annex_k_dc_chroma, np.arange(12, dtype=np.uint8), False),
+              (many_long, rng.integers(0, 256, sum(many_long)).astype(np.uint8), True)]
+    tables += [_random_table(rng) + (bool(k & 1),) for k in range(6)]
+    vstep = np.vectorize(_step_of)
+    for counts, symbols, ac in tables:
+        c = (C.c_ubyte * 16)(*counts)
+        s = np.ascontiguousarray(symbols, np.uint8)
+        out = np.zeros(65536, np.uint16)
+        assert lib.cjDebugStepTable(c, s.ctypes.data, int(ac), out.ctypes.data) == 0
+        want = vstep(_reference_lut(counts, s), ac).astype(np.uint16)
+        assert np.array_equal(out, want), (counts, ac, np.nonzero(out != want)[0][:5])
+
+
 def test_batch_tuning_validation_without_gpu(cj):
     """cjBatchSetTuning checks its arguments on the host (no device work)."""
     with cj.Batch() as b:
