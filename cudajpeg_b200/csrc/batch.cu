@@ -110,6 +110,7 @@ struct CJBatchArgs {
   uint8_t* mcode;
   CJSegment* segs;
   CJSubRec* recs;
+  CJCkpt* ckpt;
   uint64_t* snap0;
   uint64_t* snap1;
   CJWarpAgg* wagg;
@@ -232,23 +233,29 @@ __device__ void bt_build_params(const CJImageHeader& h, CJScanParams& p) {
     p.huff[slot].maxcode[17] = -1;
     p.huff[slot].valoff[17] = 0;
   }
-  // decode steps from the finished canonical tables (cj_build_steps)
+  // decode steps from the finished canonical tables (cj_build_steps); the
+  // long-code prefix range of each slot is computed once
+  __shared__ int s_pre[4][2];
+  if (threadIdx.x < 4) {
+    int pmin = 1 << CJ_FAST_BITS, pmax = -1;
+    if (h.huff_mask & (1 << threadIdx.x)) cj_long_prefixes(h.counts[threadIdx.x], &pmin, &pmax);
+    s_pre[threadIdx.x][0] = pmin;
+    s_pre[threadIdx.x][1] = pmax;
+  }
   __syncthreads();
   for (int e = threadIdx.x; e < 4 * (1 << CJ_FAST_BITS); e += blockDim.x) {
     const int slot = e >> CJ_FAST_BITS, f = e & ((1 << CJ_FAST_BITS) - 1);
-    int pmin = 1 << CJ_FAST_BITS, pmax = -1;
     const bool defined = (h.huff_mask & (1 << slot)) != 0;
-    if (defined) cj_long_prefixes(h.counts[slot], &pmin, &pmax);
-    p.steps.pri[slot][f] = defined ? cj_step_primary(p.huff[slot], pmin, pmax, f, slot >= 2) : (uint16_t)CJ_STEP_BAD;
+    p.steps.pri[slot][f] = defined ? cj_step_primary(p.huff[slot], s_pre[slot][0], s_pre[slot][1], f, slot >= 2)
+                                   : (uint16_t)CJ_STEP_BAD;
   }
   for (int e = threadIdx.x; e < 4 * CJ_STEP_SUBS * 64; e += blockDim.x) {
     const int slot = e / (CJ_STEP_SUBS * 64), i = (e >> 6) % CJ_STEP_SUBS, j = e & 63;
-    int pmin = 1 << CJ_FAST_BITS, pmax = -1;
-    const bool defined = (h.huff_mask & (1 << slot)) != 0;
-    if (defined) cj_long_prefixes(h.counts[slot], &pmin, &pmax);
-    p.steps.sub[slot][i][j] =
-        defined && pmin + i <= pmax ? cj_step_sub(p.huff[slot], pmin, i, j, slot >= 2) : (uint16_t)CJ_STEP_BAD;
+    const int pmin = s_pre[slot][0], pmax = s_pre[slot][1];
+    const bool used = (h.huff_mask & (1 << slot)) && pmin + i <= pmax;
+    p.steps.sub[slot][i][j] = used ? cj_step_sub(p.huff[slot], pmin, i, j, slot >= 2) : (uint16_t)CJ_STEP_BAD;
   }
+  __syncthreads();  // s_pre is reused by the next image of this CTA
   for (int e = threadIdx.x; e < 4 * 64; e += blockDim.x) p.qnat[e >> 6][c_bt_zz[e & 63]] = h.dq[e >> 6][e & 63];
   if (threadIdx.x < 64) p.zz[threadIdx.x] = c_bt_zz[threadIdx.x];
   if (threadIdx.x == 0) {
@@ -280,6 +287,7 @@ __device__ void bt_build_params(const CJImageHeader& h, CJScanParams& p) {
     p.restart_interval = h.restart_interval;
     p.nseg_expected = h.nseg_expected;
     p.total_blocks = h.total_blocks;
+    p.phase_pack = cj_phase_pack(p);
   }
 }
 
@@ -463,8 +471,10 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
     r.start = cj_state(ln.begin, 0);
     r.exit = r.start;
     r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
-    if (ln.active) r = cj_spec_decode(sp, words, ln, r.start);
-    cj_warp_settle(sp, words, ln, r, r.start);
+    CJCkpt* ck = cj_lane_ckpts(a.ckpt, d.sub0 + j0 + lane);
+    const uint32_t cs = cj_ckpt_step(d.sub_bits);
+    if (ln.active) r = cj_spec_decode<false>(sp, words, ln, r.start, ck, r, cs);
+    cj_warp_settle(sp, words, ln, r, r.start, ck, cs);
     if (ln.active) a.recs[d.sub0 + j0 + lane] = r;
     unsigned act = __ballot_sync(CJ_FULL, ln.active);
     if (lane == 31 - __clz(act)) a.snap0[w] = r.exit;
@@ -510,7 +520,9 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
         r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
       }
       uint64_t in0 = (j0 > 0 && lane == 0) ? __ldcg(&snap_in[w - 1]) : r.start;
-      if (cj_warp_settle(sp, words, ln, r, in0) && ln.active) a.recs[d.sub0 + j0 + lane] = r;
+      if (cj_warp_settle(sp, words, ln, r, in0, cj_lane_ckpts(a.ckpt, d.sub0 + j0 + lane),
+                         cj_ckpt_step(d.sub_bits)) && ln.active)
+        a.recs[d.sub0 + j0 + lane] = r;
       unsigned act = __ballot_sync(CJ_FULL, ln.active);
       if (lane == 31 - __clz(act)) {
         if (r.exit != __ldcg(&snap_in[w])) atomicAdd(unstable, 1);
@@ -604,8 +616,9 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
     int dc0, dc1, dc2;
     cj_warp_prefix(r, ln, __ldcg(&a.carry[w].nblocks), __ldcg(&a.carry[w].dc[0]),
                    __ldcg(&a.carry[w].dc[1]), __ldcg(&a.carry[w].dc[2]), &b, &dc0, &dc1, &dc2);
-    if (!ln.active) continue;
     const CJSegment seg = a.segs[d.seg0 + ln.seg];
+    cj_warp_zero_blocks(a.coef + d.coef0 * 64, ln, seg, r, b + seg.first_block);
+    if (!ln.active) continue;
     cj_write_lane(sp, words, ln, seg, r, b + seg.first_block, dc0, dc1, dc2,
                   a.coef + d.coef0 * 64, st, s_zz);
   }
@@ -724,7 +737,7 @@ struct CJBatch {
   int tile_cap = 0;                          // max MCUs per pixel tile (0 = layout maximum)
   JPGReader* parser = nullptr;  // host marker parse, one image at a time
   // device buffers (grow-only)
-  CJDevBuf hdr, desc, prm, st, blob, data, tile_keep, tile_mark, mpos, mcode, segs, recs, snap,
+  CJDevBuf hdr, desc, prm, st, blob, data, tile_keep, tile_mark, mpos, mcode, segs, recs, ckpt, snap,
       wagg, carry, coef, out, ctl;
   // pinned host staging
   CJHostBuf h_hdr, h_desc, h_out, h_st, h_ctl;
@@ -851,7 +864,7 @@ void cjBatchDestroy(CJBatch* b) {
     cudaStreamSynchronize(b->stream);
     CJDevBuf* bufs[] = {&b->hdr,  &b->desc, &b->prm,   &b->st,   &b->blob,  &b->data,
                         &b->tile_keep, &b->tile_mark, &b->mpos, &b->mcode, &b->segs,
-                        &b->recs, &b->snap, &b->wagg, &b->carry, &b->coef, &b->out, &b->ctl};
+                        &b->recs, &b->ckpt, &b->snap, &b->wagg, &b->carry, &b->coef, &b->out, &b->ctl};
     for (CJDevBuf* d : bufs)
       if (d->p) cudaFree(d->p);
     CJHostBuf* hb[] = {&b->h_hdr, &b->h_desc, &b->h_out, &b->h_st, &b->h_ctl};
@@ -987,6 +1000,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
       bt_ensure(b, b->mpos, (size_t)nmark * 4) || bt_ensure(b, b->mcode, (size_t)nmark) ||
       bt_ensure(b, b->segs, (size_t)nseg * sizeof(CJSegment)) ||
       bt_ensure(b, b->recs, (size_t)nsubw * 32 * sizeof(CJSubRec)) ||
+      bt_ensure(b, b->ckpt, (size_t)nsubw * 32 * CJ_CKPTS * sizeof(CJCkpt)) ||
       bt_ensure(b, b->snap, (size_t)2 * nsubw * sizeof(uint64_t)) ||
       bt_ensure(b, b->wagg, (size_t)nsubw * sizeof(CJWarpAgg)) ||
       bt_ensure(b, b->carry, (size_t)nsubw * sizeof(CJWarpAgg)) ||
@@ -1029,6 +1043,7 @@ static CJBatchArgs bt_args(const CJBatch* b) {
   a.mcode = (uint8_t*)b->mcode.p;
   a.segs = (CJSegment*)b->segs.p;
   a.recs = (CJSubRec*)b->recs.p;
+  a.ckpt = (CJCkpt*)b->ckpt.p;
   a.snap0 = (uint64_t*)b->snap.p;
   a.snap1 = a.snap0 + b->nwarps;
   a.wagg = (CJWarpAgg*)b->wagg.p;
@@ -1450,6 +1465,7 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   const size_t o_mpos = carve((size_t)d.mark_cap * 4), o_mcode = carve((size_t)d.mark_cap);
   const size_t o_segs = carve((size_t)d.seg_cap * sizeof(CJSegment));
   const size_t o_recs = carve((size_t)d.sub_cap * sizeof(CJSubRec));
+  const size_t o_ckpt = carve((size_t)d.sub_cap * CJ_CKPTS * sizeof(CJCkpt));
   const size_t o_snap = carve((size_t)2 * nwarps * sizeof(uint64_t));
   const size_t o_wagg = carve((size_t)nwarps * sizeof(CJWarpAgg));
   const size_t o_carry = carve((size_t)nwarps * sizeof(CJWarpAgg));
@@ -1488,6 +1504,7 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   a.mcode = base + o_mcode;
   a.segs = (CJSegment*)(base + o_segs);
   a.recs = (CJSubRec*)(base + o_recs);
+  a.ckpt = (CJCkpt*)(base + o_ckpt);
   a.snap0 = (uint64_t*)(base + o_snap);
   a.snap1 = a.snap0 + nwarps;
   a.wagg = (CJWarpAgg*)(base + o_wagg);

@@ -81,7 +81,20 @@ struct alignas(16) CJScanParams {
   int64_t total_blocks;              // mcux*mcuy*bpm
   int32_t comp_stride[3];            // plane strides (bytes) for plane outputs
   int32_t comp_rows[3];
+  // phases 0..bpm-1 of an MCU, 6 bits each: component | DC slot << 2 |
+  // AC slot << 4 (valid when bpm <= 10, the standard's limit)
+  uint64_t phase_pack;
 };
+
+// Component and DC / AC table slots of MCU phase m.
+CJ_HD uint64_t cj_phase_pack(const CJScanParams& p) {
+  uint64_t pack = 0;
+  for (int m = 0; m < p.bpm && m < 10; m++) {
+    const int c = p.phase_comp[m];
+    pack |= (uint64_t)(c | (p.comp_dc[c] << 2) | (p.comp_ac[c] << 4)) << (6 * m);
+  }
+  return pack;
+}
 
 // A restart interval (or the whole scan) in the destuffed buffer.
 struct CJSegment {

@@ -3,6 +3,7 @@
 // (batch.cu): destuff classification, subsequence lanes, speculative block
 // decode and the warp settle loop.
 #pragma once
+#include <limits.h>
 #include <stdint.h>
 
 #include "cj_core.h"
@@ -130,6 +131,33 @@ struct CJFBits {
   __device__ __forceinline__ uint64_t pos() const { return ((uint64_t)(wi - 1) << 5) + off; }
 };
 
+// Component, DC slot and AC slot of MCU phase m (from the packed phase
+// table; the per-phase arrays for MCUs of more than 10 blocks).
+__device__ __forceinline__ void cj_phase(const CJScanParams& sp, int bpm, uint64_t pack, uint32_t m, int& c,
+                                         uint32_t& dslot, uint32_t& aslot) {
+  if (bpm <= 10) {
+    const uint32_t f = (uint32_t)(pack >> (6 * m)) & 63;
+    c = (int)(f & 3);
+    dslot = (f >> 2) & 3;
+    aslot = f >> 4;
+  } else {
+    c = sp.phase_comp[m];
+    dslot = sp.comp_dc[c];
+    aslot = sp.comp_ac[c];
+  }
+}
+
+// Checkpoints of a subsequence decode: the decoder state at the first block
+// boundary at or after each of CJ_CKPTS thresholds (1/4, 1/2, 3/4 of the
+// subsequence): position relative to the subsequence start and MCU phase
+// (pp = phase << 24 | position), blocks begun before it, DC sums before it.
+// Thresholds the decode never passes get its exit state.
+#define CJ_CKPTS 3
+struct CJCkpt {
+  uint32_t pp;
+  int32_t nb, d0, d1, d2;
+};
+
 // Speculative decode of one subsequence from `start`: blocks beginning
 // before the subsequence's end, their DC sums, and the state after them.
 // One Huffman symbol per iteration through the decode-step tables (CJSteps):
@@ -139,17 +167,64 @@ struct CJFBits {
 // The DC symbol's window is kept and its difference added when the block
 // ends.  Symbol for symbol this is cj_block: a failing block is counted and
 // decoding goes on after the bits the failing symbol consumed.
+//
+// Checkpoints (`ck`, CJ_CKPTS of them) are written for every decode.  A
+// re-decode (RESUME) from a corrected start compares each checkpoint it
+// reaches with the previous decode's (`old`): when position and phase agree
+// the two decodes are identical from there on, so it stops and returns the
+// previous totals shifted by the difference in blocks and DC sums before that
+// point (shifting the later checkpoints too).  The result equals a full
+// decode from `start`.
+template <bool RESUME>
 __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const uint32_t* words,
-                                                   const CJLane& ln, uint64_t start) {
+                                                   const CJLane& ln, uint64_t start, CJCkpt* __restrict__ ck,
+                                                   const CJSubRec& old, uint32_t cstep) {
   CJFBits br;
   br.init(words, ln.end_byte, cj_state_bit(start));
   uint32_t m = cj_state_phase(start);
-  int c = sp.phase_comp[m];
-  uint32_t aslot = sp.comp_ac[c], slot = sp.comp_dc[c];
+  const int bpm = sp.bpm;
+  const uint64_t pack = sp.phase_pack;
+  int c;
+  uint32_t aslot, slot;
+  cj_phase(sp, bpm, pack, m, c, slot, aslot);
   int k = -1, nb = 0, d0 = 0, d1 = 0, d2 = 0;
   uint32_t dcv = 0, dcst = 0;
+  const uint32_t endrel = (uint32_t)(ln.end - ln.begin);
   int rem = (int)((int64_t)ln.end - (int64_t)cj_state_bit(start));
+  uint32_t j = 0, thresh = cstep;
+  CJSubRec r;
+  r.start = start;
+  // Checkpoints at the boundary `rel` bits into the subsequence; true when
+  // this decode has joined the previous one (r then holds the result).
+  auto checkpoint = [&](uint32_t rel, bool final) -> bool {
+    while (j < CJ_CKPTS && (final || rel >= thresh)) {
+      const uint32_t pp = (m << 24) | rel;
+      if (RESUME && !final) {
+        const CJCkpt o = ck[j];
+        if (o.pp == pp) {
+          const int dn = nb - o.nb, e0 = d0 - o.d0, e1 = d1 - o.d1, e2 = d2 - o.d2;
+          for (uint32_t q = j; q < CJ_CKPTS; q++) {
+            ck[q].nb += dn;
+            ck[q].d0 += e0;
+            ck[q].d1 += e1;
+            ck[q].d2 += e2;
+          }
+          r.exit = old.exit;
+          r.nblocks = old.nblocks + dn;
+          r.dc[0] = old.dc[0] + e0;
+          r.dc[1] = old.dc[1] + e1;
+          r.dc[2] = old.dc[2] + e2;
+          return true;
+        }
+      }
+      ck[j] = CJCkpt{pp, nb, d0, d1, d2};
+      j++;
+      thresh += cstep;
+    }
+    return false;
+  };
   if (rem > 0) {
+    if (checkpoint(endrel - (uint32_t)rem, false)) return r;
     for (;;) {
       const uint32_t v = br.peek();
       const uint32_t st = cj_step(sp, slot, v);
@@ -169,18 +244,17 @@ __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const
         else d2 += dd;
         k = -1;
         nb++;
-        m = (m + 1 == (uint32_t)sp.bpm) ? 0 : m + 1;
-        c = sp.phase_comp[m];
-        aslot = sp.comp_ac[c];
-        slot = sp.comp_dc[c];
+        m = (m + 1 == (uint32_t)bpm) ? 0 : m + 1;
+        cj_phase(sp, bpm, pack, m, c, slot, aslot);
         if (rem <= 0) break;
+        const uint32_t rel = endrel - (uint32_t)rem;
+        if (rel >= thresh && checkpoint(rel, false)) return r;
       } else {
         k = kn;
       }
     }
   }
-  CJSubRec r;
-  r.start = start;
+  checkpoint(0, true);
   r.exit = cj_state(br.pos(), m);
   r.nblocks = nb;
   r.dc[0] = d0;
@@ -189,11 +263,16 @@ __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const
   return r;
 }
 
+// Checkpoints of global lane `i` and the threshold spacing of a subsequence.
+__device__ __forceinline__ CJCkpt* cj_lane_ckpts(CJCkpt* base, int64_t i) { return base + i * CJ_CKPTS; }
+__device__ __forceinline__ uint32_t cj_ckpt_step(int sub_bits) { return (uint32_t)sub_bits / (CJ_CKPTS + 1); }
+
 // Re-decode lanes whose input state (lane 0: `lane0_in`; others: the exit of
 // the previous lane) differs from the state they last decoded from, until no
 // lane changes.  Lane l settles after at most l+1 re-decodes.
 __device__ __forceinline__ bool cj_warp_settle(const CJScanParams& sp, const uint32_t* words,
-                                               const CJLane& ln, CJSubRec& r, uint64_t lane0_in) {
+                                               const CJLane& ln, CJSubRec& r, uint64_t lane0_in,
+                                               CJCkpt* ck, uint32_t cstep) {
   int lane = threadIdx.x & 31;
   bool dirty = false;
   for (int it = 0; it < 34; it++) {
@@ -202,7 +281,7 @@ __device__ __forceinline__ bool cj_warp_settle(const CJScanParams& sp, const uin
     bool change = ln.active && want != r.start;
     if (!__any_sync(CJ_FULL, change)) break;
     if (change) {
-      r = cj_spec_decode(sp, words, ln, want);
+      r = cj_spec_decode<true>(sp, words, ln, want, ck, r, cstep);
       dirty = true;
     }
   }
@@ -278,6 +357,31 @@ __device__ __forceinline__ void cj_warp_prefix(const CJSubRec& r, const CJLane& 
   *d2 = e3;
 }
 
+// Zero, with coalesced 16-byte stores, the int16 blocks the lanes of this
+// warp are about to write: lane l writes from its first block up to its
+// block count (to its segment's last block for the segment's last lane),
+// and in a valid stream these ranges are contiguous across the warp.  Every
+// range is clamped to its segment, so a corrupt stream cannot reach past the
+// image.  All 32 lanes call this; the writes are visible to the warp after it.
+__device__ __forceinline__ void cj_warp_zero_blocks(int16_t* __restrict__ coef, const CJLane& ln,
+                                                    const CJSegment& seg, const CJSubRec& r, int64_t first) {
+  const int lane = threadIdx.x & 31;
+  const int64_t bend = seg.first_block + seg.nblocks;
+  int64_t end = ln.last ? bend : first + r.nblocks;
+  if (end > bend) end = bend;
+  const bool any = ln.active && first < end;
+  long long lo = any ? first : LLONG_MAX, hi = any ? end : LLONG_MIN;
+#pragma unroll
+  for (int d = 16; d; d >>= 1) {
+    lo = min(lo, __shfl_xor_sync(CJ_FULL, lo, d));
+    hi = max(hi, __shfl_xor_sync(CJ_FULL, hi, d));
+  }
+  uint4* p = reinterpret_cast<uint4*>(coef);
+  const uint4 z = make_uint4(0, 0, 0, 0);
+  for (long long q = lo * 8 + lane; q < hi * 8; q += 32) p[q] = z;
+  __syncwarp();
+}
+
 // Final decode of one lane from its settled start: writes quantised int16
 // coefficients (natural order) of its blocks, DC predicted per component,
 // and records structural errors of its restart interval.  `zz` is the
@@ -293,8 +397,11 @@ __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint
   CJFBits br;
   br.init(words, ln.end_byte, cj_state_bit(r.start));
   uint32_t m = cj_state_phase(r.start);
-  int c = sp.phase_comp[m];
-  uint32_t aslot = sp.comp_ac[c], slot = sp.comp_dc[c];
+  const int bpm = sp.bpm;
+  const uint64_t pack = sp.phase_pack;
+  int c;
+  uint32_t aslot, slot;
+  cj_phase(sp, bpm, pack, m, c, slot, aslot);
   int k = -1;
   int32_t dd = 0;
   int16_t* blk = coef;
@@ -315,10 +422,7 @@ __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint
       cj_raise_dec(st, b, CJ_DEV_OVERRUN);
       return false;
     }
-    blk = coef + b * 64;
-    const uint4 z = make_uint4(0, 0, 0, 0);
-#pragma unroll
-    for (int q = 0; q < 8; q++) reinterpret_cast<uint4*>(blk)[q] = z;
+    blk = coef + b * 64;  // zeroed beforehand by cj_warp_zero_blocks
     return true;
   };
   if (!block_start()) return;
@@ -356,10 +460,8 @@ __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint
     }
     blk[0] = (int16_t)dcv;
     b++;
-    m = (m + 1 == (uint32_t)sp.bpm) ? 0 : m + 1;
-    c = sp.phase_comp[m];
-    aslot = sp.comp_ac[c];
-    slot = sp.comp_dc[c];
+    m = (m + 1 == (uint32_t)bpm) ? 0 : m + 1;
+    cj_phase(sp, bpm, pack, m, c, slot, aslot);
     k = -1;
     if (!block_start()) return;
   }

@@ -37,7 +37,7 @@ struct CJReaderDevice {
   int device = -1;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_begin = nullptr, ev_scan = nullptr, ev_end = nullptr;
-  CJDevBuf raw, data, tile_keep, tile_mark, mpos, mcode, segs, recs, snap, wagg, carry, coef,
+  CJDevBuf raw, data, tile_keep, tile_mark, mpos, mcode, segs, recs, ckpt, snap, wagg, carry, coef,
       pix, params, status, wcoef;
   CJHostBuf h_params, h_status, h_pixels, h_file;
   // per-scan bookkeeping

@@ -100,7 +100,7 @@ void cj_dev_release(CJReaderDevice* d) {
   if (!d->gpu_ready) return;
   cudaStreamSynchronize(d->stream);
   CJDevBuf* bufs[] = {&d->raw,  &d->data, &d->tile_keep, &d->tile_mark, &d->mpos,
-                      &d->mcode, &d->segs, &d->recs,     &d->snap,      &d->wagg,
+                      &d->mcode, &d->segs, &d->recs, &d->ckpt,     &d->snap,      &d->wagg,
                       &d->carry, &d->coef, &d->pix,      &d->params,    &d->status,
                       &d->wcoef};
   for (CJDevBuf* b : bufs)
@@ -286,7 +286,7 @@ __device__ __forceinline__ void cj_load_params(CJScanParams& sp, const CJScanPar
 // Stage 3a: speculative decode + settle inside each warp.
 __global__ void __launch_bounds__(CJ_SYNC_THREADS)
 k_sync_intra(const CJScanParams* __restrict__ prm, const CJSegment* __restrict__ segs,
-             const uint32_t* __restrict__ words, CJSubRec* recs, uint64_t* snap_out,
+             const uint32_t* __restrict__ words, CJSubRec* recs, CJCkpt* ckpt, uint64_t* snap_out,
              const CJStatus* st, int sub_bits) {
   __shared__ CJScanParams sp;
   cj_load_params(sp, prm);
@@ -300,8 +300,10 @@ k_sync_intra(const CJScanParams* __restrict__ prm, const CJSegment* __restrict__
   r.start = cj_state(ln.begin, 0);
   r.exit = r.start;
   r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
-  if (ln.active) r = cj_spec_decode(sp, words, ln, r.start);
-  cj_warp_settle(sp, words, ln, r, r.start);
+  CJCkpt* ck = cj_lane_ckpts(ckpt, i);
+  const uint32_t cs = cj_ckpt_step(sub_bits);
+  if (ln.active) r = cj_spec_decode<false>(sp, words, ln, r.start, ck, r, cs);
+  cj_warp_settle(sp, words, ln, r, r.start, ck, cs);
   if (ln.active) recs[i] = r;
   unsigned act = __ballot_sync(CJ_FULL, ln.active);
   if (lane == 31 - __clz(act)) snap_out[warp] = r.exit;
@@ -312,7 +314,7 @@ k_sync_intra(const CJScanParams* __restrict__ prm, const CJSegment* __restrict__
 // last exit differs from what the next warp read.
 __global__ void __launch_bounds__(CJ_SYNC_THREADS)
 k_sync_inter(const CJScanParams* __restrict__ prm, const CJSegment* __restrict__ segs,
-             const uint32_t* __restrict__ words, CJSubRec* recs, const uint64_t* snap_in,
+             const uint32_t* __restrict__ words, CJSubRec* recs, CJCkpt* ckpt, const uint64_t* snap_in,
              uint64_t* snap_out, CJWarpAgg* wagg, CJStatus* st, int sub_bits) {
   __shared__ CJScanParams sp;
   cj_load_params(sp, prm);
@@ -330,7 +332,8 @@ k_sync_inter(const CJScanParams* __restrict__ prm, const CJSegment* __restrict__
   }
   uint64_t in0 = (warp > 0) ? snap_in[warp - 1] : r.start;
   if (lane != 0) in0 = 0;
-  if (cj_warp_settle(sp, words, ln, r, in0) && ln.active) recs[i] = r;
+  if (cj_warp_settle(sp, words, ln, r, in0, cj_lane_ckpts(ckpt, i), cj_ckpt_step(sub_bits)) && ln.active)
+    recs[i] = r;
   unsigned act = __ballot_sync(CJ_FULL, ln.active);
   if (lane == 31 - __clz(act)) {
     if (r.exit != snap_in[warp]) atomicAdd(&st->unstable, 1);
@@ -423,8 +426,9 @@ k_decode_write(const CJScanParams* __restrict__ prm, const CJSegment* __restrict
   int e1, e2, e3;
   const CJWarpAgg cw = carry[warp];
   cj_warp_prefix(r, ln, cw.nblocks, cw.dc[0], cw.dc[1], cw.dc[2], &e0, &e1, &e2, &e3);
-  if (!ln.active) return;
   const CJSegment seg = segs[ln.seg];
+  cj_warp_zero_blocks(coef, ln, seg, r, seg.first_block + e0);
+  if (!ln.active) return;
   cj_write_lane(sp, words, ln, seg, r, seg.first_block + e0, e1, e2, e3, coef, st, sp.zz);
 }
 
@@ -478,6 +482,7 @@ static void cj_fill_params(JPGReader* jpg, CJScanParams* hp) {
   int64_t mcus = (int64_t)hp->mcux * hp->mcuy;
   hp->nseg_expected = jpg->restart_interval ? (int)((mcus + jpg->restart_interval - 1) / jpg->restart_interval) : 1;
   hp->total_blocks = mcus * hp->bpm;
+  hp->phase_pack = cj_phase_pack(*hp);
 }
 
 int cj_scan_launch(JPGReader* jpg) {
@@ -501,6 +506,7 @@ int cj_scan_launch(JPGReader* jpg) {
       cj_dev_ensure(d->mpos, (size_t)d->mark_cap * 4) || cj_dev_ensure(d->mcode, (size_t)d->mark_cap) ||
       cj_dev_ensure(d->segs, (size_t)d->nseg_exp * sizeof(CJSegment)) ||
       cj_dev_ensure(d->recs, (size_t)d->nsub_cap * sizeof(CJSubRec)) ||
+      cj_dev_ensure(d->ckpt, (size_t)d->nsub_cap * CJ_CKPTS * sizeof(CJCkpt)) ||
       cj_dev_ensure(d->snap, (size_t)2 * d->nwarp_cap * sizeof(uint64_t)) ||
       cj_dev_ensure(d->wagg, (size_t)d->nwarp_cap * sizeof(CJWarpAgg)) ||
       cj_dev_ensure(d->carry, (size_t)d->nwarp_cap * sizeof(CJWarpAgg)) ||
@@ -543,11 +549,11 @@ int cj_scan_device(JPGReader* jpg) {
   uint64_t* snap1 = snap0 + d->nwarp_cap;
   k_sync_intra<<<sync_blocks, CJ_SYNC_THREADS, 0, s>>>(
       (const CJScanParams*)d->params.p, (const CJSegment*)d->segs.p, (const uint32_t*)d->data.p,
-      (CJSubRec*)d->recs.p, snap0, st, S);
+      (CJSubRec*)d->recs.p, (CJCkpt*)d->ckpt.p, snap0, st, S);
   cj_after_launch(d, CJ_K_SYNC_INTRA);
   k_sync_inter<<<sync_blocks, CJ_SYNC_THREADS, 0, s>>>(
       (const CJScanParams*)d->params.p, (const CJSegment*)d->segs.p, (const uint32_t*)d->data.p,
-      (CJSubRec*)d->recs.p, snap0, snap1, (CJWarpAgg*)d->wagg.p, st, S);
+      (CJSubRec*)d->recs.p, (CJCkpt*)d->ckpt.p, snap0, snap1, (CJWarpAgg*)d->wagg.p, st, S);
   cj_after_launch(d, CJ_K_SYNC_INTER);
   d->snap_parity = 1;
   CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
@@ -587,7 +593,8 @@ int cj_scan_resync(JPGReader* jpg) {
     int in = d->snap_parity;
     k_sync_inter<<<sync_blocks, CJ_SYNC_THREADS, 0, s>>>(
         (const CJScanParams*)d->params.p, (const CJSegment*)d->segs.p, (const uint32_t*)d->data.p,
-        (CJSubRec*)d->recs.p, snap[in], snap[in ^ 1], (CJWarpAgg*)d->wagg.p, st, d->sub_bits);
+        (CJSubRec*)d->recs.p, (CJCkpt*)d->ckpt.p, snap[in], snap[in ^ 1], (CJWarpAgg*)d->wagg.p, st,
+        d->sub_bits);
     cj_after_launch(d, CJ_K_SYNC_INTER);
     d->snap_parity = in ^ 1;
     CJ_CUDA_TRY(cudaMemcpyAsync(hs, st, sizeof(CJStatus), cudaMemcpyDeviceToHost, s), CUDA_MEM_ERROR);
