@@ -595,32 +595,74 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   bt_grid_sync(a.ctl, gen);
 
   bt_stamp(a.ctl, 8);
-  // ---- phase 8: coefficient write-out (items handed out dynamically)
-  for (int w = bt_next_item(&a.ctl->next_write); w < a.nwarps; w = bt_next_item(&a.ctl->next_write)) {
-    int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
-    const CJImageDesc& d = a.desc[i];
-    CJStatus* st = &a.st[i];
-    const int nsub = __ldcg(&st->nsub), nseg = __ldcg(&st->nseg);
-    const int j0 = w * 32 - d.sub0;
-    if (j0 >= nsub) continue;
-    const CJScanParams& sp = a.prm[i];
-    const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
-    CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
-    CJSubRec r;
-    if (ln.active) r = bt_load_rec(&a.recs[d.sub0 + j0 + lane]);
-    else {
-      r.start = r.exit = 0;
-      r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
+  // ---- phase 8: coefficient write-out in units of a quarter subsequence.
+  // Unit (lane, q) starts at checkpoint q - 1 of the lane's settled decode --
+  // its exact state: position, MCU phase, blocks and DC sums so far -- and
+  // stops at checkpoint q's block boundary (the last unit at the lane's end),
+  // so write items are a quarter as long as sync items whatever the
+  // subsequence size.  An item is 8 lanes x 4 units of one 32-lane warp w,
+  // whose block / DC prefix it recomputes.  (In a corrupt stream a unit may
+  // write past an error an earlier unit stopped at; only blocks after that
+  // error, so the first error of the image is the same.)
+  {
+    constexpr int UNITS = CJ_CKPTS + 1, LANES = 32 / UNITS;
+    for (int t = bt_next_item(&a.ctl->next_write); t < a.nwarps * UNITS; t = bt_next_item(&a.ctl->next_write)) {
+      const int w = t / UNITS, part = t % UNITS;
+      const int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
+      const CJImageDesc& d = a.desc[i];
+      CJStatus* st = &a.st[i];
+      const int nsub = __ldcg(&st->nsub), nseg = __ldcg(&st->nseg);
+      const int j0 = w * 32 - d.sub0;
+      if (j0 >= nsub) continue;
+      const CJScanParams& sp = a.prm[i];
+      const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
+      // block / DC prefix of the 32 lanes of warp w (thread = lane `lane`)
+      const CJLane lw = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
+      CJSubRec rw;
+      if (lw.active) rw = bt_load_rec(&a.recs[d.sub0 + j0 + lane]);
+      else {
+        rw.start = rw.exit = 0;
+        rw.nblocks = rw.dc[0] = rw.dc[1] = rw.dc[2] = 0;
+      }
+      int64_t bw;
+      int e0, e1, e2;
+      cj_warp_prefix(rw, lw, __ldcg(&a.carry[w].nblocks), __ldcg(&a.carry[w].dc[0]),
+                     __ldcg(&a.carry[w].dc[1]), __ldcg(&a.carry[w].dc[2]), &bw, &e0, &e1, &e2);
+      const int64_t firstw = bw + (lw.active ? a.segs[d.seg0 + lw.seg].first_block : 0);
+      // this thread's unit: lane ul of warp w, quarter q
+      const int ul = part * LANES + lane / UNITS, q = lane % UNITS;
+      const int64_t lane_first = __shfl_sync(CJ_FULL, firstw, ul);
+      int dc0 = __shfl_sync(CJ_FULL, e0, ul), dc1 = __shfl_sync(CJ_FULL, e1, ul), dc2 = __shfl_sync(CJ_FULL, e2, ul);
+      CJSubRec r;
+      r.start = __shfl_sync(CJ_FULL, rw.start, ul);
+      r.nblocks = __shfl_sync(CJ_FULL, rw.nblocks, ul);
+      const CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + ul, d.sub_bits);
+      const CJSegment seg = a.segs[d.seg0 + (ln.active ? ln.seg : 0)];
+      const CJCkpt* ck = cj_lane_ckpts(a.ckpt, d.sub0 + j0 + ul);
+      uint64_t start = r.start, stop = ~0ull;
+      int64_t first = lane_first, end = 0;
+      if (ln.active) {
+        if (q > 0) {
+          const uint32_t pp = __ldcg(&ck[q - 1].pp);
+          start = cj_state(ln.begin + (pp & 0xFFFFFFu), pp >> 24);
+          first += __ldcg(&ck[q - 1].nb);
+          dc0 += __ldcg(&ck[q - 1].d0);
+          dc1 += __ldcg(&ck[q - 1].d1);
+          dc2 += __ldcg(&ck[q - 1].d2);
+        }
+        if (q < UNITS - 1) {
+          stop = ln.begin + (__ldcg(&ck[q].pp) & 0xFFFFFFu);
+          const int64_t bend = seg.first_block + seg.nblocks;
+          end = lane_first + __ldcg(&ck[q].nb);
+          if (end > bend) end = bend;
+        } else {
+          end = cj_lane_write_end(ln, seg, r, lane_first);
+        }
+      }
+      cj_warp_zero_range(a.coef + d.coef0 * 64, ln.active, first, end);
+      if (!ln.active) continue;
+      cj_write_lane(sp, words, ln, seg, start, first, dc0, dc1, dc2, a.coef + d.coef0 * 64, st, s_zz, stop);
     }
-    int64_t b;
-    int dc0, dc1, dc2;
-    cj_warp_prefix(r, ln, __ldcg(&a.carry[w].nblocks), __ldcg(&a.carry[w].dc[0]),
-                   __ldcg(&a.carry[w].dc[1]), __ldcg(&a.carry[w].dc[2]), &b, &dc0, &dc1, &dc2);
-    const CJSegment seg = a.segs[d.seg0 + ln.seg];
-    cj_warp_zero_blocks(a.coef + d.coef0 * 64, ln, seg, r, b + seg.first_block);
-    if (!ln.active) continue;
-    cj_write_lane(sp, words, ln, seg, r, b + seg.first_block, dc0, dc1, dc2,
-                  a.coef + d.coef0 * 64, st, s_zz);
   }
 }
 

@@ -200,14 +200,16 @@ __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const
     while (j < CJ_CKPTS && (final || rel >= thresh)) {
       const uint32_t pp = (m << 24) | rel;
       if (RESUME && !final) {
-        const CJCkpt o = ck[j];
-        if (o.pp == pp) {
-          const int dn = nb - o.nb, e0 = d0 - o.d0, e1 = d1 - o.d1, e2 = d2 - o.d2;
+        // checkpoints may have been written by another SM in an earlier pass
+        // of the same kernel: read them from L2, never a stale L1 line
+        if (__ldcg(&ck[j].pp) == pp) {
+          const int dn = nb - __ldcg(&ck[j].nb), e0 = d0 - __ldcg(&ck[j].d0), e1 = d1 - __ldcg(&ck[j].d1),
+                    e2 = d2 - __ldcg(&ck[j].d2);
           for (uint32_t q = j; q < CJ_CKPTS; q++) {
-            ck[q].nb += dn;
-            ck[q].d0 += e0;
-            ck[q].d1 += e1;
-            ck[q].d2 += e2;
+            ck[q].nb = __ldcg(&ck[q].nb) + dn;
+            ck[q].d0 = __ldcg(&ck[q].d0) + e0;
+            ck[q].d1 = __ldcg(&ck[q].d1) + e1;
+            ck[q].d2 = __ldcg(&ck[q].d2) + e2;
           }
           r.exit = old.exit;
           r.nblocks = old.nblocks + dn;
@@ -254,8 +256,9 @@ __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const
       }
     }
   }
-  checkpoint(0, true);
-  r.exit = cj_state(br.pos(), m);
+  const uint64_t pend = br.pos();
+  checkpoint((uint32_t)(pend - ln.begin), true);  // thresholds not reached: the exit
+  r.exit = cj_state(pend, m);
   r.nblocks = nb;
   r.dc[0] = d0;
   r.dc[1] = d1;
@@ -357,46 +360,58 @@ __device__ __forceinline__ void cj_warp_prefix(const CJSubRec& r, const CJLane& 
   *d2 = e3;
 }
 
-// Zero, with coalesced 16-byte stores, the int16 blocks the lanes of this
-// warp are about to write: lane l writes from its first block up to its
-// block count (to its segment's last block for the segment's last lane),
-// and in a valid stream these ranges are contiguous across the warp.  Every
-// range is clamped to its segment, so a corrupt stream cannot reach past the
-// image.  All 32 lanes call this; the writes are visible to the warp after it.
-__device__ __forceinline__ void cj_warp_zero_blocks(int16_t* __restrict__ coef, const CJLane& ln,
-                                                    const CJSegment& seg, const CJSubRec& r, int64_t first) {
+// Zero, with coalesced 16-byte stores, the int16 blocks [first, end) that
+// each lane of this warp is about to write (inactive lanes pass active =
+// false); in a valid stream these ranges are contiguous across the warp.
+// Callers clamp every range to its segment, so a corrupt stream cannot reach
+// past the image.  All 32 lanes call this; the writes are visible to the warp
+// after it.
+__device__ __forceinline__ void cj_warp_zero_range(int16_t* __restrict__ coef, bool active, int64_t first,
+                                                   int64_t end) {
   const int lane = threadIdx.x & 31;
-  const int64_t bend = seg.first_block + seg.nblocks;
-  int64_t end = ln.last ? bend : first + r.nblocks;
-  if (end > bend) end = bend;
-  const bool any = ln.active && first < end;
+  const bool any = active && first < end;
   long long lo = any ? first : LLONG_MAX, hi = any ? end : LLONG_MIN;
 #pragma unroll
   for (int d = 16; d; d >>= 1) {
     lo = min(lo, __shfl_xor_sync(CJ_FULL, lo, d));
     hi = max(hi, __shfl_xor_sync(CJ_FULL, hi, d));
   }
-  uint4* p = reinterpret_cast<uint4*>(coef);
-  const uint4 z = make_uint4(0, 0, 0, 0);
-  for (long long q = lo * 8 + lane; q < hi * 8; q += 32) p[q] = z;
+  // no range at all: lo and hi keep their sentinels (lo * 8 would wrap)
+  if (lo < hi) {
+    uint4* p = reinterpret_cast<uint4*>(coef);
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    for (long long q = lo * 8 + lane; q < hi * 8; q += 32) p[q] = z;
+  }
   __syncwarp();
+}
+
+// Blocks lane `ln` writes from block `first`: to its block count, or to its
+// segment's last block for the segment's last lane; clamped to the segment.
+__device__ __forceinline__ int64_t cj_lane_write_end(const CJLane& ln, const CJSegment& seg, const CJSubRec& r,
+                                                     int64_t first) {
+  const int64_t bend = seg.first_block + seg.nblocks;
+  const int64_t end = ln.last ? bend : first + r.nblocks;
+  return end > bend ? bend : end;
 }
 
 // Final decode of one lane from its settled start: writes quantised int16
 // coefficients (natural order) of its blocks, DC predicted per component,
 // and records structural errors of its restart interval.  `zz` is the
-// zig-zag -> natural index table (64 entries, in shared memory).
+// zig-zag -> natural index table (64 entries, in shared memory).  A part of
+// a lane (a unit) starts at one of its checkpoints (`start`, its first block
+// and DC predictors) and stops at the block boundary `stop`, the next
+// checkpoint; stop = ~0 runs to the lane's end.
 __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint32_t* words,
                                               const CJLane& ln, const CJSegment& seg,
-                                              const CJSubRec& r, int64_t first_block, int dc0,
+                                              uint64_t start, int64_t first_block, int dc0,
                                               int dc1, int dc2, int16_t* __restrict__ coef,
-                                              CJStatus* st, const uint8_t* zz) {
+                                              CJStatus* st, const uint8_t* zz, uint64_t stop) {
   int64_t b = first_block;
   const int64_t bend = seg.first_block + seg.nblocks;
   const uint64_t seg_end = seg.bit_end;
   CJFBits br;
-  br.init(words, ln.end_byte, cj_state_bit(r.start));
-  uint32_t m = cj_state_phase(r.start);
+  br.init(words, ln.end_byte, cj_state_bit(start));
+  uint32_t m = cj_state_phase(start);
   const int bpm = sp.bpm;
   const uint64_t pack = sp.phase_pack;
   int c;
@@ -408,6 +423,7 @@ __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint
   // the structural checks made before every block; false = stop here
   auto block_start = [&]() -> bool {
     const uint64_t p = br.pos();
+    if (p >= stop) return false;  // the next unit's first block
     if (!ln.last && p >= ln.end) return false;
     if (b >= bend) {
       if (!ln.last) cj_raise_dec(st, b, CJ_DEV_EXTRA);

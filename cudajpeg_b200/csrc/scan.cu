@@ -427,9 +427,10 @@ k_decode_write(const CJScanParams* __restrict__ prm, const CJSegment* __restrict
   const CJWarpAgg cw = carry[warp];
   cj_warp_prefix(r, ln, cw.nblocks, cw.dc[0], cw.dc[1], cw.dc[2], &e0, &e1, &e2, &e3);
   const CJSegment seg = segs[ln.seg];
-  cj_warp_zero_blocks(coef, ln, seg, r, seg.first_block + e0);
+  const int64_t first = seg.first_block + e0;
+  cj_warp_zero_range(coef, ln.active, first, cj_lane_write_end(ln, seg, r, first));
   if (!ln.active) return;
-  cj_write_lane(sp, words, ln, seg, r, seg.first_block + e0, e1, e2, e3, coef, st, sp.zz);
+  cj_write_lane(sp, words, ln, seg, r.start, first, e1, e2, e3, coef, st, sp.zz, ~0ull);
 }
 
 // ---------------------------------------------------------------- host side
