@@ -22,6 +22,7 @@
 // warps behind them.  Data one CTA writes and another
 // reads inside the kernel is read with L2-coherent loads (__ldcg).  Errors
 // are kept per image: a corrupt image fails alone.
+#include <stddef.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -181,6 +182,24 @@ __device__ __forceinline__ int bt_next_item(int* counter) {
   return __shfl_sync(0xFFFFFFFFu, w, 0);
 }
 
+// Next group of BT_WARPS consecutive items for the whole CTA (thread 0 takes
+// it, the CTA shares it).  The leading barrier also ends the previous group:
+// every warp is done with it and with the tables staged for it.
+__device__ __forceinline__ int bt_next_group(int* counter, int* s_slot) {
+  __syncthreads();
+  if (threadIdx.x == 0) *s_slot = atomicAdd(counter, BT_WARPS);
+  __syncthreads();
+  return *s_slot;
+}
+
+// Copy one image's decode-step tables (16 KB) into shared memory.  The
+// tables were built by another CTA in this kernel: read them from L2.
+__device__ __forceinline__ void bt_copy_steps(CJSteps* dst, const CJSteps* src) {
+  const int4* s = reinterpret_cast<const int4*>(src);
+  int4* d = reinterpret_cast<int4*>(dst);
+  for (int k = threadIdx.x; k < (int)(sizeof(CJSteps) / 16); k += blockDim.x) d[k] = __ldcg(s + k);
+}
+
 // Largest i with key(i) <= v over a sorted int32 field of the descriptors.
 template <class F>
 __device__ __forceinline__ int bt_find(int n, int v, F key) {
@@ -191,6 +210,39 @@ __device__ __forceinline__ int bt_find(int n, int v, F key) {
     else hi = mid - 1;
   }
   return lo;
+}
+
+// Step tables of the entropy phases, staged per item group: a group's warps
+// [wa, wb] span few images, and the step tables of the first and the last
+// of them are copied into shared memory (slots 0 and 1), so every symbol
+// lookup is a shared-memory load instead of an L2 round trip (the tables of
+// all images of a batch do not fit in L1).  Images strictly between the two
+// (a run of tiny images) read their tables from global memory.
+struct BTStaged {
+  int ia, ib;
+};
+#define BT_DECODE_SMEM (2 * sizeof(CJSteps))
+static_assert(sizeof(CJSteps) % 16 == 0 && offsetof(CJScanParams, steps) % 16 == 0, "int4 table copy");
+static_assert(BT_DECODE_SMEM >= BT_THREADS * sizeof(CJAgg5), "phase 7 scan space");
+
+__device__ __forceinline__ int bt_image_of_warp(const CJBatchArgs& a, int w) {
+  return bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
+}
+
+// All threads of the CTA: stage the tables of warps [wa, wb]'s first and last image.
+__device__ __forceinline__ BTStaged bt_stage(const CJBatchArgs& a, int wa, int wb, CJSteps* tab) {
+  BTStaged g;
+  g.ia = bt_image_of_warp(a, wa);
+  g.ib = bt_image_of_warp(a, wb);
+  bt_copy_steps(&tab[0], &a.prm[g.ia].steps);
+  if (g.ib != g.ia) bt_copy_steps(&tab[1], &a.prm[g.ib].steps);
+  __syncthreads();
+  return g;
+}
+
+__device__ __forceinline__ const CJSteps& bt_steps_of(const CJBatchArgs& a, const BTStaged& g, const CJSteps* tab,
+                                                      int i) {
+  return i == g.ia ? tab[0] : (i == g.ib ? tab[1] : a.prm[i].steps);
 }
 
 __constant__ uint8_t c_bt_zz[64] = CJ_ZIGZAG_INIT;  // zig-zag -> natural index
@@ -304,6 +356,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ int2 sm2[33];
   __shared__ uint8_t s_zz[64];
+  __shared__ int s_grp;
   unsigned gen = 0;
   if (threadIdx.x == 0) gen = atomicAdd(&a.ctl->bar_gen, 0);
   if (threadIdx.x < 64) s_zz[threadIdx.x] = c_bt_zz[threadIdx.x];
@@ -457,14 +510,22 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   bt_grid_sync(a.ctl, gen);
 
   bt_stamp(a.ctl, 5);
-  // ---- phase 5: speculative decode + warp settle (items handed out dynamically)
-  for (int w = bt_next_item(&a.ctl->next_sync); w < a.nwarps; w = bt_next_item(&a.ctl->next_sync)) {
-    int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
+  // ---- phase 5: speculative decode + warp settle, in groups of BT_WARPS
+  // consecutive warps per CTA (handed out dynamically) with staged tables
+  CJSteps* tab = reinterpret_cast<CJSteps*>(smem);
+  for (;;) {
+    const int g0 = bt_next_group(&a.ctl->next_sync, &s_grp);
+    if (g0 >= a.nwarps) break;
+    const BTStaged sg = bt_stage(a, g0, min(g0 + BT_WARPS, a.nwarps) - 1, tab);
+    const int w = g0 + (int)(threadIdx.x >> 5);
+    if (w >= a.nwarps) continue;  // warp-uniform
+    const int i = bt_image_of_warp(a, w);
     const CJImageDesc& d = a.desc[i];
     const int nsub = __ldcg(&a.st[i].nsub), nseg = __ldcg(&a.st[i].nseg);
     const int j0 = w * 32 - d.sub0;
     if (j0 >= nsub) continue;  // warp-uniform
     const CJScanParams& sp = a.prm[i];
+    const CJSteps& T = bt_steps_of(a, sg, tab, i);
     const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
     CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
     CJSubRec r;
@@ -473,8 +534,8 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
     r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
     CJCkpt* ck = cj_lane_ckpts(a.ckpt, d.sub0 + j0 + lane);
     const uint32_t cs = cj_ckpt_step(d.sub_bits);
-    if (ln.active) r = cj_spec_decode<false>(sp, words, ln, r.start, ck, r, cs);
-    cj_warp_settle(sp, words, ln, r, r.start, ck, cs);
+    if (ln.active) r = cj_spec_decode<false>(sp, T, words, ln, r.start, ck, r, cs);
+    cj_warp_settle(sp, T, words, ln, r, r.start, ck, cs);
     if (ln.active) a.recs[d.sub0 + j0 + lane] = r;
     unsigned act = __ballot_sync(CJ_FULL, ln.active);
     if (lane == 31 - __clz(act)) a.snap0[w] = r.exit;
@@ -497,30 +558,44 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       a.ctl->unstable[(pass + 1) % 3] = 0;
       a.ctl->next_fix[(pass + 1) % 3] = 0;
     }
-    for (int w = bt_next_item(next); w < a.nwarps; w = bt_next_item(next)) {
-      int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
-      const CJImageDesc& d = a.desc[i];
-      const int nsub = __ldcg(&a.st[i].nsub), nseg = __ldcg(&a.st[i].nseg);
-      const int j0 = w * 32 - d.sub0;
-      if (j0 >= nsub) {
-        if (lane == 0) {
-          CJWarpAgg z;
-          memset(&z, 0, sizeof(z));
-          a.wagg[w] = z;
+    for (;;) {
+      const int g0 = bt_next_group(next, &s_grp);
+      if (g0 >= a.nwarps) break;
+      const int w = g0 + (int)(threadIdx.x >> 5);
+      bool work = w < a.nwarps;  // warp-uniform, like everything below
+      int i = 0, nsub = 0, nseg = 0, j0 = 0;
+      if (work) {
+        i = bt_image_of_warp(a, w);
+        nsub = __ldcg(&a.st[i].nsub);
+        nseg = __ldcg(&a.st[i].nseg);
+        j0 = w * 32 - a.desc[i].sub0;
+        if (j0 >= nsub) {
+          if (lane == 0) {
+            CJWarpAgg z;
+            memset(&z, 0, sizeof(z));
+            a.wagg[w] = z;
+          }
+          work = false;
         }
-        continue;
       }
-      const CJScanParams& sp = a.prm[i];
-      const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
-      CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
+      const CJImageDesc& d = a.desc[i];
+      CJLane ln = cj_lane(a.segs + d.seg0, nseg, work ? nsub : 0, j0 + lane, d.sub_bits);
       CJSubRec r;
       if (ln.active) r = bt_load_rec(&a.recs[d.sub0 + j0 + lane]);
       else {
         r.start = r.exit = 0;
         r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
       }
-      uint64_t in0 = (j0 > 0 && lane == 0) ? __ldcg(&snap_in[w - 1]) : r.start;
-      if (cj_warp_settle(sp, words, ln, r, in0, cj_lane_ckpts(a.ckpt, d.sub0 + j0 + lane),
+      const uint64_t in0 = (work && j0 > 0 && lane == 0) ? __ldcg(&snap_in[w - 1]) : r.start;
+      // the settle's first test; only a group with a lane to re-decode stages tables
+      const uint64_t pred = __shfl_up_sync(CJ_FULL, r.exit, 1);
+      const uint64_t want = ln.head ? r.start : (lane == 0 ? in0 : pred);
+      BTStaged sg = {-1, -1};
+      if (__syncthreads_or(ln.active && want != r.start)) sg = bt_stage(a, g0, min(g0 + BT_WARPS, a.nwarps) - 1, tab);
+      if (!work) continue;
+      const CJScanParams& sp = a.prm[i];
+      const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
+      if (cj_warp_settle(sp, bt_steps_of(a, sg, tab, i), words, ln, r, in0, cj_lane_ckpts(a.ckpt, d.sub0 + j0 + lane),
                          cj_ckpt_step(d.sub_bits)) && ln.active)
         a.recs[d.sub0 + j0 + lane] = r;
       unsigned act = __ballot_sync(CJ_FULL, ln.active);
@@ -560,7 +635,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   bt_stamp(a.ctl, 7);
   // ---- phase 7: segmented scan of the warp aggregates (CTA 0)
   if (blockIdx.x == 0) {
-    CJAgg5* sm = reinterpret_cast<CJAgg5*>(smem);  // BT_THREADS entries
+    CJAgg5* sm = reinterpret_cast<CJAgg5*>(smem);  // BT_THREADS entries (within BT_DECODE_SMEM)
     const int nw = a.nwarps;
     int per = (nw + blockDim.x - 1) / blockDim.x;
     int lo = threadIdx.x * per, hi = min(nw, lo + per);
@@ -606,15 +681,22 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   // error, so the first error of the image is the same.)
   {
     constexpr int UNITS = CJ_CKPTS + 1, LANES = 32 / UNITS;
-    for (int t = bt_next_item(&a.ctl->next_write); t < a.nwarps * UNITS; t = bt_next_item(&a.ctl->next_write)) {
+    const int nitems = a.nwarps * UNITS;
+    for (;;) {
+      const int g0 = bt_next_group(&a.ctl->next_write, &s_grp);
+      if (g0 >= nitems) break;
+      const BTStaged sg = bt_stage(a, g0 / UNITS, (min(g0 + BT_WARPS, nitems) - 1) / UNITS, tab);
+      const int t = g0 + (int)(threadIdx.x >> 5);
+      if (t >= nitems) continue;  // warp-uniform
       const int w = t / UNITS, part = t % UNITS;
-      const int i = bt_find(a.n, w, [&](int k) { return a.desc[k].sub0 >> 5; });
+      const int i = bt_image_of_warp(a, w);
       const CJImageDesc& d = a.desc[i];
       CJStatus* st = &a.st[i];
       const int nsub = __ldcg(&st->nsub), nseg = __ldcg(&st->nseg);
       const int j0 = w * 32 - d.sub0;
       if (j0 >= nsub) continue;
       const CJScanParams& sp = a.prm[i];
+      const CJSteps& T = bt_steps_of(a, sg, tab, i);
       const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
       // block / DC prefix of the 32 lanes of warp w (thread = lane `lane`)
       const CJLane lw = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
@@ -661,7 +743,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       }
       cj_warp_zero_range(a.coef + d.coef0 * 64, ln.active, first, end);
       if (!ln.active) continue;
-      cj_write_lane(sp, words, ln, seg, start, first, dc0, dc1, dc2, a.coef + d.coef0 * 64, st, s_zz, stop);
+      cj_write_lane(sp, T, words, ln, seg, start, first, dc0, dc1, dc2, a.coef + d.coef0 * 64, st, s_zz, stop);
     }
   }
 }
@@ -1031,7 +1113,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   b->out_total = out_total;
   b->blocks = blocks;
   b->scan_bytes = data_bytes;
-  b->smem = (size_t)BT_THREADS * sizeof(CJAgg5);
+  b->smem = BT_DECODE_SMEM;
   b->smem_pix = smem;
   if (!nd) return 0;
   size_t nd_ = (size_t)nd;
@@ -1526,7 +1608,7 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   g.vmax = h.vmax;
   g.T = d.T;
   const size_t smem_pix = cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1], 2);
-  const size_t smem = (size_t)BT_THREADS * sizeof(CJAgg5);
+  const size_t smem = BT_DECODE_SMEM;
 
   cudaStream_t s = (cudaStream_t)stream;
   CJ_CUDA_TRY(cudaMemcpyAsync(base + o_hdr, &h, sizeof(h), cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);

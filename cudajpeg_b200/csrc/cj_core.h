@@ -232,16 +232,18 @@ CJ_HD uint16_t cj_step_sub(const CJHuff& t, int pmin, int s, int j, bool ac) {
   return (uint16_t)cj_step_of(cj_huff_slow(t, win), ac);
 }
 
-// The decode step for the 32-bit window v (MSB = next bit) of table `slot`.
-CJ_HD uint32_t cj_step(const CJScanParams& sp, uint32_t slot, uint32_t v) {
-  uint32_t st = sp.steps.pri[slot][v >> (32 - CJ_FAST_BITS)];
+// The decode step for the 32-bit window v (MSB = next bit) of table `slot`,
+// from step tables `T` (sp.steps or a copy of them, e.g. in shared memory).
+CJ_HD uint32_t cj_step(const CJSteps& T, const CJScanParams& sp, uint32_t slot, uint32_t v) {
+  uint32_t st = T.pri[slot][v >> (32 - CJ_FAST_BITS)];
   if (!(st & 31)) {
     const uint32_t i = st >> 5;
-    st = i != CJ_STEP_SEARCH ? sp.steps.sub[slot][i][(v >> 16) & 63]
+    st = i != CJ_STEP_SEARCH ? T.sub[slot][i][(v >> 16) & 63]
                              : cj_step_of(cj_huff_slow(sp.huff[slot], v >> 16), slot >= 2);
   }
   return st;
 }
+CJ_HD uint32_t cj_step(const CJScanParams& sp, uint32_t slot, uint32_t v) { return cj_step(sp.steps, sp, slot, v); }
 
 
 // Sign extension of a `size`-bit magnitude category value (T.81 F.2.2.1).

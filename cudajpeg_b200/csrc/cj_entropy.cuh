@@ -176,8 +176,9 @@ struct CJCkpt {
 // point (shifting the later checkpoints too).  The result equals a full
 // decode from `start`.
 template <bool RESUME>
-__device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const uint32_t* words,
-                                                   const CJLane& ln, uint64_t start, CJCkpt* __restrict__ ck,
+__device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const CJSteps& T,
+                                                   const uint32_t* words, const CJLane& ln, uint64_t start,
+                                                   CJCkpt* __restrict__ ck,
                                                    const CJSubRec& old, uint32_t cstep) {
   CJFBits br;
   br.init(words, ln.end_byte, cj_state_bit(start));
@@ -229,7 +230,7 @@ __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const
     if (checkpoint(endrel - (uint32_t)rem, false)) return r;
     for (;;) {
       const uint32_t v = br.peek();
-      const uint32_t st = cj_step(sp, slot, v);
+      const uint32_t st = cj_step(T, sp, slot, v);
       const int kn = k + (int)((st >> 5) & 127);
       const uint32_t used = (st & 31) - (kn > 63 ? (st >> 12) : 0u);
       const bool isdc = k < 0;
@@ -273,7 +274,7 @@ __device__ __forceinline__ uint32_t cj_ckpt_step(int sub_bits) { return (uint32_
 // Re-decode lanes whose input state (lane 0: `lane0_in`; others: the exit of
 // the previous lane) differs from the state they last decoded from, until no
 // lane changes.  Lane l settles after at most l+1 re-decodes.
-__device__ __forceinline__ bool cj_warp_settle(const CJScanParams& sp, const uint32_t* words,
+__device__ __forceinline__ bool cj_warp_settle(const CJScanParams& sp, const CJSteps& T, const uint32_t* words,
                                                const CJLane& ln, CJSubRec& r, uint64_t lane0_in,
                                                CJCkpt* ck, uint32_t cstep) {
   int lane = threadIdx.x & 31;
@@ -284,7 +285,7 @@ __device__ __forceinline__ bool cj_warp_settle(const CJScanParams& sp, const uin
     bool change = ln.active && want != r.start;
     if (!__any_sync(CJ_FULL, change)) break;
     if (change) {
-      r = cj_spec_decode<true>(sp, words, ln, want, ck, r, cstep);
+      r = cj_spec_decode<true>(sp, T, words, ln, want, ck, r, cstep);
       dirty = true;
     }
   }
@@ -401,7 +402,7 @@ __device__ __forceinline__ int64_t cj_lane_write_end(const CJLane& ln, const CJS
 // a lane (a unit) starts at one of its checkpoints (`start`, its first block
 // and DC predictors) and stops at the block boundary `stop`, the next
 // checkpoint; stop = ~0 runs to the lane's end.
-__device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint32_t* words,
+__device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const CJSteps& T, const uint32_t* words,
                                               const CJLane& ln, const CJSegment& seg,
                                               uint64_t start, int64_t first_block, int dc0,
                                               int dc1, int dc2, int16_t* __restrict__ coef,
@@ -444,7 +445,7 @@ __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const uint
   if (!block_start()) return;
   for (;;) {
     const uint32_t v = br.peek();
-    const uint32_t stp = cj_step(sp, slot, v);
+    const uint32_t stp = cj_step(T, sp, slot, v);
     const uint32_t dk = (stp >> 5) & 127, size = stp >> 12, total = stp & 31;
     const int kn = k + (int)dk;
     const uint32_t len = total - size;

@@ -302,8 +302,8 @@ k_sync_intra(const CJScanParams* __restrict__ prm, const CJSegment* __restrict__
   r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
   CJCkpt* ck = cj_lane_ckpts(ckpt, i);
   const uint32_t cs = cj_ckpt_step(sub_bits);
-  if (ln.active) r = cj_spec_decode<false>(sp, words, ln, r.start, ck, r, cs);
-  cj_warp_settle(sp, words, ln, r, r.start, ck, cs);
+  if (ln.active) r = cj_spec_decode<false>(sp, sp.steps, words, ln, r.start, ck, r, cs);
+  cj_warp_settle(sp, sp.steps, words, ln, r, r.start, ck, cs);
   if (ln.active) recs[i] = r;
   unsigned act = __ballot_sync(CJ_FULL, ln.active);
   if (lane == 31 - __clz(act)) snap_out[warp] = r.exit;
@@ -332,7 +332,7 @@ k_sync_inter(const CJScanParams* __restrict__ prm, const CJSegment* __restrict__
   }
   uint64_t in0 = (warp > 0) ? snap_in[warp - 1] : r.start;
   if (lane != 0) in0 = 0;
-  if (cj_warp_settle(sp, words, ln, r, in0, cj_lane_ckpts(ckpt, i), cj_ckpt_step(sub_bits)) && ln.active)
+  if (cj_warp_settle(sp, sp.steps, words, ln, r, in0, cj_lane_ckpts(ckpt, i), cj_ckpt_step(sub_bits)) && ln.active)
     recs[i] = r;
   unsigned act = __ballot_sync(CJ_FULL, ln.active);
   if (lane == 31 - __clz(act)) {
@@ -430,7 +430,7 @@ k_decode_write(const CJScanParams* __restrict__ prm, const CJSegment* __restrict
   const int64_t first = seg.first_block + e0;
   cj_warp_zero_range(coef, ln.active, first, cj_lane_write_end(ln, seg, r, first));
   if (!ln.active) return;
-  cj_write_lane(sp, words, ln, seg, r.start, first, e1, e2, e3, coef, st, sp.zz, ~0ull);
+  cj_write_lane(sp, sp.steps, words, ln, seg, r.start, first, e1, e2, e3, coef, st, sp.zz, ~0ull);
 }
 
 // ---------------------------------------------------------------- host side
