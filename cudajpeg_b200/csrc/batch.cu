@@ -811,39 +811,57 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
     cj_pix_layout(&gg, prm.comp_sx[1], prm.comp_sy[1], 2);
     return gg;
   };
-  // thread 0 issues each tile's copy one tile ahead of the compute
+  // thread 0 issues each tile's copy one tile ahead of the compute; it keeps
+  // the geometry of the image it prefetches from
+  __shared__ CJPixGeom s_pg;  // thread 0's prefetch geometry (kept out of registers)
+  __shared__ int s_pimg;
+  if (threadIdx.x == 0) s_pimg = -1;
+  CJPixGeom& pg = s_pg;
   auto issue = [&](int tt, int i, int which) {
-    const CJPixGeom gg = geom_of(i);
-    const int local = tt - a.desc[i].ptile0, gx = (gg.mcux + gg.T - 1) / gg.T;
-    cj_pixel_issue(a.coef + a.desc[i].coef0 * 64, gg, local / gx, (local % gx) * gg.T,
-                   reinterpret_cast<int16_t*>(smem + which * gg.sc1_off), &bar2[which]);
+    if (i != s_pimg) {
+      pg = geom_of(i);
+      s_pimg = i;
+    }
+    const int local = tt - a.desc[i].ptile0, gx = (pg.mcux + pg.T - 1) / pg.T;
+    cj_pixel_issue(a.coef + a.desc[i].coef0 * 64, pg, local / gx, (local % gx) * pg.T,
+                   reinterpret_cast<int16_t*>(smem + which * pg.sc1_off), &bar2[which]);
   };
   int img = bt_find(a.n, t0, [&](int k) { return a.desc[k].ptile0; });
-  int pimg = img;  // image of the tile being prefetched (thread 0)
   if (threadIdx.x == 0) issue(t0, img, 0);
+  int nimg = img;  // image of the next tile to prefetch (thread 0)
   CJPixGeom g = geom_of(img);
   int gimg = img;
+  cj_pixel_setup(a.prm[img], g, &P);
+  // tile position in its image's grid, advanced tile by tile
+  int gx = (g.mcux + g.T - 1) / g.T;
+  int trow = (t0 - a.desc[img].ptile0) / gx, tcol = (t0 - a.desc[img].ptile0) % gx;
   int buf = 0;
-  uint32_t par[2] = {0, 0};
+  uint32_t par = 0;  // bit b: the phase parity buffer b's barrier waits for next
   for (int t = t0; t < t1; t++) {
     if (t + 1 < t1 && threadIdx.x == 0) {
-      pimg = advance(t + 1, pimg);
-      issue(t + 1, pimg, buf ^ 1);
+      nimg = advance(t + 1, nimg);
+      issue(t + 1, nimg, buf ^ 1);
     }
     img = advance(t, img);
-    if (img != gimg) {
+    if (img != gimg) {  // CTA-uniform; the previous tile ended with a barrier
       g = geom_of(img);
       gimg = img;
+      cj_pixel_setup(a.prm[img], g, &P);
+      gx = (g.mcux + g.T - 1) / g.T;
+      trow = tcol = 0;  // a new image starts at its first tile
     }
     const CJImageDesc& d = a.desc[img];
-    const int local = t - d.ptile0, gx = (g.mcux + g.T - 1) / g.T;
     const int16_t* sc = reinterpret_cast<const int16_t*>(smem + buf * g.sc1_off);
-    if (!cj_pixel_compute(a.prm[img], a.out + d.out_off, &a.st[img], g, local / gx, (local % gx) * g.T, sc,
-                          smem, &bar2[buf], par[buf], &P)) {
-      if (t + 1 < t1) cj_mbar_wait(&bar2[buf ^ 1], par[buf ^ 1]);  // the prefetch in flight
+    if (!cj_pixel_compute(a.prm[img], a.out + d.out_off, &a.st[img], g, trow, tcol * g.T, sc, smem, &bar2[buf],
+                          (par >> buf) & 1u, &P)) {
+      if (t + 1 < t1) cj_mbar_wait(&bar2[buf ^ 1], (par >> (buf ^ 1)) & 1u);  // the prefetch in flight
       break;
     }
-    par[buf] ^= 1;
+    if (++tcol == gx) {
+      tcol = 0;
+      trow++;
+    }
+    par ^= 1u << buf;
     buf ^= 1;
   }
 }

@@ -48,8 +48,9 @@ __device__ __forceinline__ void cj_idct_row(int* d) {
   d[7] = (x7 - x1) >> 8;
 }
 
-// Column pass with level shift and clip (pixelTransformGPU.cu:87-141).
-__device__ __forceinline__ void cj_idct_col(const int* d, uint32_t* o) {
+// Column pass (pixelTransformGPU.cu:87-141) up to the final >> 14: the
+// samples before the +128 level shift and the clip.
+__device__ __forceinline__ void cj_idct_col_s(const int* d, int* o) {
   int x0 = (d[0] * 256) + 8192, x1 = d[4] * 256, x2 = d[6], x3 = d[2];
   int x4 = d[1], x5 = d[7], x6 = d[5], x7 = d[3], x8;
   x8 = CJ_W7 * (x4 + x5) + 4;
@@ -73,16 +74,32 @@ __device__ __forceinline__ void cj_idct_col(const int* d, uint32_t* o) {
   x0 -= x2;
   x2 = (181 * (x4 + x5) + 128) >> 8;
   x4 = (181 * (x4 - x5) + 128) >> 8;
-  o[0] = cj_clip8(((x7 + x1) >> 14) + 128);
-  o[1] = cj_clip8(((x3 + x2) >> 14) + 128);
-  o[2] = cj_clip8(((x0 + x4) >> 14) + 128);
-  o[3] = cj_clip8(((x8 + x6) >> 14) + 128);
-  o[4] = cj_clip8(((x8 - x6) >> 14) + 128);
-  o[5] = cj_clip8(((x0 - x4) >> 14) + 128);
-  o[6] = cj_clip8(((x3 - x2) >> 14) + 128);
-  o[7] = cj_clip8(((x7 - x1) >> 14) + 128);
+  o[0] = (x7 + x1) >> 14;
+  o[1] = (x3 + x2) >> 14;
+  o[2] = (x0 + x4) >> 14;
+  o[3] = (x8 + x6) >> 14;
+  o[4] = (x8 - x6) >> 14;
+  o[5] = (x0 - x4) >> 14;
+  o[6] = (x3 - x2) >> 14;
+  o[7] = (x7 - x1) >> 14;
 }
 
+// Column pass with level shift and clip.
+__device__ __forceinline__ void cj_idct_col(const int* d, uint32_t* o) {
+  int s[8];
+  cj_idct_col_s(d, s);
+#pragma unroll
+  for (int j = 0; j < 8; j++) o[j] = cj_clip8(s[j] + 128);
+}
+
+// Two column-pass samples a, b -> the bytes clip(a + 128), clip(b + 128) in
+// the low half (a in the low byte): a signed saturating pack to [-128, 127]
+// and a flip of each byte's top bit (s + 128 == s ^ 0x80 for a signed byte).
+__device__ __forceinline__ uint32_t cj_level2(int a, int b) {
+  uint32_t d;
+  asm("cvt.pack.sat.s8.s32.b32 %0, %1, %2, 0;" : "=r"(d) : "r"(b), "r"(a));
+  return d ^ 0x8080u;
+}
 
 // Unpack 8 int16 coefficients (one 16-byte row) and dequantise them.
 __device__ __forceinline__ void cj_unpack_dequant(uint4 raw, const int16_t* q, int* v) {

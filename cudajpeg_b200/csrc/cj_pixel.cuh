@@ -148,23 +148,56 @@ __device__ __forceinline__ CJChromaTerms cj_chroma_terms(int cb_byte, int cr_byt
   return {(359 * cr + 128) >> 8, (-88 * cb - 183 * cr + 128) >> 8, (454 * cb + 128) >> 8};
 }
 
-// 8 pixels of one row (Y bytes in yv) -> 24 RGB bytes in six words.
+// Four int32 values saturated to [0, 255] and packed little-endian
+// (v0 in the low byte): cvt.pack.sat packs two saturated bytes under the
+// low half of its third operand.
+__device__ __forceinline__ uint32_t cj_pack_sat4(int v0, int v1, int v2, int v3) {
+  uint32_t hi, d;
+  asm("cvt.pack.sat.u8.s32.b32 %0, %1, %2, 0;" : "=r"(hi) : "r"(v3), "r"(v2));
+  asm("cvt.pack.sat.u8.s32.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(v1), "r"(v0), "r"(hi));
+  return d;
+}
+
+// 8 pixels of one row (Y bytes in yv) -> 24 RGB bytes in six words; pixel k
+// takes chroma terms d[k >> dshift].  R = clip(Y + dR) etc. (cj_chroma_terms).
 __device__ __forceinline__ void cj_rgb8(uint2 yv, const CJChromaTerms* d, int dshift, uint32_t* wds) {
-  uint32_t bytes[24];
+  int c[24];
 #pragma unroll
   for (int k = 0; k < 8; k++) {
     const int Y = (int)(((k < 4 ? yv.x : yv.y) >> (8 * (k & 3))) & 0xFF);
     const CJChromaTerms t = d[k >> dshift];
-    bytes[3 * k] = cj_clip8(Y + t.r);
-    bytes[3 * k + 1] = cj_clip8(Y + t.g);
-    bytes[3 * k + 2] = cj_clip8(Y + t.b);
+    c[3 * k] = Y + t.r;
+    c[3 * k + 1] = Y + t.g;
+    c[3 * k + 2] = Y + t.b;
   }
 #pragma unroll
-  for (int w = 0; w < 6; w++)
-    wds[w] = bytes[4 * w] | (bytes[4 * w + 1] << 8) | (bytes[4 * w + 2] << 16) | (bytes[4 * w + 3] << 24);
+  for (int w = 0; w < 6; w++) wds[w] = cj_pack_sat4(c[4 * w], c[4 * w + 1], c[4 * w + 2], c[4 * w + 3]);
 }
 
-// One tile, MCU row `mrow`, MCUs [mc0, mc0 + T), whose coefficients arrive
+// Per-image part of the tile setup (all threads; the tile's own barrier
+// after the coefficient copy orders it before use): dequantisation tables and,
+// for every block of a full tile, its destination in the plane tiles, its
+// component and its quantisation table.  A shorter last tile of an MCU row
+// uses a prefix of the same entries.
+__device__ __forceinline__ void cj_pixel_setup(const CJScanParams& prmr, const CJPixGeom& g, CJPixSmemParams* Pp) {
+  const CJScanParams* prm = &prmr;
+  CJPixSmemParams& P = *Pp;
+  const int nblk = g.T * g.bpm;
+  for (int k = threadIdx.x; k < 4 * 64; k += blockDim.x) P.q[k >> 6][k & 63] = prm->qnat[k >> 6][k & 63];
+  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
+    const int mi = k / g.bpm, ph = k - mi * g.bpm;
+    const int c = prm->phase_comp[ph], bl = prm->phase_blk[ph], sxc = prm->comp_sx[c];
+    const int bx = mi * sxc + bl % sxc, by = bl / sxc;
+    const int base = c == 0 ? g.y_off : (c == 1 ? g.cb_off : g.cr_off);
+    const int ps = c == 0 ? g.y_stride : g.c_stride;
+    P.boff[k] = (uint16_t)(base + by * 8 * ps + bx * 8);
+    P.bc[k] = (uint8_t)c;
+    P.bq[k] = prm->comp_q[c];
+  }
+}
+
+// One tile (after cj_pixel_setup for its image), MCU row `mrow`, MCUs
+// [mc0, mc0 + T), whose coefficients arrive
 // in `sc` on phase `parity` of `bar`: dequantise + integer iDCT into plane
 // tiles, then nearest upsampling + YCbCr->RGB (or a grey copy) into `out`.
 // Returns false if the copy did not land within the wait bound (recorded).
@@ -181,18 +214,6 @@ __device__ __forceinline__ bool cj_pixel_compute(const CJScanParams& prmr, uint8
   uint8_t* py = smem + g.y_off;
   uint8_t* pcb = smem + g.cb_off;
   uint8_t* pcr = smem + g.cr_off;
-  for (int k = threadIdx.x; k < 4 * 64; k += blockDim.x) P.q[k >> 6][k & 63] = prm->qnat[k >> 6][k & 63];
-  // per-block destination table (one division per block, not per row)
-  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
-    const int mi = k / g.bpm, ph = k - mi * g.bpm;
-    const int c = prm->phase_comp[ph], bl = prm->phase_blk[ph], sxc = prm->comp_sx[c];
-    const int bx = mi * sxc + bl % sxc, by = bl / sxc;
-    const int base = c == 0 ? g.y_off : (c == 1 ? g.cb_off : g.cr_off);
-    const int ps = c == 0 ? g.y_stride : g.c_stride;
-    P.boff[k] = (uint16_t)(base + by * 8 * ps + bx * 8);
-    P.bc[k] = (uint8_t)c;
-    P.bq[k] = prm->comp_q[c];
-  }
   bool ok = cj_mbar_wait(barp, parity);
   if (!__syncthreads_and(ok)) {
     if (threadIdx.x == 0) atomicMax(&st->dec_err_key, ~((unsigned long long)CJ_DEV_CAPACITY));
@@ -214,18 +235,24 @@ __device__ __forceinline__ bool cj_pixel_compute(const CJScanParams& prmr, uint8
   }
   __syncthreads();
 
-  // Column pass: one thread per (block, column); 8 samples into the plane tile.
-  for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
-    const int k = t >> 3, col = t & 7;
-    int d[8];
+  // Column pass: one thread per (block, column pair); the two columns' 8
+  // samples go into the plane tile as one 16-bit store per row.
+  for (int t = threadIdx.x; t < nblk * 4; t += blockDim.x) {
+    const int k = t >> 2, c0 = (t & 3) * 2;
+    int d0[8], d1[8];
 #pragma unroll
-    for (int j = 0; j < 8; j++) d[j] = tmp[k * CJ_TMP_STRIDE + j * 8 + col];
-    uint32_t o[8];
-    cj_idct_col(d, o);
+    for (int j = 0; j < 8; j++) {
+      const int2 v = *reinterpret_cast<const int2*>(tmp + k * CJ_TMP_STRIDE + j * 8 + c0);
+      d0[j] = v.x;
+      d1[j] = v.y;
+    }
+    int o0[8], o1[8];
+    cj_idct_col_s(d0, o0);
+    cj_idct_col_s(d1, o1);
     const int ps = P.bc[k] == 0 ? g.y_stride : g.c_stride;
-    uint8_t* dst = smem + P.boff[k] + col;
+    uint8_t* dst = smem + P.boff[k] + c0;
 #pragma unroll
-    for (int j = 0; j < 8; j++) dst[j * ps] = (uint8_t)o[j];
+    for (int j = 0; j < 8; j++) *reinterpret_cast<uint16_t*>(dst + j * ps) = (uint16_t)cj_level2(o0[j], o1[j]);
   }
   __syncthreads();
 

@@ -33,6 +33,7 @@ k_pixel(const CJScanParams* __restrict__ prm, const int16_t* __restrict__ coef,
     cj_pixel_issue(coef, g, blockIdx.y, blockIdx.x * g.T, reinterpret_cast<int16_t*>(smem), &bar);
   }
   __syncthreads();
+  cj_pixel_setup(*prm, g, &P);
   cj_pixel_compute(*prm, out, st, g, blockIdx.y, blockIdx.x * g.T, reinterpret_cast<int16_t*>(smem), smem,
                    &bar, 0, &P);
 }
