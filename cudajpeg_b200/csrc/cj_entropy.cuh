@@ -100,13 +100,20 @@ __device__ __forceinline__ CJLane cj_lane(const CJSegment* segs, int nseg, int n
 // Bit reader of the decode loops: the current and the next big-endian word
 // and a bit offset; a 32-bit window is one funnel shift, and a word boundary
 // is crossed at most once per symbol (a symbol consumes at most 31 bits).
+// One more word is loaded a crossing ahead and kept as read from memory
+// (byte-swapped only when it becomes the next word), so a load has several
+// symbols to arrive before the window needs it.
 // Bytes at or past `end_byte` read as 0xFF, as in CJBits.
 struct CJFBits {
   const uint32_t* words;
-  uint32_t wfull, end_byte, cur, nxt, wi, off;
+  uint32_t wfull, end_byte, cur, nxt, raw2, wi, off;
 
   __device__ __forceinline__ uint32_t word(uint32_t i) const {
     return i < wfull ? cj_bswap(words[i]) : cj_word(words, i, end_byte);
+  }
+  // word i as stored (cj_bswap of it is word(i))
+  __device__ __forceinline__ uint32_t word_raw(uint32_t i) const {
+    return i < wfull ? words[i] : cj_bswap(cj_word(words, i, end_byte));
   }
   __device__ __forceinline__ void init(const uint32_t* w, uint64_t eb, uint64_t p) {
     words = w;
@@ -117,6 +124,7 @@ struct CJFBits {
     cur = word(w0);
     wi = w0 + 1;
     nxt = word(wi);
+    raw2 = word_raw(wi + 1);
   }
   __device__ __forceinline__ uint32_t peek() const { return __funnelshift_l(nxt, cur, off); }
   __device__ __forceinline__ void skip(uint32_t u) {
@@ -124,8 +132,9 @@ struct CJFBits {
     if (off >= 32) {
       off -= 32;
       cur = nxt;
+      nxt = cj_bswap(raw2);
       wi++;
-      nxt = word(wi);
+      raw2 = word_raw(wi + 1);
     }
   }
   __device__ __forceinline__ uint64_t pos() const { return ((uint64_t)(wi - 1) << 5) + off; }
