@@ -212,7 +212,7 @@ __device__ __forceinline__ int bt_find(int n, int v, F key) {
   return lo;
 }
 
-// Step tables of the entropy phases, staged per item group: a group's warps
+// Step tables of the sync and fix-up phases, staged per item group: a group's warps
 // [wa, wb] span few images, and the step tables of the first and the last
 // of them are copied into shared memory (slots 0 and 1), so every symbol
 // lookup is a shared-memory load instead of an L2 round trip (the tables of
@@ -221,7 +221,13 @@ __device__ __forceinline__ int bt_find(int n, int v, F key) {
 struct BTStaged {
   int ia, ib;
 };
+// Dynamic shared memory of the decode kernel: two staged table slots in the
+// sync and fix-up phases, the write-out's block buffers (one 64-entry int16
+// block per thread) in phase 8.  More would shrink the L1 share the
+// bitstream reads of the sync phase depend on.
+#define BT_WBUF_BYTES (BT_THREADS * 64 * 2)
 #define BT_DECODE_SMEM (2 * sizeof(CJSteps))
+static_assert(BT_DECODE_SMEM >= BT_WBUF_BYTES, "write-out block buffers");
 static_assert(sizeof(CJSteps) % 16 == 0 && offsetof(CJScanParams, steps) % 16 == 0, "int4 table copy");
 static_assert(BT_DECODE_SMEM >= BT_THREADS * sizeof(CJAgg5), "phase 7 scan space");
 
@@ -676,18 +682,19 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   // stops at checkpoint q's block boundary (the last unit at the lane's end),
   // so write items are a quarter as long as sync items whatever the
   // subsequence size.  An item is 8 lanes x 4 units of one 32-lane warp w,
-  // whose block / DC prefix it recomputes.  (In a corrupt stream a unit may
+  // whose block / DC prefix it recomputes; the warp writes its 32 units'
+  // blocks cooperatively (cj_write_units_warp).  (In a corrupt stream a unit may
   // write past an error an earlier unit stopped at; only blocks after that
   // error, so the first error of the image is the same.)
   {
     constexpr int UNITS = CJ_CKPTS + 1, LANES = 32 / UNITS;
     const int nitems = a.nwarps * UNITS;
-    for (;;) {
-      const int g0 = bt_next_group(&a.ctl->next_write, &s_grp);
-      if (g0 >= nitems) break;
-      const BTStaged sg = bt_stage(a, g0 / UNITS, (min(g0 + BT_WARPS, nitems) - 1) / UNITS, tab);
-      const int t = g0 + (int)(threadIdx.x >> 5);
-      if (t >= nitems) continue;  // warp-uniform
+    // the warp's block buffers, zero between blocks (the step tables are read
+    // from global memory here: the buffers take the staging space)
+    int16_t* wbuf = reinterpret_cast<int16_t*>(smem) + (threadIdx.x >> 5) * 32 * 64;
+    for (int k = lane; k < 32 * 64 * 2 / 16; k += 32) reinterpret_cast<uint4*>(wbuf)[k] = make_uint4(0, 0, 0, 0);
+    __syncwarp();
+    for (int t = bt_next_item(&a.ctl->next_write); t < nitems; t = bt_next_item(&a.ctl->next_write)) {
       const int w = t / UNITS, part = t % UNITS;
       const int i = bt_image_of_warp(a, w);
       const CJImageDesc& d = a.desc[i];
@@ -696,7 +703,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       const int j0 = w * 32 - d.sub0;
       if (j0 >= nsub) continue;
       const CJScanParams& sp = a.prm[i];
-      const CJSteps& T = bt_steps_of(a, sg, tab, i);
+      const CJSteps& T = sp.steps;
       const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
       // block / DC prefix of the 32 lanes of warp w (thread = lane `lane`)
       const CJLane lw = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
@@ -741,9 +748,8 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
           end = cj_lane_write_end(ln, seg, r, lane_first);
         }
       }
-      cj_warp_zero_range(a.coef + d.coef0 * 64, ln.active, first, end);
-      if (!ln.active) continue;
-      cj_write_lane(sp, T, words, ln, seg, start, first, dc0, dc1, dc2, a.coef + d.coef0 * 64, st, s_zz, stop);
+      cj_write_units_warp(sp, T, words, ln, seg, start, first, dc0, dc1, dc2, a.coef + d.coef0 * 64, st, s_zz, stop,
+                          end, ln.active, wbuf);
     }
   }
 }
@@ -756,6 +762,18 @@ static bt_decode_fn bt_decode_kernel(int ctas_per_sm) {
     case 5: return k_decode_batch<5>;
     default: return k_decode_batch<4>;
   }
+}
+
+// The decode kernels' dynamic shared memory is above the 48 KB a launch gets
+// without opting in.
+static cudaError_t bt_decode_attrs() {
+  const int bytes = (int)BT_DECODE_SMEM;
+  cudaError_t e = cudaFuncSetAttribute(k_decode_batch<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_decode_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_decode_batch<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
 }
 
 __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int t1, uint8_t* smem,
@@ -940,6 +958,7 @@ static int bt_init(CJBatch* b) {
   CJ_CUDA_TRY(cudaEventCreate(&b->ev1), CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaFuncSetAttribute(k_pixel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
               CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(bt_decode_attrs(), CUDA_MEM_ERROR);
   b->parser = newJPGReader();
   if (!b->parser) return OOM_ERROR;
   b->ready = true;
@@ -1513,6 +1532,7 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
     }
     CJ_CUDA_TRY(cudaFuncSetAttribute(k_pixel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
                 CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(bt_decode_attrs(), CUDA_MEM_ERROR);
     g_noalloc_ptr[dev] = (unsigned char*)p;
   }
   unsigned char* base = g_noalloc_ptr[dev];

@@ -404,6 +404,132 @@ __device__ __forceinline__ int64_t cj_lane_write_end(const CJLane& ln, const CJS
   return end > bend ? bend : end;
 }
 
+// Warp-cooperative write-out of 32 units (one per lane; `active` = false for
+// lanes without one), symbol for symbol the decode of cj_write_lane with the
+// same structural checks.  Each lane builds its current block in its own
+// 64-entry int16 buffer in shared memory (`wbuf` + lane * 64, all zero on
+// entry and on return).  After every symbol the warp stores the blocks its
+// lanes completed in that step: 8 lanes per block, 4 blocks per round, one
+// 16-byte store each -- a whole 128-byte line per block instead of one
+// scattered 2-byte store per coefficient -- and clears those buffers.  Blocks
+// go to memory whole, so the range needs no zero fill; a unit that stops at
+// an error stores its partial block (as cj_write_lane leaves it) and zeroes
+// the rest of its range, up to `zero_end`.
+__device__ __forceinline__ void cj_write_units_warp(const CJScanParams& sp, const CJSteps& T, const uint32_t* words,
+                                                    const CJLane& ln, const CJSegment& seg, uint64_t start,
+                                                    int64_t first_block, int dc0, int dc1, int dc2,
+                                                    int16_t* __restrict__ coef, CJStatus* st, const uint8_t* zz,
+                                                    uint64_t stop, int64_t zero_end, bool active, int16_t* wbuf) {
+  const int lane = threadIdx.x & 31;
+  int16_t* mine = wbuf + lane * 64;
+  int64_t b = first_block;
+  const int64_t bend = seg.first_block + seg.nblocks;
+  const uint64_t seg_end = seg.bit_end;
+  const int bpm = sp.bpm;
+  const uint64_t pack = sp.phase_pack;
+  CJFBits br;
+  uint32_t m = 0, aslot = 0, slot = 0;
+  int c = 0;
+  if (active) {
+    br.init(words, ln.end_byte, cj_state_bit(start));
+    m = cj_state_phase(start);
+    cj_phase(sp, bpm, pack, m, c, slot, aslot);
+  }
+  int k = -1;
+  int32_t dd = 0;
+  bool cut = false;  // stopped inside block b at an error
+  // the structural checks made before every block; false = stop here
+  auto block_start = [&]() -> bool {
+    const uint64_t p = br.pos();
+    if (p >= stop) return false;  // the next unit's first block
+    if (!ln.last && p >= ln.end) return false;
+    if (b >= bend) {
+      if (!ln.last) cj_raise_dec(st, b, CJ_DEV_EXTRA);
+      else if (seg.marker_follows) {
+        if (((p + 7) >> 3) != ln.end_byte) cj_raise_dec(st, b, CJ_DEV_TRAILING);
+      } else if (ln.end_byte > ((p + 7) >> 3) + 2) {
+        cj_raise_dec(st, b, CJ_DEV_TRAILING);
+      }
+      return false;
+    }
+    if (seg.marker_follows && p >= seg_end) {
+      cj_raise_dec(st, b, CJ_DEV_OVERRUN);
+      return false;
+    }
+    return true;
+  };
+  bool run = active && block_start();
+  for (;;) {
+    int64_t done = -1;  // block to store after this step
+    if (run) {
+      const uint32_t v = br.peek();
+      const uint32_t stp = cj_step(T, sp, slot, v);
+      const uint32_t dk = (stp >> 5) & 127, size = stp >> 12, total = stp & 31;
+      const int kn = k + (int)dk;
+      const uint32_t len = total - size;
+      const int32_t val = size ? cj_extend((v << len) >> (32 - size), size) : 0;
+      if (k < 0) dd = val;
+      else if (size && kn <= 63) mine[zz[kn]] = (int16_t)val;
+      br.skip(total - (kn > 63 ? size : 0u));
+      slot = aslot;
+      if (kn < 63) {
+        k = kn;
+      } else if (kn > 63 && dk != CJ_STEP_EOB) {  // failing symbol: the block is cut here
+        cj_raise_dec(st, b, dk == CJ_STEP_NO_CODE ? CJ_DEV_BAD_CODE : CJ_DEV_BAD_AC);
+        done = b;
+        cut = true;
+        run = false;
+      } else if (seg.marker_follows && br.pos() > seg_end) {
+        cj_raise_dec(st, b, CJ_DEV_OVERRUN);
+        done = b;
+        cut = true;
+        run = false;
+      } else {
+        int dcv;
+        if (c == 0) dcv = dc0 += dd;
+        else if (c == 1) dcv = dc1 += dd;
+        else dcv = dc2 += dd;
+        if (dcv < -32768 || dcv > 32767) {
+          cj_raise_dec(st, b, CJ_DEV_DC_RANGE);
+          cut = true;
+          run = false;
+        } else {
+          mine[0] = (int16_t)dcv;
+          b++;
+          m = (m + 1 == (uint32_t)bpm) ? 0 : m + 1;
+          cj_phase(sp, bpm, pack, m, c, slot, aslot);
+          k = -1;
+          run = block_start();
+        }
+        done = cut ? b : b - 1;
+      }
+    }
+    unsigned mask = __ballot_sync(CJ_FULL, done >= 0);
+    __syncwarp();
+    while (mask) {  // warp-uniform
+      unsigned mm = mask;
+      for (int i = 0; i < (lane >> 3); i++) mm &= mm - 1;
+      const int src = mm ? __ffs(mm) - 1 : -1;
+      const long long bsrc = __shfl_sync(CJ_FULL, (long long)done, src < 0 ? 0 : src);
+      if (src >= 0) {
+        uint4* s = reinterpret_cast<uint4*>(wbuf + src * 64) + (lane & 7);
+        reinterpret_cast<uint4*>(coef + bsrc * 64)[lane & 7] = *s;
+        *s = make_uint4(0, 0, 0, 0);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; i++) mask &= mask - 1;
+    }
+    __syncwarp();
+    if (!__any_sync(CJ_FULL, run)) break;
+  }
+  // blocks of the range an early stop left undecoded read as zeros
+  for (int64_t x = cut ? b + 1 : b; active && x < zero_end; x++) {
+    uint4* p = reinterpret_cast<uint4*>(coef + x * 64);
+#pragma unroll
+    for (int i = 0; i < 8; i++) p[i] = make_uint4(0, 0, 0, 0);
+  }
+}
+
 // Final decode of one lane from its settled start: writes quantised int16
 // coefficients (natural order) of its blocks, DC predicted per component,
 // and records structural errors of its restart interval.  `zz` is the
