@@ -381,9 +381,13 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   bt_grid_sync(a.ctl, gen);
 
   bt_stamp(a.ctl, 1);
-  // ---- phase 1: destuff count
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    int i = bt_find(a.n, t, [&](int k) { return a.desc[k].tile0; });
+  // ---- phase 1: destuff count.  Each CTA takes a contiguous run of tiles
+  // (equal 4 KB pieces), so the image index only walks forward.
+  const int tper = (a.ntiles + gridDim.x - 1) / gridDim.x;
+  const int tt0 = blockIdx.x * tper, tt1 = min(tt0 + tper, a.ntiles);
+  const int timg0 = tt0 < tt1 ? bt_find(a.n, tt0, [&](int k) { return a.desc[k].tile0; }) : 0;
+  for (int t = tt0, i = timg0; t < tt1; t++) {
+    while (t >= a.desc[i].tile0 + a.desc[i].ntiles) i++;
     const CJImageDesc& d = a.desc[i];
     int64_t base = (int64_t)(t - d.tile0) * BT_TILE_BYTES + threadIdx.x * 16;
     CJChunk c = cj_classify(a.blob + d.src_off, d.raw_len, base);
@@ -423,28 +427,49 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   bt_grid_sync(a.ctl, gen);
 
   bt_stamp(a.ctl, 3);
-  // ---- phase 3: destuff scatter
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    int i = bt_find(a.n, t, [&](int k) { return a.desc[k].tile0; });
+  // ---- phase 3: destuff scatter, over the same tile runs.  A tile's kept
+  // bytes are compacted in shared memory and then written to their
+  // contiguous destination [o0, o0 + n) as aligned 4-byte words; only the
+  // partial words at the two ends, which may border another tile's bytes,
+  // are written byte by byte.
+  for (int t = tt0, i = timg0; t < tt1; t++) {
+    while (t >= a.desc[i].tile0 + a.desc[i].ntiles) i++;
     const CJImageDesc& d = a.desc[i];
     int64_t base = (int64_t)(t - d.tile0) * BT_TILE_BYTES + threadIdx.x * 16;
     CJChunk c = cj_classify(a.blob + d.src_off, d.raw_len, base);
     int2 tot;
     int2 ex = cj_block_exclusive(make_int2(__popc(c.keep), __popc(c.mark)), sm2, &tot);
-    int64_t o = (int64_t)__ldcg(&a.tile_keep[t]) + ex.x;
+    const int64_t o0 = (int64_t)__ldcg(&a.tile_keep[t]);
+    int q = ex.x;
     int r = __ldcg(&a.tile_mark[t]) + ex.y;
-    uint8_t* out = a.data + d.data_off;
 #pragma unroll
     for (int j = 0; j < 16; j++) {
-      if (c.keep & (1u << j)) out[o++] = (uint8_t)cj_byte(c, j);
+      if (c.keep & (1u << j)) smem[q++] = (uint8_t)cj_byte(c, j);
       if (c.mark & (1u << j)) {
         if (r < d.mark_cap) {
-          a.mpos[d.mark0 + r] = (uint32_t)o;
+          a.mpos[d.mark0 + r] = (uint32_t)(o0 + q);
           a.mcode[d.mark0 + r] = (uint8_t)(j < 15 ? cj_byte(c, j + 1) : c.next);
         }
         r++;
       }
     }
+    __syncthreads();
+    uint8_t* out = a.data + d.data_off;
+    const int n = tot.x;
+    const int64_t wb = (o0 + 3) >> 2, we = (o0 + n) >> 2;  // words wholly inside the range
+    if (wb < we) {
+      for (int64_t w = wb + threadIdx.x; w < we; w += BT_THREADS) {
+        const int sofs = (int)(4 * w - o0);
+        reinterpret_cast<uint32_t*>(out)[w] = (uint32_t)smem[sofs] | ((uint32_t)smem[sofs + 1] << 8) |
+                                              ((uint32_t)smem[sofs + 2] << 16) | ((uint32_t)smem[sofs + 3] << 24);
+      }
+      const int head = (int)(4 * wb - o0), tail = (int)(o0 + n - 4 * we);
+      if ((int)threadIdx.x < head) out[o0 + threadIdx.x] = smem[threadIdx.x];
+      if ((int)threadIdx.x < tail) out[4 * we + threadIdx.x] = smem[4 * we - o0 + threadIdx.x];
+    } else {
+      for (int k = threadIdx.x; k < n; k += BT_THREADS) out[o0 + k] = smem[k];
+    }
+    __syncthreads();
   }
   bt_grid_sync(a.ctl, gen);
 
