@@ -460,7 +460,7 @@ __device__ __forceinline__ void cj_write_units_warp(const CJScanParams& sp, cons
   };
   bool run = active && block_start();
   for (;;) {
-    int64_t done = -1;  // block to store after this step
+    int done = -1;  // block (of this image) to store after this step
     if (run) {
       const uint32_t v = br.peek();
       const uint32_t stp = cj_step(T, sp, slot, v);
@@ -476,12 +476,12 @@ __device__ __forceinline__ void cj_write_units_warp(const CJScanParams& sp, cons
         k = kn;
       } else if (kn > 63 && dk != CJ_STEP_EOB) {  // failing symbol: the block is cut here
         cj_raise_dec(st, b, dk == CJ_STEP_NO_CODE ? CJ_DEV_BAD_CODE : CJ_DEV_BAD_AC);
-        done = b;
+        done = (int)b;
         cut = true;
         run = false;
       } else if (seg.marker_follows && br.pos() > seg_end) {
         cj_raise_dec(st, b, CJ_DEV_OVERRUN);
-        done = b;
+        done = (int)b;
         cut = true;
         run = false;
       } else {
@@ -501,23 +501,28 @@ __device__ __forceinline__ void cj_write_units_warp(const CJScanParams& sp, cons
           k = -1;
           run = block_start();
         }
-        done = cut ? b : b - 1;
+        done = (int)(cut ? b : b - 1);
       }
     }
     unsigned mask = __ballot_sync(CJ_FULL, done >= 0);
     __syncwarp();
-    while (mask) {  // warp-uniform
-      unsigned mm = mask;
-      for (int i = 0; i < (lane >> 3); i++) mm &= mm - 1;
-      const int src = mm ? __ffs(mm) - 1 : -1;
-      const long long bsrc = __shfl_sync(CJ_FULL, (long long)done, src < 0 ? 0 : src);
+    while (mask) {  // warp-uniform: up to 4 blocks per round, lanes 8j..8j+7 take the j-th
+      const int s0 = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const int s1 = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const int s2 = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const int s3 = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const int j = lane >> 3;
+      const int src = j == 0 ? s0 : (j == 1 ? s1 : (j == 2 ? s2 : s3));
+      const int bsrc = __shfl_sync(CJ_FULL, done, src < 0 ? 0 : src);
       if (src >= 0) {
         uint4* s = reinterpret_cast<uint4*>(wbuf + src * 64) + (lane & 7);
-        reinterpret_cast<uint4*>(coef + bsrc * 64)[lane & 7] = *s;
+        reinterpret_cast<uint4*>(coef + (int64_t)bsrc * 64)[lane & 7] = *s;
         *s = make_uint4(0, 0, 0, 0);
       }
-#pragma unroll
-      for (int i = 0; i < 4; i++) mask &= mask - 1;
     }
     __syncwarp();
     if (!__any_sync(CJ_FULL, run)) break;
