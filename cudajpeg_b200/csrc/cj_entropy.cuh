@@ -22,26 +22,45 @@ __device__ __forceinline__ uint32_t cj_byte(const CJChunk& c, int j) {
   return (c.w[j >> 2] >> (8 * (j & 3))) & 0xFF;
 }
 
+// The chunk's 16 bytes and the one after it come from the two aligned
+// 16-byte words around them (funnel shifts), whatever the chunk's alignment:
+// for a chunk that starts inside the data (base < n) they lie below
+// raw + n + 31, and the callers' buffers hold at least 31 bytes past the
+// data and start on a 16-byte boundary; bytes at or past n read as 0.
 __device__ __forceinline__ CJChunk cj_classify(const uint8_t* raw, int64_t n, int64_t base) {
   CJChunk c;
   c.keep = c.mark = 0;
   c.bad = false;
-  if (base + 16 <= n && (((uintptr_t)(raw + base)) & 15) == 0) {
-    uint4 v = *reinterpret_cast<const uint4*>(raw + base);
-    c.w[0] = v.x; c.w[1] = v.y; c.w[2] = v.z; c.w[3] = v.w;
-  } else {
+  c.w[0] = c.w[1] = c.w[2] = c.w[3] = 0;
+  c.next = 0;
+  if (base < n) {
+    const uintptr_t addr = (uintptr_t)(raw + base);
+    const uint4* q = reinterpret_cast<const uint4*>(addr & ~(uintptr_t)15);
+    const uint4 lo = q[0], hi = q[1];
+    const uint32_t sh = (uint32_t)(addr & 15), bs = (sh & 3) * 8;
+    uint32_t a0, a1, a2, a3, a4, a5;
+    switch (sh >> 2) {
+      case 0: a0 = lo.x; a1 = lo.y; a2 = lo.z; a3 = lo.w; a4 = hi.x; a5 = hi.y; break;
+      case 1: a0 = lo.y; a1 = lo.z; a2 = lo.w; a3 = hi.x; a4 = hi.y; a5 = hi.z; break;
+      case 2: a0 = lo.z; a1 = lo.w; a2 = hi.x; a3 = hi.y; a4 = hi.z; a5 = hi.w; break;
+      default: a0 = lo.w; a1 = hi.x; a2 = hi.y; a3 = hi.z; a4 = hi.w; a5 = 0; break;
+    }
+    c.w[0] = __funnelshift_r(a0, a1, bs);
+    c.w[1] = __funnelshift_r(a1, a2, bs);
+    c.w[2] = __funnelshift_r(a2, a3, bs);
+    c.w[3] = __funnelshift_r(a3, a4, bs);
+    // byte 16 of the chunk: byte 0 of the next word
+    const uint32_t after = __funnelshift_r(a4, a5, bs) & 0xFF;
+    c.next = (base + 16 < n) ? after : 0;
+    if (base + 16 > n) {
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      uint32_t x = 0;
-#pragma unroll
-      for (int b = 0; b < 4; b++) {
-        int64_t q = base + 4 * k + b;
-        if (q < n) x |= (uint32_t)raw[q] << (8 * b);
+      for (int k = 0; k < 4; k++) {
+        const int64_t valid = n - (base + 4 * k);  // bytes of word k below n
+        if (valid <= 0) c.w[k] = 0;
+        else if (valid < 4) c.w[k] &= (1u << (8 * valid)) - 1u;
       }
-      c.w[k] = x;
     }
   }
-  c.next = (base + 16 < n) ? raw[base + 16] : 0;
   uint32_t prev = (base > 0 && base - 1 < n) ? raw[base - 1] : 0;
 #pragma unroll
   for (int j = 0; j < 16; j++) {
