@@ -386,11 +386,22 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   const int tper = (a.ntiles + gridDim.x - 1) / gridDim.x;
   const int tt0 = blockIdx.x * tper, tt1 = min(tt0 + tper, a.ntiles);
   const int timg0 = tt0 < tt1 ? bt_find(a.n, tt0, [&](int k) { return a.desc[k].tile0; }) : 0;
+  // a tile's chunk (tile t of the run, image index i walking forward)
+  auto tile_in = [&](int t, int& i) -> CJChunkIn {
+    while (t >= a.desc[i].tile0 + a.desc[i].ntiles) i++;
+    const CJImageDesc& d = a.desc[i];
+    return cj_chunk_load(a.blob + d.src_off, d.raw_len, (int64_t)(t - d.tile0) * BT_TILE_BYTES + threadIdx.x * 16);
+  };
+  int pi = timg0;  // image of the prefetched tile
+  CJChunkIn nx;
+  if (tt0 < tt1) nx = tile_in(tt0, pi);
   for (int t = tt0, i = timg0; t < tt1; t++) {
     while (t >= a.desc[i].tile0 + a.desc[i].ntiles) i++;
     const CJImageDesc& d = a.desc[i];
     int64_t base = (int64_t)(t - d.tile0) * BT_TILE_BYTES + threadIdx.x * 16;
-    CJChunk c = cj_classify(a.blob + d.src_off, d.raw_len, base);
+    const CJChunkIn in = nx;
+    if (t + 1 < tt1) nx = tile_in(t + 1, pi);  // the next tile's load overlaps this one's scan
+    CJChunk c = cj_classify_in(in, d.raw_len, base);
     int2 tot;
     cj_block_exclusive(make_int2(__popc(c.keep), __popc(c.mark)), sm2, &tot);
     if (threadIdx.x == 0) {
@@ -432,11 +443,15 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   // contiguous destination [o0, o0 + n) as aligned 4-byte words; only the
   // partial words at the two ends, which may border another tile's bytes,
   // are written byte by byte.
+  pi = timg0;
+  if (tt0 < tt1) nx = tile_in(tt0, pi);
   for (int t = tt0, i = timg0; t < tt1; t++) {
     while (t >= a.desc[i].tile0 + a.desc[i].ntiles) i++;
     const CJImageDesc& d = a.desc[i];
     int64_t base = (int64_t)(t - d.tile0) * BT_TILE_BYTES + threadIdx.x * 16;
-    CJChunk c = cj_classify(a.blob + d.src_off, d.raw_len, base);
+    const CJChunkIn in = nx;
+    if (t + 1 < tt1) nx = tile_in(t + 1, pi);
+    CJChunk c = cj_classify_in(in, d.raw_len, base);
     int2 tot;
     int2 ex = cj_block_exclusive(make_int2(__popc(c.keep), __popc(c.mark)), sm2, &tot);
     const int64_t o0 = (int64_t)__ldcg(&a.tile_keep[t]);

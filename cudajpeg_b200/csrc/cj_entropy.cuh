@@ -22,22 +22,44 @@ __device__ __forceinline__ uint32_t cj_byte(const CJChunk& c, int j) {
   return (c.w[j >> 2] >> (8 * (j & 3))) & 0xFF;
 }
 
-// The chunk's 16 bytes and the one after it come from the two aligned
-// 16-byte words around them (funnel shifts), whatever the chunk's alignment:
-// for a chunk that starts inside the data (base < n) they lie below
-// raw + n + 31, and the callers' buffers hold at least 31 bytes past the
-// data and start on a 16-byte boundary; bytes at or past n read as 0.
-__device__ __forceinline__ CJChunk cj_classify(const uint8_t* raw, int64_t n, int64_t base) {
+// The memory a chunk is classified from: the two aligned 16-byte words
+// around its 16 bytes and the one after them, and the byte before it.  For a
+// chunk that starts inside the data (base < n) the words lie below
+// raw + n + 31; the callers' buffers hold at least 31 bytes past the data and
+// start on a 16-byte boundary.  Loaded apart from the classification so that
+// a loop can fetch its next chunk early.
+struct CJChunkIn {
+  uint4 lo, hi;
+  uint32_t sh;    // the chunk's offset inside lo
+  uint32_t prev;  // the byte before the chunk (0 at the start)
+};
+
+__device__ __forceinline__ CJChunkIn cj_chunk_load(const uint8_t* raw, int64_t n, int64_t base) {
+  CJChunkIn x;
+  x.lo = x.hi = make_uint4(0, 0, 0, 0);
+  x.sh = 0;
+  if (base < n) {
+    const uintptr_t addr = (uintptr_t)(raw + base);
+    const uint4* q = reinterpret_cast<const uint4*>(addr & ~(uintptr_t)15);
+    x.lo = q[0];
+    x.hi = q[1];
+    x.sh = (uint32_t)(addr & 15);
+  }
+  x.prev = (base > 0 && base - 1 < n) ? raw[base - 1] : 0;
+  return x;
+}
+
+// Classify a loaded chunk: its bytes come out of the two words by funnel
+// shifts, whatever its alignment; bytes at or past n read as 0.
+__device__ __forceinline__ CJChunk cj_classify_in(const CJChunkIn& x, int64_t n, int64_t base) {
   CJChunk c;
   c.keep = c.mark = 0;
   c.bad = false;
   c.w[0] = c.w[1] = c.w[2] = c.w[3] = 0;
   c.next = 0;
   if (base < n) {
-    const uintptr_t addr = (uintptr_t)(raw + base);
-    const uint4* q = reinterpret_cast<const uint4*>(addr & ~(uintptr_t)15);
-    const uint4 lo = q[0], hi = q[1];
-    const uint32_t sh = (uint32_t)(addr & 15), bs = (sh & 3) * 8;
+    const uint4 lo = x.lo, hi = x.hi;
+    const uint32_t sh = x.sh, bs = (sh & 3) * 8;
     uint32_t a0, a1, a2, a3, a4, a5;
     switch (sh >> 2) {
       case 0: a0 = lo.x; a1 = lo.y; a2 = lo.z; a3 = lo.w; a4 = hi.x; a5 = hi.y; break;
@@ -61,7 +83,7 @@ __device__ __forceinline__ CJChunk cj_classify(const uint8_t* raw, int64_t n, in
       }
     }
   }
-  uint32_t prev = (base > 0 && base - 1 < n) ? raw[base - 1] : 0;
+  uint32_t prev = x.prev;
 #pragma unroll
   for (int j = 0; j < 16; j++) {
     if (base + j >= n) break;
@@ -81,6 +103,10 @@ __device__ __forceinline__ CJChunk cj_classify(const uint8_t* raw, int64_t n, in
     prev = b;
   }
   return c;
+}
+
+__device__ __forceinline__ CJChunk cj_classify(const uint8_t* raw, int64_t n, int64_t base) {
+  return cj_classify_in(cj_chunk_load(raw, n, base), n, base);
 }
 
 struct CJLane {
