@@ -624,7 +624,7 @@ __device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const CJSt
       cj_raise_dec(st, b, CJ_DEV_OVERRUN);
       return false;
     }
-    blk = coef + b * 64;  // zeroed beforehand by cj_warp_zero_blocks
+    blk = coef + b * 64;  // zeroed beforehand by cj_warp_zero_range
     return true;
   };
   if (!block_start()) return;
