@@ -144,8 +144,17 @@ __device__ __forceinline__ void bt_grid_sync(CJBatchCtl* ctl, unsigned& gen) {
       __threadfence();
       atomicAdd(&ctl->bar_gen, 1);
     } else {
-      unsigned it = 0;
-      while (atomicAdd(&ctl->bar_gen, 0) == g) {
+      // poll with a relaxed load, not an atomic: hundreds of CTAs polling
+      // one word by atomics serialise at its L2 slice, and the releasing
+      // CTA's atomics then queue behind them (tens of microseconds when most
+      // CTAs wait long, as in the fix-up passes).  Not an acquire load
+      // either: each would invalidate the SM's L1 under the warps of other
+      // CTAs still working there.  The fence after the loop orders what
+      // follows (the releasing CTA fenced before its increment).
+      unsigned it = 0, v;
+      for (;;) {
+        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(&ctl->bar_gen) : "memory");
+        if (v != g) break;
         if (++it > (1u << 24)) {
           atomicExch(&ctl->timeout, 1);
           break;
@@ -673,7 +682,9 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       }
     }
     bt_grid_sync(a.ctl, gen);
-    if (atomicAdd(unstable, 0) == 0) break;
+    // the barrier orders every increment before this read; a load, not an
+    // atomic (one per thread of the grid would serialise at the word's slice)
+    if (__ldcg(unstable) == 0) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->passes = pass + 1;
   // the last pass wrote its exits into the other snapshot; nothing reads them
