@@ -287,6 +287,13 @@ def read_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
+def traffic_key(workload: str, batch_size: int) -> str:
+    """Name of the committed ncu summary that holds DRAM bytes per launch for
+    this run: the summaries are captured on the default 1024-image batch, so
+    other batch sizes look for a summary of their own (and report null)."""
+    return workload if batch_size == 1024 else f"{workload}_{batch_size}"
+
+
 def read_traffic(kernel: str, workload: str):
     """DRAM bytes per launch from the committed ncu summary, if present."""
     p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
@@ -465,8 +472,7 @@ def run_batch(args, wl, world, rank, local, dist):
     alg_decode = st_run["input_bytes"] + 3 * st_run["scan_bytes"] + coef_bytes
     alg_pixel = coef_bytes + st_run["output_bytes"]
     ach_decode = alg_decode / (decode_ms / 1e3) / 1e9
-    # the committed DRAM figures are per launch of the default 1024-image batch
-    traffic_key = args.workload if args.batch_size == 1024 else f"{args.workload}_{args.batch_size}"
+    tkey = traffic_key(args.workload, args.batch_size)
     ach_pixel = alg_pixel / (pixel_ms / 1e3) / 1e9
     line = {"metric": METRIC, "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean_ms, 4),
@@ -496,13 +502,13 @@ def run_batch(args, wl, world, rank, local, dist):
             "roofline": {"bound": "hbm", "kernel": "k_decode_batch", "achieved": round(ach_decode, 1),
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": round(ach_decode / peaks["hbm_gbs"], 4),
-                         "traffic": read_traffic("k_decode_batch", traffic_key),
+                         "traffic": read_traffic("k_decode_batch", tkey),
                          "algorithmic_bytes": int(alg_decode), "kernel_ms": round(decode_ms, 4),
                          "peak_source": peaks["source"]},
             "roofline_pixel": {"bound": "hbm", "kernel": "k_pixel_batch", "achieved": round(ach_pixel, 1),
                                "peak": peaks["hbm_gbs"], "unit": "GB/s",
                                "frac": round(ach_pixel / peaks["hbm_gbs"], 4),
-                               "traffic": read_traffic("k_pixel_batch", traffic_key),
+                               "traffic": read_traffic("k_pixel_batch", tkey),
                                "algorithmic_bytes": int(alg_pixel), "kernel_ms": round(pixel_ms, 4),
                                "peak_source": peaks["source"]},
             "phase_ms": pm, "gpu_launches": int(launches), "clocks": clocks.summary()}

@@ -97,3 +97,17 @@ def test_bench_workload_shards():
     assert parts[0].pixels + parts[1].pixels == full.pixels
     weak1 = bench.Workload("mixed_batch", 8, 1, 2)
     assert len(weak1.files) == 8 and set(weak1.files).isdisjoint(full.files)
+
+
+def test_bench_traffic_lookup():
+    """The roofline's DRAM traffic comes from the committed ncu summaries of
+    the default 1024-image batch; another batch size finds none."""
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.traffic_key("mixed_batch", 1024) == "mixed_batch"
+    assert bench.traffic_key("mixed_batch", 128) == "mixed_batch_128"
+    for k in ("k_decode_batch", "k_pixel_batch"):
+        v = bench.read_traffic(k, bench.traffic_key("mixed_batch", 1024))
+        assert v is not None and 1e8 < v < 1e10
+        assert bench.read_traffic(k, bench.traffic_key("mixed_batch", 128)) is None
