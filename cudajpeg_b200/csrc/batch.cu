@@ -39,6 +39,11 @@
 #include "cj_tables.h"
 
 #define BT_THREADS 256
+// Default bits per speculative subsequence of a batch: with many images
+// decoding side by side, long subsequences (fewer lanes and settle chains)
+// win; the autotuner chooses 4096 on the mixed 1024-image workload.  The
+// single-image paths keep CJ_SUB_BITS_DEFAULT (more lanes per image).
+#define BT_SUB_BITS_DEFAULT 4096
 #define BT_WARPS (BT_THREADS / 32)
 #define BT_TILE_BYTES 4096  // destuff tile: 256 threads x 16 bytes
 
@@ -943,7 +948,7 @@ struct CJBatch {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // tuning (cjBatchSetTuning / cjBatchAutotune)
-  int sub_bits = CJ_SUB_BITS_DEFAULT;
+  int sub_bits = BT_SUB_BITS_DEFAULT;
   int decode_ctas = BT_DECODE_CTAS_DEFAULT;  // decode-kernel CTAs per SM (3, 4 or 5)
   int tile_cap = 0;                          // max MCUs per pixel tile (0 = layout maximum)
   JPGReader* parser = nullptr;  // host marker parse, one image at a time
@@ -1092,7 +1097,7 @@ void cjBatchDestroy(CJBatch* b) {
 }
 
 int cjBatchSetSubsequenceBits(CJBatch* b, int bits) {
-  if (bits == 0) bits = CJ_SUB_BITS_DEFAULT;
+  if (bits == 0) bits = BT_SUB_BITS_DEFAULT;
   if (bits < 128 || bits > 65536 || (bits & 31)) return PROGRAMMER_ERROR;
   b->sub_bits = bits;
   return 0;

@@ -107,7 +107,7 @@ void cjBatchDestroy(CJBatch *b);
 int cjBatchSetSubsequenceBits(CJBatch *b, int bits);
 
 /* Tuning of later stages/runs: bits per speculative subsequence (0 =
- * default; multiple of 32, 128..65536), decode-kernel CTAs per SM (3, 4 or 5,
+ * default, 4096 for a batch; multiple of 32, 128..65536), decode-kernel CTAs per SM (3, 4 or 5,
  * 0 = 4: the register budget per thread of the entropy kernel, 80/64/48), and
  * the largest pixel tile in MCUs (power of two, 0 = the layout maximum:
  * 128 pixels across). */

@@ -159,7 +159,7 @@ def test_decode_steps_match_reference_lut(cj):
 def test_batch_tuning_validation_without_gpu(cj):
     """cjBatchSetTuning checks its arguments on the host (no device work)."""
     with cj.Batch() as b:
-        assert b.tuning() == {"sub_bits": 1024, "decode_ctas_per_sm": 4, "pixel_tile_cap": 0}
+        assert b.tuning() == {"sub_bits": 4096, "decode_ctas_per_sm": 4, "pixel_tile_cap": 0}
         b.set_tuning(2048, 5, 4)
         assert b.tuning() == {"sub_bits": 2048, "decode_ctas_per_sm": 5, "pixel_tile_cap": 4}
         for bad in [(100, 4, 0), (1000, 4, 0), (1024, 7, 0), (1024, 2, 0), (1024, 4, 3), (1024, 4, -2)]:
