@@ -46,6 +46,7 @@
 #define BT_SUB_BITS_DEFAULT 4096
 #define BT_WARPS (BT_THREADS / 32)
 #define BT_TILE_BYTES 4096  // destuff tile: 256 threads x 16 bytes
+#define BT_TILE_BAD (1 << 30)  // flag in a tile's marker count: malformed FF sequence
 
 // ---------------------------------------------------------------- layouts
 
@@ -392,7 +393,8 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       a.st[i] = z;
     }
   }
-  bt_grid_sync(a.ctl, gen);
+  // no grid barrier: phase 1 reads nothing phase 0 writes (a tile's marker
+  // error goes to its count and reaches the image's status in phase 2)
 
   bt_stamp(a.ctl, 1);
   // ---- phase 1: destuff count.  Each CTA takes a contiguous run of tiles
@@ -418,11 +420,11 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
     CJChunk c = cj_classify_in(in, d.raw_len, base);
     int2 tot;
     cj_block_exclusive(make_int2(__popc(c.keep), __popc(c.mark)), sm2, &tot);
+    const int bad = __syncthreads_or(c.bad);
     if (threadIdx.x == 0) {
       a.tile_keep[t] = tot.x;
-      a.tile_mark[t] = tot.y;
+      a.tile_mark[t] = tot.y | (bad ? BT_TILE_BAD : 0);  // counts stay below 2^13
     }
-    if (c.bad) bt_raise(&a.st[i], 0, CJ_DEV_MARKER);
   }
   bt_grid_sync(a.ctl, gen);
 
@@ -431,10 +433,13 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   for (int i = blockIdx.x; i < a.n; i += gridDim.x) {
     const CJImageDesc& d = a.desc[i];
     int2 run = make_int2(0, 0);
+    int bad = 0;
     for (int t0 = 0; t0 < d.ntiles; t0 += blockDim.x) {
       int t = t0 + threadIdx.x;
       int2 v = make_int2(0, 0);
       if (t < d.ntiles) v = make_int2(__ldcg(&a.tile_keep[d.tile0 + t]), __ldcg(&a.tile_mark[d.tile0 + t]));
+      bad |= v.y & BT_TILE_BAD;
+      v.y &= ~BT_TILE_BAD;
       int2 tot;
       int2 ex = cj_block_exclusive(v, sm2, &tot);
       if (t < d.ntiles) {
@@ -444,6 +449,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       run.x += tot.x;
       run.y += tot.y;
     }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) bt_raise(&a.st[i], 0, CJ_DEV_MARKER);
     if (threadIdx.x == 0) {
       a.st[i].destuffed = run.x;
       a.st[i].nmarkers = run.y;
