@@ -932,7 +932,7 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
     }
     const CJImageDesc& d = a.desc[img];
     const int16_t* sc = reinterpret_cast<const int16_t*>(smem + buf * g.sc1_off);
-    if (!cj_pixel_compute(a.prm[img], a.out + d.out_off, &a.st[img], g, trow, tcol * g.T, sc, smem, &bar2[buf],
+    if (!cj_pixel_compute(a.out + d.out_off, &a.st[img], g, trow, tcol * g.T, sc, smem, &bar2[buf],
                           (par >> buf) & 1u, &P)) {
       if (t + 1 < t1) cj_mbar_wait(&bar2[buf ^ 1], (par >> (buf ^ 1)) & 1u);  // the prefetch in flight
       break;

@@ -202,11 +202,9 @@ __device__ __forceinline__ void cj_pixel_setup(const CJScanParams& prmr, const C
 // tiles, then nearest upsampling + YCbCr->RGB (or a grey copy) into `out`.
 // Returns false if the copy did not land within the wait bound (recorded).
 // Ends with a barrier, so `sc` and the plane tiles are free afterwards.
-__device__ __forceinline__ bool cj_pixel_compute(const CJScanParams& prmr, uint8_t* __restrict__ out,
-                                                 CJStatus* st, const CJPixGeom& g, int mrow, int mc0,
-                                                 const int16_t* sc, uint8_t* smem, uint64_t* barp,
-                                                 uint32_t parity, CJPixSmemParams* Pp) {
-  const CJScanParams* prm = &prmr;
+__device__ __forceinline__ bool cj_pixel_compute(uint8_t* __restrict__ out, CJStatus* st, const CJPixGeom& g,
+                                                 int mrow, int mc0, const int16_t* sc, uint8_t* smem,
+                                                 uint64_t* barp, uint32_t parity, CJPixSmemParams* Pp) {
   CJPixSmemParams& P = *Pp;
   const int nm = min(g.T, g.mcux - mc0);
   const int nblk = nm * g.bpm;

@@ -34,8 +34,7 @@ k_pixel(const CJScanParams* __restrict__ prm, const int16_t* __restrict__ coef,
   }
   __syncthreads();
   cj_pixel_setup(*prm, g, &P);
-  cj_pixel_compute(*prm, out, st, g, blockIdx.y, blockIdx.x * g.T, reinterpret_cast<int16_t*>(smem), smem,
-                   &bar, 0, &P);
+  cj_pixel_compute(out, st, g, blockIdx.y, blockIdx.x * g.T, reinterpret_cast<int16_t*>(smem), smem, &bar, 0, &P);
 }
 
 // Dequantised int32 coefficients in the reference's per-channel layout
