@@ -113,6 +113,18 @@ __device__ __forceinline__ void cj_unpack_dequant(uint4 raw, const int16_t* q, i
   v[7] = (int)(int16_t)(raw.w >> 16) * q[7];
 }
 
+// The same with the quantisation factors already widened to int32.
+__device__ __forceinline__ void cj_unpack_dequant32(uint4 raw, const int* q, int* v) {
+  v[0] = (int)(int16_t)(raw.x & 0xFFFF) * q[0];
+  v[1] = (int)(int16_t)(raw.x >> 16) * q[1];
+  v[2] = (int)(int16_t)(raw.y & 0xFFFF) * q[2];
+  v[3] = (int)(int16_t)(raw.y >> 16) * q[3];
+  v[4] = (int)(int16_t)(raw.z & 0xFFFF) * q[4];
+  v[5] = (int)(int16_t)(raw.z >> 16) * q[5];
+  v[6] = (int)(int16_t)(raw.w & 0xFFFF) * q[6];
+  v[7] = (int)(int16_t)(raw.w >> 16) * q[7];
+}
+
 // FP32 8-point inverse DCT-II: o[x] = sum_u in[u] * basis[u*8 + x].
 __device__ __forceinline__ void cj_idct8_f32(const int* in, const float* basis, float* o) {
 #pragma unroll

@@ -64,7 +64,7 @@ struct CJPixGeom {
 #define CJ_TMP_STRIDE 72
 
 struct alignas(16) CJPixSmemParams {
-  int16_t q[4][64];       // dequantisation tables, natural order
+  int32_t q[4][64];       // dequantisation tables, natural order (int32: no unpacking per row)
   uint16_t boff[64];      // per block of the tile: smem offset of its 8x8 destination
   uint8_t bc[64];         // per block of the tile: component
   uint8_t bq[64];         // per block of the tile: quantisation table
@@ -221,11 +221,12 @@ __device__ __forceinline__ bool cj_pixel_compute(uint8_t* __restrict__ out, CJSt
   // Row pass: one thread per (block, row); dequantise on load.
   for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
     const int k = t >> 3, r = t & 7;
-    const uint4 qv = *reinterpret_cast<const uint4*>(&P.q[P.bq[k]][r * 8]);
-    const int16_t* q = reinterpret_cast<const int16_t*>(&qv);
+    const int4* qp = reinterpret_cast<const int4*>(&P.q[P.bq[k]][r * 8]);
+    const int4 qa = qp[0], qb = qp[1];
+    const int q[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
     uint4 raw = *reinterpret_cast<const uint4*>(sc + k * 64 + r * 8);
     int v[8];
-    cj_unpack_dequant(raw, q, v);
+    cj_unpack_dequant32(raw, q, v);
     cj_idct_row(v);
     int4* o = reinterpret_cast<int4*>(tmp + k * CJ_TMP_STRIDE + r * 8);
     o[0] = make_int4(v[0], v[1], v[2], v[3]);
