@@ -87,6 +87,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the single-image and precision configurations in the default run")
     ap.add_argument("--split", action="store_true",
                     help="under torchrun: partition one batch across ranks (strong scaling) "
                          "instead of one batch per rank (weak scaling)")
@@ -360,6 +362,44 @@ def serving_value(wl, seconds: float) -> dict:
     return out
 
 
+def batch_tc_value(args, src, offsets, sizes, tune, wl, dist) -> dict:
+    """Device-resident MPix/s of the batch decoded with the tensor-core iDCT
+    (cjBatchSetOutput(RGB, CJ_IDCT_TC)) under the same tuning, and its pixel
+    kernel's time."""
+    import torch
+
+    import cudajpeg_b200 as cj
+    from cudajpeg_b200 import replicas as R
+    with cj.Batch() as b:
+        b.set_tuning(tune["sub_bits"], tune["decode_ctas_per_sm"], tune["pixel_tile_cap"])
+        b.set_output(cj.OUTPUT_RGB, cj.IDCT_TC)
+        b.stage(src.data_ptr(), offsets, sizes)
+        ext = torch.cuda.ExternalStream(b.stream())
+        for _ in range(args.warmup):
+            b.run()
+        if any(b.wait()):
+            raise RuntimeError("batch decode errors (tensor-core iDCT)")
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        pix = []
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            starts[k].record(ext)
+            b.run()
+            ends[k].record(ext)
+            b.wait()
+            pix.append(b.phase_ms()["pixel"])
+        torch.cuda.synchronize()
+        total = R.max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(starts, ends)), dist, "cuda")
+        job_pixels = R.sum_over_ranks(wl.pixels, dist, "cuda")
+    return {"value": round(job_pixels * args.steps / (total / 1e3) / 1e6, 2), "unit": "MPix/s",
+            "ms_per_step": round(total / args.steps, 4), "pixel_kernel_ms": round(statistics.mean(pix), 4),
+            "how": "k_pixel_batch with tcgen05 FP16 hi/lo iDCT (FP32 accumulation in tensor memory), "
+                   "same batch and tuning, CUDA events on the decoder's stream"}
+
+
 def run_batch(args, wl, world, rank, local, dist):
     import numpy as np
     import torch
@@ -465,15 +505,22 @@ def run_batch(args, wl, world, rank, local, dist):
     decode_ms = sum(pm[k] for k in cj.BATCH_PHASES[:9])
     pixel_ms = pm["pixel"]
     coef_bytes = st_run["blocks"] * 128
-    # k_decode_batch must read the compressed scans, write the destuffed
-    # copy, read it at least twice (speculative sync + write-out) and write
-    # the int16 coefficient blocks; k_pixel_batch reads the blocks and
-    # writes the interleaved output
-    alg_decode = st_run["input_bytes"] + 3 * st_run["scan_bytes"] + coef_bytes
-    alg_pixel = coef_bytes + st_run["output_bytes"]
-    ach_decode = alg_decode / (decode_ms / 1e3) / 1e9
+    # the path's algorithmic bytes are the compressed scans read
+    # plus the decoded pixels written; intermediates are not counted.  The
+    # dominant kernel is k_decode_batch, so the roofline is those bytes over
+    # its time; the same bytes over the whole step, and each kernel's own
+    # minimum with its intermediates (destuffed copy written and read twice,
+    # int16 blocks written / read), are reported beside it.
+    alg_path = st_run["input_bytes"] + st_run["output_bytes"]
+    min_decode = st_run["input_bytes"] + 3 * st_run["scan_bytes"] + coef_bytes
+    min_pixel = coef_bytes + st_run["output_bytes"]
+    ach_decode = alg_path / (decode_ms / 1e3) / 1e9
+    ach_step = alg_path / (mean_ms / 1e3) / 1e9
     tkey = traffic_key(args.workload, args.batch_size)
-    ach_pixel = alg_pixel / (pixel_ms / 1e3) / 1e9
+    ach_pixel = min_pixel / (pixel_ms / 1e3) / 1e9
+    tr_decode = read_traffic("k_decode_batch", tkey)
+    tr_pixel = read_traffic("k_pixel_batch", tkey)
+    tr_step = tr_decode + tr_pixel if tr_decode and tr_pixel else None
     line = {"metric": METRIC, "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean_ms, 4),
             "higher_is_better": True, "scaling": "strong" if args.split else "weak",
@@ -502,25 +549,44 @@ def run_batch(args, wl, world, rank, local, dist):
             "roofline": {"bound": "hbm", "kernel": "k_decode_batch", "achieved": round(ach_decode, 1),
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": round(ach_decode / peaks["hbm_gbs"], 4),
-                         "traffic": read_traffic("k_decode_batch", tkey),
-                         "algorithmic_bytes": int(alg_decode), "kernel_ms": round(decode_ms, 4),
+                         "traffic": tr_decode,
+                         "algorithmic_bytes": int(alg_path), "kernel_ms": round(decode_ms, 4),
+                         "kernel_min_bytes": int(min_decode),
+                         "bytes": "compressed scans read + decoded pixels written (per batch); "
+                                  "kernel_min_bytes adds the kernel's own intermediates",
                          "peak_source": peaks["source"]},
+            "roofline_step": {"bound": "hbm", "kernels": "k_decode_batch + k_pixel_batch",
+                              "achieved": round(ach_step, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                              "frac": round(ach_step / peaks["hbm_gbs"], 4), "algorithmic_bytes": int(alg_path),
+                              "traffic": tr_step,
+                              "traffic_over_algorithmic": (round(tr_step / alg_path, 3) if tr_step else None),
+                              "ms": round(mean_ms, 4)},
             "roofline_pixel": {"bound": "hbm", "kernel": "k_pixel_batch", "achieved": round(ach_pixel, 1),
                                "peak": peaks["hbm_gbs"], "unit": "GB/s",
                                "frac": round(ach_pixel / peaks["hbm_gbs"], 4),
-                               "traffic": read_traffic("k_pixel_batch", tkey),
-                               "algorithmic_bytes": int(alg_pixel), "kernel_ms": round(pixel_ms, 4),
+                               "traffic": tr_pixel,
+                               "kernel_min_bytes": int(min_pixel), "kernel_ms": round(pixel_ms, 4),
+                               "bytes": "int16 blocks read + decoded pixels written",
                                "peak_source": peaks["source"]},
             "phase_ms": pm, "gpu_launches": int(launches), "clocks": clocks.summary()}
+    # the same batch with the tensor-core iDCT in the pixel kernel (the
+    # metric's batched + TC-iDCT form; output within +-1 per sample of the
+    # integer iDCT's), timed the same way
+    tc = batch_tc_value(args, src, offsets, sizes, tune, wl, dist)
+    line["batched_tc"] = tc
     if rank == 0 and world == 1:
         line["plain_path"] = plain_path_value(cj, wl.files)
         line["plain_path"]["batched_over_plain"] = round(value / line["plain_path"]["value"], 2)
+        line["plain_path"]["batched_tc_over_plain"] = round(tc["value"] / line["plain_path"]["value"], 2)
         if args.serve_seconds > 0:
             line["serving"] = serving_value(wl, args.serve_seconds)
     return line
 
 
 def run_single(args, wl, world, rank, local, dist):
+    """The plain per-image path (openJPG / cjReaderRedecodeDevice) on one
+    image: device time per decode with L2 flushed before each, and the end
+    to end call (host parse, copies, kernels) per decode."""
     import numpy as np
     import torch
 
@@ -569,8 +635,8 @@ def run_single(args, wl, world, rank, local, dist):
     if reader.sync():
         raise RuntimeError("device decode reported an error")
     reader.set_profile(False)
-    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    total_ms = R.max_over_ranks(total_ms, dist, "cuda")
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = R.max_over_ranks(sum(step_ms), dist, "cuda")
     job_pixels = R.sum_over_ranks(wl.pixels, dist, "cuda")  # each rank decodes its own copy
     value = job_pixels * args.steps / (total_ms / 1e3) / 1e6
     e2e_ms = []
@@ -583,13 +649,14 @@ def run_single(args, wl, world, rank, local, dist):
         t0 = time.perf_counter()
         reader.open_bytes((src.data_ptr(), n))
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
-    e2e_total = sum(e2e_ms)
-    e2e_total = R.max_over_ranks(e2e_total, dist, "cuda")
+    e2e_total = R.max_over_ranks(sum(e2e_ms), dist, "cuda")
     e2e_value = job_pixels * args.steps / (e2e_total / 1e3) / 1e6
     means = {k: statistics.mean(v) for k, v in kern_ms.items()}
     dom = max(means, key=means.get)
     peaks = read_peaks()
-    alg = KERNEL_BYTES[dom](geom)
+    # SURVEY 8(d) bytes of the path (compressed scan read + pixels written)
+    # over the dominant kernel's time; the kernel's own minimum bytes beside
+    alg = geom["B"] + geom["P"]
     achieved = alg / (means[dom] / 1e3) / 1e9
     reader.close()
     return {"metric": METRIC, "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
@@ -600,18 +667,22 @@ def run_single(args, wl, world, rank, local, dist):
                            l2="flushed before each step (256 MiB write, outside the timing)",
                            compressed_MB_per_s=round(world * info["scan_bytes"] * args.steps
                                                      / (total_ms / 1e3) / 1e6, 1)),
+            "latency_ms": {"device_p50": round(float(np.percentile(step_ms, 50)), 4),
+                           "device_p99": round(float(np.percentile(step_ms, 99)), 4),
+                           "e2e_p50": round(float(np.percentile(e2e_ms, 50)), 4),
+                           "e2e_p99": round(float(np.percentile(e2e_ms, 99)), 4)},
             "e2e": {"value": round(e2e_value, 2), "unit": "MPix/s",
                     "h2d_bytes_per_step": info["scan_bytes"] + info["param_bytes"],
                     "d2h_bytes_per_step": wl.out_bytes + 32,
                     "ms_per_step": round(e2e_total / args.steps, 3),
-                    "lone_step_ms": round(min(e2e_lat), 3),
-                    "how": "two cjBatch decoders alternate: step k's D2H overlaps step k+1's host parse, "
-                           "H2D and kernels; every step's copies are inside the timed region"},
+                    "how": "openJPGMem per step from pinned host memory: host parse, H2D copy of the "
+                           "scan and tables, kernels, D2H copy of the image, all inside the timed region"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": round(achieved / peaks["hbm_gbs"], 4),
                          "traffic": read_traffic(dom, args.workload), "algorithmic_bytes": int(alg),
-                         "peak_source": peaks["source"]},
+                         "kernel_min_bytes": int(KERNEL_BYTES[dom](geom)),
+                         "kernel_ms": round(means[dom], 4), "peak_source": peaks["source"]},
             "kernel_ms": {k: round(v, 4) for k, v in means.items()},
             "gpu_launches": int(launches), "clocks": clocks.summary()}
 
@@ -626,26 +697,28 @@ def idct_basis_f64():
     return cu / 2 * np.cos((2 * x + 1) * u * np.pi / 16)
 
 
-def run_precision(args):
-    """Precision form: plane iDCT of 8192x8192 q95 images (4:4:4, 4:2:2,
+def precision_line(args, steps: int, warmup: int, size: int) -> dict:
+    """Precision form: plane iDCT of size x size q95 images (4:4:4, 4:2:2,
     grey; 50/50 uniform noise and gradient) in the three arithmetic forms of
     cjIDCTPlane -- the bit-exact fixed-point iDCT, FP32 on CUDA cores, FP16
     hi+lo basis on tensor cores with FP32 accumulation -- timed with CUDA
-    events, with the raw FP32 outputs (cjIDCTBlocksRaw) compared against a
-    float64 iDCT of the same dequantised coefficients."""
+    events (L2 flushed before each launch), with the raw FP32 outputs
+    (cjIDCTBlocksRaw) compared on the GPU against a float64 iDCT of the same
+    dequantised coefficients, and the pixels against the integer form."""
     import numpy as np
     import torch
 
     import cudajpeg_b200 as cj
     from cudajpeg_b200 import workloads as W
-    samples = [W.precision_8192(m, size=args.precision_size) for m in ("444", "422", "gray")]
-    torch.cuda.set_device(0)
+    samples = [W.precision_8192(m, size=size) for m in ("444", "422", "gray")]
     basis = torch.from_numpy(idct_basis_f64()).cuda()
     peaks = read_peaks()
     modes = {"int": cj.IDCT_INT, "f32": cj.IDCT_F32, "tc": cj.IDCT_TC}
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    ones = torch.ones(64, dtype=torch.int16, device="cuda")
     rows = []
     tot = {m: [0.0, 0] for m in modes}
+    worst = {"f32": 0.0, "tc": 0.0}
     for smp in samples:
         with cj.Reader(host_coefficients=True) as r:
             r.open_bytes(smp.data)
@@ -654,13 +727,13 @@ def run_precision(args):
                 g = r.plane_geometry(c)
                 nblk = coefs[c].shape[0]
                 planes, ms = {}, {}
+                stream = torch.cuda.current_stream()
                 for name, mode in modes.items():
                     out = torch.zeros((g["rows"], g["stride"]), dtype=torch.uint8, device="cuda")
-                    stream = torch.cuda.current_stream()
-                    for _ in range(args.warmup):
+                    for _ in range(warmup):
                         r.plane_launch(g, out.data_ptr(), mode, stream.cuda_stream)
                     ts = []
-                    for _ in range(args.steps):
+                    for _ in range(steps):
                         flush.zero_()  # coefficients (128 B/block) start outside L2
                         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                         s0.record(stream)
@@ -679,23 +752,24 @@ def run_precision(args):
                     match[name] = {"exact": round(float((d == 0).double().mean()), 6),
                                    "within_1": round(float((d <= 1).double().mean()), 6),
                                    "max_abs": int(d.max())}
-                # raw (pre-rounding) error against float64, in chunks
-                err = {}
+                # raw (pre-rounding) error against float64, in chunks on the GPU
                 deq = coefs[c]
                 if np.abs(deq).max() > 32767:
                     raise RuntimeError("dequantised coefficient outside int16")
-                ones = np.ones(64, np.int16)
+                dev = torch.from_numpy(deq.astype(np.int16)).cuda()
+                err = {}
                 for name in ("f32", "tc"):
                     mx, sm = 0.0, 0.0
                     for k0 in range(0, nblk, 1 << 18):
-                        blk = deq[k0:k0 + (1 << 18)]
-                        raw = torch.from_numpy(cj.idct_blocks_raw(blk.astype(np.int16), ones, modes[name])).cuda()
-                        x = torch.from_numpy(blk).cuda().double().view(-1, 8, 8)
-                        want = (basis.t() @ x @ basis).reshape(-1, 64)   # out[x][y] = sum_uv C[u,x] C[v,y] F[u,v]
+                        blk = dev[k0:k0 + (1 << 18)].contiguous()
+                        raw = cj.idct_blocks_raw_device(blk, ones, modes[name])
+                        x = blk.double().view(-1, 8, 8)
+                        want = (basis.t() @ x @ basis).reshape(-1, 64)   # out[y][x] = sum_vu C[v,y] C[u,x] F[v,u]
                         e = (raw.double() - want).abs()
                         mx = max(mx, float(e.max()))
                         sm += float(e.sum())
                     err[name] = {"max_abs_vs_f64": round(mx, 6), "mean_abs_vs_f64": round(sm / (nblk * 64), 8)}
+                    worst[name] = max(worst[name], mx)
                 mpix = {k: round(nblk * 64 / (v / 1e3) / 1e6, 1) for k, v in ms.items()}
                 gbs = {k: round(nblk * 192 / (v / 1e3) / 1e9, 1) for k, v in ms.items()}
                 rows.append({"image": f"{smp.mode}_{smp.width}x{smp.height}_q{smp.quality}", "component": c,
@@ -703,23 +777,52 @@ def run_precision(args):
                              "MPix_per_s": mpix, "GB_per_s": gbs, "match_vs_int": match, "raw_error": err})
     tc_mpix = tot["tc"][1] / (tot["tc"][0] / 1e3) / 1e6
     tc_gbs = tot["tc"][1] * 3 / (tot["tc"][0] / 1e3) / 1e9   # 2 B coefficient in + 1 B sample out per pixel
-    worst_tc = max(r_["raw_error"]["tc"]["max_abs_vs_f64"] for r_ in rows)
-    line = {"metric": "plane iDCT MPix/s (tensor-core FP16 hi/lo, FP32 accumulate)", "value": round(tc_mpix, 1),
-            "unit": "MPix/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+    exact = {k: round(min(r_["match_vs_int"][k]["exact"] for r_ in rows), 6) for k in ("f32", "tc")}
+    within = {k: round(min(r_["match_vs_int"][k]["within_1"] for r_ in rows), 6) for k in ("f32", "tc")}
+    return {"metric": "plane iDCT MPix/s (tensor-core FP16 hi/lo, FP32 accumulate)", "value": round(tc_mpix, 1),
+            "unit": "MPix/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
             "ms_per_step": round(tot["tc"][0] / max(1, len(rows)), 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp16 hi/lo in, fp32 accumulate",
             "data": "synthetic",
-            "config": {"workload": f"precision_{args.precision_size}", "images": "444, 422, grey at q95",
+            "config": {"workload": f"precision_{size}", "images": "444, 422, grey at q95",
                        "content": "50/50 uniform noise and gradient (cudajpeg_b200/workloads.py)",
                        "l2": "L2 flushed (256 MB write) before every timed launch"},
             "per_mode_MPix_per_s": {k: round(v[1] / (v[0] / 1e3) / 1e6, 1) for k, v in tot.items()},
-            "tc_max_abs_error_vs_f64": worst_tc, "tc_error_below_0_5": worst_tc < 0.5,
+            "max_abs_error_vs_f64": {k: round(v, 6) for k, v in worst.items()},
+            "error_below_0_5": {k: v < 0.5 for k, v in worst.items()},
+            "min_exact_fraction_vs_int": exact, "min_within_1_fraction_vs_int": within,
             "roofline": {"bound": "hbm", "kernel": "k_idct_tc", "achieved": round(tc_gbs, 1),
                          "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(tc_gbs / peaks["hbm_gbs"], 4),
-                         "traffic": read_traffic("k_idct_tc", f"precision_{args.precision_size}"),
+                         "traffic": read_traffic("k_idct_tc", f"precision_{size}"),
                          "peak_source": peaks["source"]},
             "rows": rows}
-    print(json.dumps(line), flush=True)
+
+
+def run_precision(args):
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(precision_line(args, args.steps, args.warmup, args.precision_size)), flush=True)
+
+
+def other_configs(args) -> dict:
+    """The other benchmark configurations, measured in the default run at
+    fewer steps: the plain per-image path on the 1024x768 and 4096x4096
+    single images (MPix/s and p50/p99 latency), and the precision A/B of the
+    plane iDCT forms on the 8192x8192 images."""
+    out = {}
+    for name in ("single_1024", "single_4096"):
+        a = argparse.Namespace(**vars(args))
+        a.steps, a.warmup, a.workload = 20, 3, name
+        wl = Workload(name, 1)
+        line = run_single(a, wl, 1, 0, 0, None)
+        out[name] = {k: line[k] for k in ("value", "unit", "ms_per_step", "latency_ms", "e2e", "roofline",
+                                          "kernel_ms", "gpu_launches", "clocks")}
+        out[name]["config"] = line["config"]
+    p = precision_line(args, 5, 3, args.precision_size)
+    out[f"precision_{args.precision_size}"] = {k: p[k] for k in (
+        "value", "unit", "per_mode_MPix_per_s", "max_abs_error_vs_f64", "error_below_0_5",
+        "min_exact_fraction_vs_int", "min_within_1_fraction_vs_int", "roofline", "config")}
+    return out
 
 
 def run_gpu(args):
@@ -741,6 +844,8 @@ def run_gpu(args):
         line = run_batch(args, wl, world, rank, local, dist)
     else:
         line = run_single(args, wl, world, rank, local, dist)
+    if rank == 0 and world == 1 and args.workload == "mixed_batch" and not args.no_other_configs:
+        line["other_configs"] = other_configs(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl, os.cpu_count() or 1, args.cpu_seconds)
     if dist:

@@ -35,6 +35,7 @@ ERROR_NAMES = {0: "NO_ERROR", 1: "SYNTAX_ERROR", 2: "UNSUPPORTED_ERROR", 3: "OOM
 
 READER_HOST_COEFFICIENTS = 1
 IDCT_INT, IDCT_F32, IDCT_TC = 0, 1, 2
+OUTPUT_RGB, OUTPUT_PLANAR, OUTPUT_NV12 = 0, 1, 2
 
 # Every symbol the C headers in include/ declare (checked by the CPU tests).
 EXPORTED = [
@@ -52,6 +53,8 @@ EXPORTED = [
     "cjServerCreate", "cjServerDestroy", "cjServerSubmit", "cjServerWait", "cjServerCopyOut",
     "cjServerRelease", "cjServerStats", "cjServerReplay", "cjServerSetTuning",
     "cjBatchSetTuning", "cjBatchGetTuning", "cjBatchAutotune", "cjDebugStepTable",
+    "cjBatchCopyCoefficients", "cjBuildInfo", "cjBatchSetWaitLimit", "cjBatchSetOutput",
+    "cjBatchGetOutput", "cjBatchChromaGeometry",
 ]
 
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
@@ -107,6 +110,7 @@ def load(build_if_missing: bool = True):
     lib.cjIDCTBlocksRaw.argtypes = [vp, C.c_longlong, vp, vp, C.c_int, vp]
     lib.cjDebugHuffDecode.argtypes = [vp, vp, C.c_uint]
     lib.cjDebugStepTable.argtypes = [vp, vp, C.c_int, vp]
+    lib.cjBuildInfo.argtypes = [C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]
     lib.cjReaderRedecodeDevice.argtypes = [vp]
     lib.cjReaderSync.argtypes = [vp]
     lib.cjReaderDevicePixels.restype = vp
@@ -130,6 +134,8 @@ def load(build_if_missing: bool = True):
     lib.cjBatchDeviceImage.argtypes = [vp, C.c_int]
     lib.cjBatchStream.restype = vp
     lib.cjBatchStream.argtypes = [vp]
+    lib.cjBatchCopyCoefficients.restype = C.c_longlong
+    lib.cjBatchCopyCoefficients.argtypes = [vp, C.c_int, vp, C.c_longlong]
     lib.cjBatchStats.argtypes = [vp, i64p]
     lib.cjBatchKernelMs.restype = C.c_float
     lib.cjBatchKernelMs.argtypes = [vp]
@@ -138,6 +144,10 @@ def load(build_if_missing: bool = True):
     lib.cjDecodeNoAlloc.argtypes = [vp, C.c_size_t, vp, C.c_size_t, ip, ip, ip, vp]
     lib.cjBatchImageGeometry.argtypes = [vp, C.c_int, ip, ip, ip]
     lib.cjBatchSetTuning.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+    lib.cjBatchSetWaitLimit.argtypes = [vp, C.c_uint]
+    lib.cjBatchSetOutput.argtypes = [vp, C.c_int, C.c_int]
+    lib.cjBatchGetOutput.argtypes = [vp, ip, ip]
+    lib.cjBatchChromaGeometry.argtypes = [vp, C.c_int, ip, ip]
     lib.cjBatchGetTuning.argtypes = [vp, ip, ip, ip]
     lib.cjBatchAutotune.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, C.POINTER(C.c_float),
                                     C.POINTER(C.c_float), C.c_int]
@@ -386,15 +396,27 @@ class Batch:
             raise DecodeError(err, "cjBatchWait")
         return [int(e) for e in errs[: self.n]]
 
+    def set_output(self, fmt: int = OUTPUT_RGB, idct: int = IDCT_INT):
+        """Output format and pixel-stage iDCT of batches staged from now on."""
+        if self.lib.cjBatchSetOutput(self.ptr, fmt, idct):
+            raise ValueError(f"bad output {(fmt, idct)}")
+        self.fmt = fmt
+
     def image(self, i: int, copy: bool = True):
+        """Image i after a fetch: RGB [H, W, 3] / grey [H, W]; in the planar
+        format a tuple (Y, Cb, Cr) of 2-D planes, in NV12 (Y, CbCr [ch, cw, 2])."""
         w, h, c = C.c_int(0), C.c_int(0), C.c_int(0)
         p = self.lib.cjBatchImage(self.ptr, i, C.byref(w), C.byref(h), C.byref(c))
         if not p:
             return None
-        n = w.value * h.value * c.value
-        arr = np.frombuffer((C.c_uint8 * n).from_address(p), np.uint8)
-        arr = arr.reshape((h.value, w.value, 3) if c.value == 3 else (h.value, w.value))
-        return arr.copy() if copy else arr
+        return _image_view(p, w.value, h.value, c.value, getattr(self, "fmt", OUTPUT_RGB),
+                           self._chroma_size(i), copy)
+
+    def _chroma_size(self, i: int):
+        """(cw, ch) of image i: the reference's channel sizes."""
+        cw, ch = C.c_int(0), C.c_int(0)
+        self.lib.cjBatchChromaGeometry(self.ptr, i, C.byref(cw), C.byref(ch))
+        return cw.value, ch.value
 
     def decode(self, files) -> tuple:
         """Decode a list of JPEG byte strings -> (list of arrays or None, errors)."""
@@ -405,6 +427,15 @@ class Batch:
         self.fetch()
         errs = self.wait()
         return [self.image(i) if not e else None for i, e in enumerate(errs)], errs
+
+    def coefficients(self, i: int, nblocks: int) -> np.ndarray:
+        """Image i's quantised int16 blocks [n, 64] (natural order, MCU scan
+        order, components interleaved) from the last run."""
+        out = np.empty((nblocks, 64), np.int16)
+        n = self.lib.cjBatchCopyCoefficients(self.ptr, i, out.ctypes.data, nblocks)
+        if n < 0:
+            raise DecodeError(int(n), "cjBatchCopyCoefficients")
+        return out[:n]
 
     def stats(self) -> dict:
         a = (C.c_int64 * 16)()
@@ -426,6 +457,18 @@ class Batch:
         err = self.lib.cjBatchSetTuning(self.ptr, sub_bits, decode_ctas_per_sm, pixel_tile_cap)
         if err:
             raise ValueError(f"bad tuning {(sub_bits, decode_ctas_per_sm, pixel_tile_cap)}")
+
+    def set_wait_limit(self, polls: int):
+        """Bound each grid-barrier wait of the decode kernel (0 = default)."""
+        if self.lib.cjBatchSetWaitLimit(self.ptr, polls):
+            raise ValueError("cjBatchSetWaitLimit")
+
+    def wait_status(self) -> tuple:
+        """(batch-level code, per-image codes) of the queued work, without
+        raising: cjBatchWait's return value and its errors[]."""
+        errs = np.zeros(max(self.n, 1), np.int32)
+        err = self.lib.cjBatchWait(self.ptr, errs.ctypes.data)
+        return int(err), [int(e) for e in errs[: self.n]]
 
     def tuning(self) -> dict:
         a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
@@ -507,6 +550,47 @@ def idct_blocks_raw(coef_q: np.ndarray, q_nat: np.ndarray, mode: int) -> np.ndar
         raise DecodeError(err, "cjIDCTBlocksRaw")
     torch.cuda.synchronize()
     return out.cpu().numpy()
+
+
+def _image_view(p: int, w: int, h: int, c: int, fmt: int, chroma, copy: bool):
+    if c != 3 or fmt == OUTPUT_RGB:
+        n = w * h * c
+        arr = np.frombuffer((C.c_uint8 * n).from_address(p), np.uint8)
+        arr = arr.reshape((h, w, 3) if c == 3 else (h, w))
+        return arr.copy() if copy else arr
+    cw, ch = chroma
+    n = w * h + 2 * cw * ch
+    flat = np.frombuffer((C.c_uint8 * n).from_address(p), np.uint8)
+    flat = flat.copy() if copy else flat
+    y = flat[: w * h].reshape(h, w)
+    if fmt == OUTPUT_NV12:
+        return y, flat[w * h:].reshape(ch, cw, 2)
+    return y, flat[w * h: w * h + cw * ch].reshape(ch, cw), flat[w * h + cw * ch:].reshape(ch, cw)
+
+
+def build_info() -> dict:
+    """cjBuildInfo: compute capabilities compiled into the library and the
+    binary version of the device code the current GPU runs (0 without one)."""
+    lib = load()
+    archs = (C.c_int * 8)()
+    ver = C.c_int(0)
+    n = lib.cjBuildInfo(archs, 8, C.byref(ver))
+    return {"archs": [int(archs[k]) for k in range(min(n, 8))], "binary_version": ver.value}
+
+
+def idct_blocks_raw_device(coef_q, q_nat, mode: int):
+    """cjIDCTBlocksRaw on device tensors: int16 blocks [n, 64] and the int16
+    natural-order table [64] (both on the GPU) -> float32 [n, 64] on the GPU,
+    queued on torch's current stream."""
+    import torch
+    lib = load()
+    out = torch.empty((coef_q.shape[0], 64), dtype=torch.float32, device=coef_q.device)
+    err = lib.cjIDCTBlocksRaw(C.c_void_p(coef_q.data_ptr()), coef_q.shape[0], C.c_void_p(q_nat.data_ptr()),
+                              C.c_void_p(out.data_ptr()), mode,
+                              C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    if err:
+        raise DecodeError(err, "cjIDCTBlocksRaw")
+    return out
 
 
 def decode(data, sub_bits: int = 0) -> np.ndarray:

@@ -128,3 +128,26 @@ int cjDebugStepTable(const unsigned char counts[16], const unsigned char* symbol
 }
 
 }  // extern "C"
+
+// Never launched: its attributes tell which device code the library holds.
+__global__ void k_build_probe() {}
+
+extern "C" int cjBuildInfo(int* archs, int max_archs, int* binary_version) {
+#ifdef __CUDA_ARCH_LIST__
+  static const int list[] = {__CUDA_ARCH_LIST__};
+#else
+  static const int list[] = {0};
+#endif
+  const int n = (int)(sizeof(list) / sizeof(list[0]));
+  for (int k = 0; k < n && k < max_archs; k++) archs[k] = list[k];
+  if (binary_version) {
+    *binary_version = 0;
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) == cudaSuccess && devices > 0) {
+      cudaFuncAttributes fa;
+      if (cudaFuncGetAttributes(&fa, k_build_probe) == cudaSuccess) *binary_version = fa.binaryVersion;
+    }
+    cudaGetLastError();
+  }
+  return n;
+}

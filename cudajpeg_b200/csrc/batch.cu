@@ -27,6 +27,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -47,6 +49,10 @@
 #define BT_WARPS (BT_THREADS / 32)
 #define BT_TILE_BYTES 4096  // destuff tile: 256 threads x 16 bytes
 #define BT_TILE_BAD (1 << 30)  // flag in a tile's marker count: malformed FF sequence
+// fixed shared-memory offsets of the tensor-core form's A tile and basis
+// (cj_pix_layout with two coefficient buffers)
+#define BT_TC_A_OFF 16384
+#define BT_TC_B_OFF 32768
 
 // ---------------------------------------------------------------- layouts
 
@@ -126,6 +132,7 @@ struct CJBatchArgs {
   uint8_t* out;
   CJBatchCtl* ctl;
   int n, ntiles, nwarps, nptiles, max_passes;
+  unsigned wait_limit;  // grid-barrier polls before a timeout (0 = default)
 };
 
 // ---------------------------------------------------------------- device helpers
@@ -138,13 +145,16 @@ __device__ __forceinline__ void bt_raise_dec(CJStatus* st, int64_t block, int co
 }
 
 // Grid barrier for a cooperative launch (all CTAs co-resident).  The wait is
-// bounded: on timeout the batch is flagged and the CTA carries on, so the
-// kernel always terminates.
-__device__ __forceinline__ void bt_grid_sync(CJBatchCtl* ctl, unsigned& gen) {
+// bounded by `limit` polls (0: 2^24, about 2 s): a CTA whose wait runs out
+// flags the batch (ctl->timeout, read by the host) and returns false, and the
+// caller leaves the kernel at once, so no CTA ever runs a phase whose inputs
+// the barrier did not complete.  The CTAs still waiting time out in turn.
+__device__ __forceinline__ bool bt_grid_sync(CJBatchCtl* ctl, unsigned& gen, unsigned limit, int* s_ok) {
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned g = gen;
+    int ok = 1;
     if (atomicAdd(&ctl->bar_count, 1) == gridDim.x - 1) {
       atomicExch(&ctl->bar_count, 0);
       __threadfence();
@@ -157,12 +167,14 @@ __device__ __forceinline__ void bt_grid_sync(CJBatchCtl* ctl, unsigned& gen) {
       // either: each would invalidate the SM's L1 under the warps of other
       // CTAs still working there.  The fence after the loop orders what
       // follows (the releasing CTA fenced before its increment).
+      const unsigned lim = limit ? limit : (1u << 24);
       unsigned it = 0, v;
       for (;;) {
         asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(&ctl->bar_gen) : "memory");
         if (v != g) break;
-        if (++it > (1u << 24)) {
+        if (++it >= lim) {
           atomicExch(&ctl->timeout, 1);
+          ok = 0;
           break;
         }
         __nanosleep(128);
@@ -170,8 +182,10 @@ __device__ __forceinline__ void bt_grid_sync(CJBatchCtl* ctl, unsigned& gen) {
     }
     __threadfence();
     gen = g + 1;
+    *s_ok = ok;
   }
   __syncthreads();
+  return *s_ok != 0;
 }
 
 // L2-coherent loads of records another SM may have rewritten in this kernel.
@@ -377,7 +391,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ int2 sm2[33];
   __shared__ uint8_t s_zz[64];
-  __shared__ int s_grp;
+  __shared__ int s_grp, s_ok;
   unsigned gen = 0;
   if (threadIdx.x == 0) gen = atomicAdd(&a.ctl->bar_gen, 0);
   if (threadIdx.x < 64) s_zz[threadIdx.x] = c_bt_zz[threadIdx.x];
@@ -426,7 +440,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       a.tile_mark[t] = tot.y | (bad ? BT_TILE_BAD : 0);  // counts stay below 2^13
     }
   }
-  bt_grid_sync(a.ctl, gen);
+  if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
 
   bt_stamp(a.ctl, 2);
   // ---- phase 2: per-image tile offsets
@@ -455,7 +469,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       a.st[i].nmarkers = run.y;
     }
   }
-  bt_grid_sync(a.ctl, gen);
+  if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
 
   bt_stamp(a.ctl, 3);
   // ---- phase 3: destuff scatter, over the same tile runs.  A tile's kept
@@ -506,7 +520,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
     }
     __syncthreads();
   }
-  bt_grid_sync(a.ctl, gen);
+  if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
 
   bt_stamp(a.ctl, 4);
   // ---- phase 4: segments and subsequences, one CTA per image
@@ -573,7 +587,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       st->nsub = running;
     }
   }
-  bt_grid_sync(a.ctl, gen);
+  if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
 
   bt_stamp(a.ctl, 5);
   // ---- phase 5: speculative decode + warp settle, in groups of BT_WARPS
@@ -610,7 +624,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
     a.ctl->unstable[0] = 0;
     a.ctl->unstable[1] = 0;
   }
-  bt_grid_sync(a.ctl, gen);
+  if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
 
   bt_stamp(a.ctl, 6);
   // ---- phase 6: fix-up passes until no warp's last exit moves
@@ -692,7 +706,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
         a.wagg[w] = g;
       }
     }
-    bt_grid_sync(a.ctl, gen);
+    if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
     // the barrier orders every increment before this read; a load, not an
     // atomic (one per thread of the grid would serialise at the word's slice)
     if (__ldcg(unstable) == 0) break;
@@ -735,7 +749,7 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       run = cj_op(run, CJAgg5{g.has_head, g.nblocks, g.dc[0], g.dc[1], g.dc[2]});
     }
   }
-  bt_grid_sync(a.ctl, gen);
+  if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
 
   bt_stamp(a.ctl, 8);
   // ---- phase 8: coefficient write-out in units of a quarter subsequence.
@@ -838,58 +852,96 @@ static cudaError_t bt_decode_attrs() {
   return e;
 }
 
+template <int MODE, int OUT>
 __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int t1, uint8_t* smem,
-                                               uint64_t* bar2, CJPixSmemParams* Pp);
+                                               uint64_t* bar2, CJPixSmemParams* Pp, CJTcState* tc);
 
 // Phase 9 runs as its own kernel, launched right after k_decode_batch on the
 // same stream: the pixel work needs no grid barrier, and on its own it runs
 // at the occupancy of its 32-40 registers per thread instead of the entropy
 // phases' 64.  Pixel tiles, double-buffered: the TMA copy of a CTA's next
-// tile is in flight while it computes the current one.
-__global__ void __launch_bounds__(CJ_PIX_THREADS, 6) k_pixel_batch(CJBatchArgs a) {
+// tile is in flight while it computes the current one.  MODE is the iDCT
+// arithmetic (integer: the reference's, bit-exact; tensor cores: FP16 hi/lo
+// with FP32 accumulation), OUT the output format.  The tensor-core form
+// keeps a 64-column accumulator in tensor memory per CTA and the hi/lo
+// Kronecker basis, built by the CTA, in shared memory.
+template <int MODE, int OUT>
+__global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? 4 : 6) k_pixel_batch(CJBatchArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ uint64_t bar2[2];
   __shared__ CJPixSmemParams P;
+  // a decode kernel whose grid barrier timed out left no settled
+  // coefficients: nothing to transform
+  if (__ldcg(&a.ctl->timeout)) return;
+  __shared__ uint64_t s_mma_bar;
+  __shared__ uint32_t s_tmem;
+  __shared__ double s_b64[64];
+  __shared__ float s_b32[64];
   if (threadIdx.x == 0) {
     cj_mbar_init(&bar2[0], 1);
     cj_mbar_init(&bar2[1], 1);
+    if (MODE == CJ_PIX_IDCT_TC) cj_mbar_init(&s_mma_bar, 1);
+  }
+  CJTcState tc;
+  if (MODE == CJ_PIX_IDCT_TC) {
+    // the A tile starts zeroed (rows past a tile's blocks are never written)
+    for (int k = threadIdx.x; k < 16384 / 16; k += blockDim.x)
+      reinterpret_cast<uint4*>(smem + BT_TC_A_OFF)[k] = make_uint4(0, 0, 0, 0);
+    tc_build_basis(reinterpret_cast<uint16_t*>(smem + BT_TC_B_OFF), s_b64, s_b32);
+    if ((threadIdx.x >> 5) == 0) tc_alloc(&s_tmem, 64);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   }
   bt_stamp(a.ctl, 9);
   __syncthreads();
+  if (MODE == CJ_PIX_IDCT_TC) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    tc.tmem = s_tmem;
+    tc.bar = &s_mma_bar;
+    tc.parity = 0;
+    tc.basis = s_b32;
+  }
   // Each CTA takes a contiguous run of tiles, so consecutive tiles mostly
   // belong to one image: the image index only ever moves forward and the
   // tile geometry is rebuilt only when it changes.
   const int per = (a.nptiles + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(t0 + per, a.nptiles);
-  if (t0 < t1) bt_pixel_tiles(a, t0, t1, smem, bar2, &P);
+  if (t0 < t1) bt_pixel_tiles<MODE, OUT>(a, t0, t1, smem, bar2, &P, &tc);
   __syncthreads();
+  if (MODE == CJ_PIX_IDCT_TC && (threadIdx.x >> 5) == 0) tc_dealloc(s_tmem, 64);
   if (threadIdx.x == 0 && atomicAdd(&a.ctl->pix_done, 1) == gridDim.x - 1) bt_stamp_any(a.ctl, BT_NPHASE);
 }
 
+// Geometry of image i's pixel tiles.
+__device__ __forceinline__ CJPixGeom bt_pix_geom(const CJBatchArgs& a, int i, bool tc) {
+  const CJScanParams& prm = a.prm[i];
+  CJPixGeom gg;
+  gg.nch = prm.nch;
+  gg.bpm = prm.bpm;
+  gg.mcux = prm.mcux;
+  gg.mcuy = prm.mcuy;
+  gg.width = prm.width;
+  gg.height = prm.height;
+  gg.hmax = prm.hmax;
+  gg.vmax = prm.vmax;
+  gg.xs = prm.xshift;
+  gg.ys = prm.yshift;
+  gg.T = a.desc[i].T;
+  gg.cw = prm.nch == 3 ? (prm.width * prm.comp_sx[1] + prm.hmax - 1) / prm.hmax : 0;
+  gg.ch = prm.nch == 3 ? (prm.height * prm.comp_sy[1] + prm.vmax - 1) / prm.vmax : 0;
+  cj_pix_layout(&gg, prm.comp_sx[1], prm.comp_sy[1], 2, tc);
+  return gg;
+}
+
 // Tiles [t0, t1) of one pixel-kernel CTA.
+template <int MODE, int OUT>
 __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int t1, uint8_t* smem,
-                                               uint64_t* bar2, CJPixSmemParams* Pp) {
+                                               uint64_t* bar2, CJPixSmemParams* Pp, CJTcState* tc) {
+  constexpr bool TC = MODE == CJ_PIX_IDCT_TC;
   CJPixSmemParams& P = *Pp;
   auto advance = [&](int tt, int i) {
     while (tt >= a.desc[i].ptile0 + a.desc[i].nptiles) i++;
     return i;
-  };
-  auto geom_of = [&](int i) {
-    const CJScanParams& prm = a.prm[i];
-    CJPixGeom gg;
-    gg.nch = prm.nch;
-    gg.bpm = prm.bpm;
-    gg.mcux = prm.mcux;
-    gg.mcuy = prm.mcuy;
-    gg.width = prm.width;
-    gg.height = prm.height;
-    gg.hmax = prm.hmax;
-    gg.vmax = prm.vmax;
-    gg.xs = prm.xshift;
-    gg.ys = prm.yshift;
-    gg.T = a.desc[i].T;
-    cj_pix_layout(&gg, prm.comp_sx[1], prm.comp_sy[1], 2);
-    return gg;
   };
   // thread 0 issues each tile's copy one tile ahead of the compute; it keeps
   // the geometry of the image it prefetches from
@@ -899,7 +951,7 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
   CJPixGeom& pg = s_pg;
   auto issue = [&](int tt, int i, int which) {
     if (i != s_pimg) {
-      pg = geom_of(i);
+      pg = bt_pix_geom(a, i, TC);
       s_pimg = i;
     }
     const int local = tt - a.desc[i].ptile0, gx = (pg.mcux + pg.T - 1) / pg.T;
@@ -909,7 +961,7 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
   int img = bt_find(a.n, t0, [&](int k) { return a.desc[k].ptile0; });
   if (threadIdx.x == 0) issue(t0, img, 0);
   int nimg = img;  // image of the next tile to prefetch (thread 0)
-  CJPixGeom g = geom_of(img);
+  CJPixGeom g = bt_pix_geom(a, img, TC);
   int gimg = img;
   cj_pixel_setup(a.prm[img], g, &P);
   // tile position in its image's grid, advanced tile by tile
@@ -924,7 +976,7 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
     }
     img = advance(t, img);
     if (img != gimg) {  // CTA-uniform; the previous tile ended with a barrier
-      g = geom_of(img);
+      g = bt_pix_geom(a, img, TC);
       gimg = img;
       cj_pixel_setup(a.prm[img], g, &P);
       gx = (g.mcux + g.T - 1) / g.T;
@@ -932,8 +984,8 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
     }
     const CJImageDesc& d = a.desc[img];
     const int16_t* sc = reinterpret_cast<const int16_t*>(smem + buf * g.sc1_off);
-    if (!cj_pixel_compute(a.out + d.out_off, &a.st[img], g, trow, tcol * g.T, sc, smem, &bar2[buf],
-                          (par >> buf) & 1u, &P)) {
+    if (!cj_pixel_tile<MODE, OUT>(a.out + d.out_off, &a.st[img], g, trow, tcol * g.T, sc, smem, &bar2[buf],
+                                  (par >> buf) & 1u, &P, tc)) {
       if (t + 1 < t1) cj_mbar_wait(&bar2[buf ^ 1], (par >> (buf ^ 1)) & 1u);  // the prefetch in flight
       break;
     }
@@ -944,6 +996,41 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
     par ^= 1u << buf;
     buf ^= 1;
   }
+}
+
+typedef void (*bt_pixel_fn)(CJBatchArgs);
+static bt_pixel_fn bt_pixel_kernel(int mode, int out) {
+  if (mode == CJ_PIX_IDCT_TC) {
+    if (out == CJ_OUT_PLANAR) return k_pixel_batch<CJ_PIX_IDCT_TC, CJ_OUT_PLANAR>;
+    if (out == CJ_OUT_NV12) return k_pixel_batch<CJ_PIX_IDCT_TC, CJ_OUT_NV12>;
+    return k_pixel_batch<CJ_PIX_IDCT_TC, CJ_OUT_RGB>;
+  }
+  if (out == CJ_OUT_PLANAR) return k_pixel_batch<CJ_PIX_IDCT_INT, CJ_OUT_PLANAR>;
+  if (out == CJ_OUT_NV12) return k_pixel_batch<CJ_PIX_IDCT_INT, CJ_OUT_NV12>;
+  return k_pixel_batch<CJ_PIX_IDCT_INT, CJ_OUT_RGB>;
+}
+
+// Every pixel-kernel variant may use up to 96 KiB of dynamic shared memory.
+static cudaError_t bt_pixel_attrs() {
+  const int modes[] = {CJ_PIX_IDCT_INT, CJ_PIX_IDCT_TC};
+  const int outs[] = {CJ_OUT_RGB, CJ_OUT_PLANAR, CJ_OUT_NV12};
+  for (int m : modes)
+    for (int o : outs) {
+      cudaError_t e = cudaFuncSetAttribute((const void*)bt_pixel_kernel(m, o),
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+      if (e != cudaSuccess) return e;
+    }
+  return cudaSuccess;
+}
+
+// Output bytes of one image in a format.
+static int64_t bt_out_bytes(const CJImageHeader& h, int out) {
+  const int64_t y = (int64_t)h.width * h.height;
+  if (h.nch != 3) return y;
+  if (out == CJ_OUT_RGB) return 3 * y;
+  const int64_t cw = ((int64_t)h.width * h.comp_sx[1] + h.hmax - 1) / h.hmax;
+  const int64_t ch = ((int64_t)h.height * h.comp_sy[1] + h.vmax - 1) / h.vmax;
+  return y + 2 * cw * ch;
 }
 
 // ---------------------------------------------------------------- host side
@@ -957,6 +1044,9 @@ struct CJBatch {
   int sub_bits = BT_SUB_BITS_DEFAULT;
   int decode_ctas = BT_DECODE_CTAS_DEFAULT;  // decode-kernel CTAs per SM (3, 4 or 5)
   int tile_cap = 0;                          // max MCUs per pixel tile (0 = layout maximum)
+  unsigned wait_limit = 0;                   // grid-barrier polls before a timeout (0 = default)
+  int idct = CJ_PIX_IDCT_INT;                // pixel-stage iDCT arithmetic
+  int out_format = CJ_OUT_RGB;               // output format
   JPGReader* parser = nullptr;  // host marker parse, one image at a time
   // device buffers (grow-only)
   CJDevBuf hdr, desc, prm, st, blob, data, tile_keep, tile_mark, mpos, mcode, segs, recs, ckpt, snap,
@@ -967,7 +1057,7 @@ struct CJBatch {
   int n_in = 0, n_dev = 0;
   std::vector<int> dev_of;     // device slot of each submitted image, -1 if rejected
   std::vector<int> host_err;   // host-side (parse) error of each submitted image
-  std::vector<int> dims;       // width, height, channels per device slot
+  std::vector<int> dims;       // width, height, channels, chroma width, chroma height per device slot
   std::vector<int64_t> outoff; // output offset per device slot
   int ntiles = 0, nwarps = 0, nptiles = 0;
   int64_t blob_bytes = 0, out_total = 0, blocks = 0, scan_bytes = 0;
@@ -1018,8 +1108,7 @@ static int bt_init(CJBatch* b) {
   CJ_CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaEventCreate(&b->ev0), CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaEventCreate(&b->ev1), CUDA_MEM_ERROR);
-  CJ_CUDA_TRY(cudaFuncSetAttribute(k_pixel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
-              CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(bt_pixel_attrs(), CUDA_MEM_ERROR);
   CJ_CUDA_TRY(bt_decode_attrs(), CUDA_MEM_ERROR);
   b->parser = newJPGReader();
   if (!b->parser) return OOM_ERROR;
@@ -1121,6 +1210,27 @@ int cjBatchSetTuning(CJBatch* b, int sub_bits, int decode_ctas_per_sm, int pixel
   return 0;
 }
 
+int cjBatchSetOutput(CJBatch* b, int format, int idct) {
+  if (!b) return PROGRAMMER_ERROR;
+  if (format != CJ_OUT_RGB && format != CJ_OUT_PLANAR && format != CJ_OUT_NV12) return PROGRAMMER_ERROR;
+  if (idct != CJ_PIX_IDCT_INT && idct != CJ_PIX_IDCT_TC) return PROGRAMMER_ERROR;
+  b->out_format = format;
+  b->idct = idct;
+  return 0;
+}
+
+void cjBatchGetOutput(const CJBatch* b, int* format, int* idct) {
+  if (format) *format = b->out_format;
+  if (idct) *idct = b->idct;
+}
+
+int cjBatchSetWaitLimit(CJBatch* b, unsigned polls) {
+  if (!b) return PROGRAMMER_ERROR;
+  b->wait_limit = polls;
+  b->graph_stale = true;  // the limit is a kernel argument baked into the graph
+  return 0;
+}
+
 void cjBatchGetTuning(const CJBatch* b, int* sub_bits, int* decode_ctas_per_sm, int* pixel_tile_cap) {
   if (sub_bits) *sub_bits = b->sub_bits;
   if (decode_ctas_per_sm) *decode_ctas_per_sm = b->decode_ctas;
@@ -1189,18 +1299,20 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
     blocks += h.total_blocks;
     d.out_off = out_total;
     int ch = h.nch == 3 ? 3 : 1;
-    out_total += ((int64_t)h.width * h.height * ch + 15) & ~(int64_t)15;  // 16-byte aligned starts
+    out_total += (bt_out_bytes(h, b->out_format) + 15) & ~(int64_t)15;  // 16-byte aligned starts
     CJPixGeom g;
     g.nch = h.nch;
     g.bpm = bpm;
     g.hmax = h.hmax;
     g.vmax = h.vmax;
     g.T = d.T;
-    smem = std::max(smem, cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1], 2));
+    smem = std::max(smem, cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1], 2, b->idct == CJ_PIX_IDCT_TC));
     b->dev_of[i] = nd;
     b->dims.push_back(h.width);
     b->dims.push_back(h.height);
     b->dims.push_back(ch);
+    b->dims.push_back(h.nch == 3 ? (h.width * h.comp_sx[1] + h.hmax - 1) / h.hmax : 0);
+    b->dims.push_back(h.nch == 3 ? (h.height * h.comp_sy[1] + h.vmax - 1) / h.vmax : 0);
     b->outoff.push_back(d.out_off);
     nd++;
   }
@@ -1245,7 +1357,8 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
               CUDA_KERNEL_LAUNCH_ERROR);
   if (per_sm < 1) return UNSUPPORTED_ERROR;
   b->grid = std::min(per_sm, b->decode_ctas) * b->sm_count;
-  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pixel_batch, CJ_PIX_THREADS, b->smem_pix),
+  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                  &per_sm, (const void*)bt_pixel_kernel(b->idct, b->out_format), CJ_PIX_THREADS, b->smem_pix),
               CUDA_KERNEL_LAUNCH_ERROR);
   if (per_sm < 1) return UNSUPPORTED_ERROR;
   b->grid_pix = std::min(nptiles, per_sm * b->sm_count);
@@ -1279,6 +1392,7 @@ static CJBatchArgs bt_args(const CJBatch* b) {
   a.nwarps = b->nwarps;
   a.nptiles = b->nptiles;
   a.max_passes = b->nwarps + 2;
+  a.wait_limit = b->wait_limit;
   return a;
 }
 
@@ -1329,7 +1443,7 @@ static bool bt_build_graph(CJBatch* b) {
   }
   if (ok && b->grid_pix > 0) {
     cudaKernelNodeParams pp = kp;
-    pp.func = (void*)k_pixel_batch;
+    pp.func = (void*)bt_pixel_kernel(b->idct, b->out_format);
     pp.gridDim = dim3(b->grid_pix);
     pp.blockDim = dim3(CJ_PIX_THREADS);
     pp.sharedMemBytes = (unsigned)b->smem_pix;
@@ -1378,7 +1492,7 @@ int cjBatchRun(CJBatch* b) {
               CUDA_KERNEL_LAUNCH_ERROR);
   b->launches++;
   if (b->grid_pix > 0) {
-    k_pixel_batch<<<b->grid_pix, CJ_PIX_THREADS, b->smem_pix, s>>>(a);
+    bt_pixel_kernel(b->idct, b->out_format)<<<b->grid_pix, CJ_PIX_THREADS, b->smem_pix, s>>>(a);
     CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
     b->launches++;
   }
@@ -1409,7 +1523,8 @@ int cjBatchWait(CJBatch* b, int* errors) {
   CJ_CUDA_TRY(cudaStreamSynchronize(s), CUDA_KERNEL_LAUNCH_ERROR);
   const CJBatchCtl* ctl = (const CJBatchCtl*)b->h_ctl.p;
   int batch_err = 0;
-  if (b->n_dev && (ctl->timeout || ctl->passes > b->nwarps + 2)) batch_err = PROGRAMMER_ERROR;
+  if (b->n_dev && ctl->timeout) batch_err = CUDA_KERNEL_LAUNCH_ERROR;  // a grid barrier's wait ran out
+  else if (b->n_dev && ctl->passes > b->nwarps + 2) batch_err = PROGRAMMER_ERROR;
   const CJStatus* st = (const CJStatus*)b->h_st.p;
   if (errors)
     for (int i = 0; i < b->n_in; i++) {
@@ -1431,18 +1546,26 @@ int cjBatchDecode(CJBatch* b, int n, const unsigned char* blob, const int64_t* o
 const unsigned char* cjBatchImage(const CJBatch* b, int i, int* w, int* h, int* c) {
   if (i < 0 || i >= b->n_in || b->dev_of[i] < 0 || !b->h_out.p) return NULL;
   int k = b->dev_of[i];
-  if (w) *w = b->dims[3 * k];
-  if (h) *h = b->dims[3 * k + 1];
-  if (c) *c = b->dims[3 * k + 2];
+  if (w) *w = b->dims[5 * k];
+  if (h) *h = b->dims[5 * k + 1];
+  if (c) *c = b->dims[5 * k + 2];
   return (const unsigned char*)b->h_out.p + b->outoff[k];
 }
 
 int cjBatchImageGeometry(const CJBatch* b, int i, int* w, int* h, int* c) {
   if (i < 0 || i >= b->n_in || b->dev_of[i] < 0) return PROGRAMMER_ERROR;
   int k = b->dev_of[i];
-  if (w) *w = b->dims[3 * k];
-  if (h) *h = b->dims[3 * k + 1];
-  if (c) *c = b->dims[3 * k + 2];
+  if (w) *w = b->dims[5 * k];
+  if (h) *h = b->dims[5 * k + 1];
+  if (c) *c = b->dims[5 * k + 2];
+  return 0;
+}
+
+int cjBatchChromaGeometry(const CJBatch* b, int i, int* cw, int* ch) {
+  if (i < 0 || i >= b->n_in || b->dev_of[i] < 0) return PROGRAMMER_ERROR;
+  int k = b->dev_of[i];
+  if (cw) *cw = b->dims[5 * k + 3];
+  if (ch) *ch = b->dims[5 * k + 4];
   return 0;
 }
 
@@ -1452,6 +1575,20 @@ const unsigned char* cjBatchDeviceImage(const CJBatch* b, int i) {
 }
 
 void* cjBatchStream(const CJBatch* b) { return (void*)b->stream; }
+
+long long cjBatchCopyCoefficients(CJBatch* b, int i, short* dst, long long max_blocks) {
+  if (!b || !b->ready || i < 0 || i >= b->n_in || b->dev_of[i] < 0 || !dst) return PROGRAMMER_ERROR;
+  const int k = b->dev_of[i];
+  const CJImageDesc* dd = (const CJImageDesc*)b->h_desc.p;
+  const CJImageHeader* hh = (const CJImageHeader*)b->h_hdr.p;
+  const int64_t n = hh[k].total_blocks;
+  if (n > max_blocks) return PROGRAMMER_ERROR;
+  CJ_CUDA_TRY(cudaMemcpyAsync(dst, (const int16_t*)b->coef.p + dd[k].coef0 * 64, (size_t)n * 128,
+                              cudaMemcpyDeviceToHost, b->stream),
+              CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaStreamSynchronize(b->stream), CUDA_KERNEL_LAUNCH_ERROR);
+  return n;
+}
 
 int cjBatchPhaseTimes(const CJBatch* b, float* ms) {
   const CJBatchCtl* ctl = (const CJBatchCtl*)b->h_ctl.p;
@@ -1572,9 +1709,38 @@ int cjBatchAutotune(CJBatch* b, int n, const unsigned char* blob, const int64_t*
 #define CJ_NOALLOC_MAX_DEVICES 64
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CJ_NOALLOC_SCRATCH_BYTES];
-static unsigned char* g_noalloc_ptr[CJ_NOALLOC_MAX_DEVICES];  // device address per device
+// Device address of the array per device, set once under g_noalloc_mu; the
+// host-side symbol g_noalloc_scratch is not a device address.
+static std::atomic<unsigned char*> g_noalloc_ptr[CJ_NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_mu;
 
 static size_t bt_align(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// One-time set-up on device `dev` (current): the array's device address and
+// the kernels' shared-memory attributes.  Host threads calling at once wait
+// for the first; a failed set-up is retried by the next call.
+static unsigned char* bt_noalloc_base(int dev) {
+  unsigned char* p = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+  if (p) return p;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  p = g_noalloc_ptr[dev].load(std::memory_order_relaxed);
+  if (p) return p;
+  void* addr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+  if (e != cudaSuccess || !addr) {
+    cj_note_cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+    return nullptr;
+  }
+  e = bt_pixel_attrs();
+  if (e == cudaSuccess) e = bt_decode_attrs();
+  if (e != cudaSuccess) {
+    cj_note_cuda_error(e, "cjDecodeNoAlloc kernel attributes", __FILE__, __LINE__);
+    return nullptr;
+  }
+  p = (unsigned char*)addr;
+  g_noalloc_ptr[dev].store(p, std::memory_order_release);
+  return p;
+}
 
 extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned char* d_out,
                                size_t out_capacity, int* width, int* height, int* channels,
@@ -1583,21 +1749,8 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   int dev = 0;
   CJ_CUDA_TRY(cudaGetDevice(&dev), CUDA_MEM_ERROR);
   if (dev < 0 || dev >= CJ_NOALLOC_MAX_DEVICES) return UNSUPPORTED_ERROR;
-  if (!g_noalloc_ptr[dev]) {
-    // one-time set-up on this device: the static array's device address
-    // (the host-side symbol is not a device pointer)
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      cj_note_cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
-      return CUDA_MEM_ERROR;
-    }
-    CJ_CUDA_TRY(cudaFuncSetAttribute(k_pixel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024),
-                CUDA_MEM_ERROR);
-    CJ_CUDA_TRY(bt_decode_attrs(), CUDA_MEM_ERROR);
-    g_noalloc_ptr[dev] = (unsigned char*)p;
-  }
-  unsigned char* base = g_noalloc_ptr[dev];
+  unsigned char* base = bt_noalloc_base(dev);
+  if (!base) return CUDA_MEM_ERROR;
 
   // host parse on the stack
   JPGReader r;
@@ -1655,7 +1808,10 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   const int64_t scan_off = (int64_t)(r.pos - jpeg), scan_len = (int64_t)(r.end - r.pos);
   if ((uint64_t)scan_len > CJ_MAX_SCAN_BYTES) return UNSUPPORTED_ERROR;
 
-  // plan: one image, every buffer carved out of the static array
+  // plan: one image, every buffer carved out of the static array.  One image
+  // alone spreads over the whole GPU only with more, shorter subsequences
+  // than a batch uses: the single-image paths' 1024 bits (as openJPG), with
+  // the batch's full-width pixel tiles.
   const int S = CJ_SUB_BITS_DEFAULT;
   d.src_off = scan_off;
   d.raw_len = scan_len;
@@ -1709,12 +1865,18 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   g.T = d.T;
   const size_t smem_pix = cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1], 2);
   const size_t smem = BT_DECODE_SMEM;
+  // every check that can fail before the GPU runs anything: launch shapes
+  int sms = 0, per_dec = 0, per_pix = 0;
+  const bt_decode_fn dk = bt_decode_kernel(BT_DECODE_CTAS_DEFAULT);
+  CJ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), CUDA_MEM_ERROR);
+  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_dec, (const void*)dk, BT_THREADS, smem),
+              CUDA_KERNEL_LAUNCH_ERROR);
+  const bt_pixel_fn pk = bt_pixel_kernel(CJ_PIX_IDCT_INT, CJ_OUT_RGB);
+  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_pix, (const void*)pk, CJ_PIX_THREADS, smem_pix),
+              CUDA_KERNEL_LAUNCH_ERROR);
+  if (per_dec < 1 || per_pix < 1) return UNSUPPORTED_ERROR;
+  per_dec = std::min(per_dec, BT_DECODE_CTAS_DEFAULT);
 
-  cudaStream_t s = (cudaStream_t)stream;
-  CJ_CUDA_TRY(cudaMemcpyAsync(base + o_hdr, &h, sizeof(h), cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
-  CJ_CUDA_TRY(cudaMemcpyAsync(base + o_desc, &d, sizeof(d), cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
-  CJ_CUDA_TRY(cudaMemcpyAsync(base + o_blob, jpeg, size, cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
-  CJ_CUDA_TRY(cudaMemsetAsync(base + o_ctl, 0, sizeof(CJBatchCtl), s), CUDA_MEM_ERROR);
   CJBatchArgs a;
   a.hdr = (const CJImageHeader*)(base + o_hdr);
   a.desc = (const CJImageDesc*)(base + o_desc);
@@ -1741,27 +1903,35 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   a.nwarps = nwarps;
   a.nptiles = d.nptiles;
   a.max_passes = nwarps + 2;
-  int sms = 0, per_sm = 0;
-  CJ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), CUDA_MEM_ERROR);
-  const bt_decode_fn dk = bt_decode_kernel(BT_DECODE_CTAS_DEFAULT);
-  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)dk, BT_THREADS, smem),
-              CUDA_KERNEL_LAUNCH_ERROR);
-  if (per_sm < 1) return UNSUPPORTED_ERROR;
-  per_sm = std::min(per_sm, BT_DECODE_CTAS_DEFAULT);
+  a.wait_limit = 0;
+
+  // From the first queued copy on, every return waits for the stream: the
+  // shared array must be idle when the call returns.
+  cudaStream_t s = (cudaStream_t)stream;
+  auto fail = [&](cudaError_t e, const char* what, int code) {
+    cj_note_cuda_error(e, what, __FILE__, __LINE__);
+    cudaStreamSynchronize(s);
+    cudaGetLastError();
+    return code;
+  };
+  cudaError_t e = cudaMemcpyAsync(base + o_hdr, &h, sizeof(h), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + o_desc, &d, sizeof(d), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + o_blob, jpeg, size, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + o_ctl, 0, sizeof(CJBatchCtl), s);
+  if (e != cudaSuccess) return fail(e, "cjDecodeNoAlloc copies", CUDA_MEM_ERROR);
   void* args[] = {&a};
-  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)dk, dim3(per_sm * sms), dim3(BT_THREADS), args,
-                                          smem, s),
-              CUDA_KERNEL_LAUNCH_ERROR);
-  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pixel_batch, CJ_PIX_THREADS, smem_pix),
-              CUDA_KERNEL_LAUNCH_ERROR);
-  if (per_sm < 1) return UNSUPPORTED_ERROR;
-  k_pixel_batch<<<std::min(d.nptiles, per_sm * sms), CJ_PIX_THREADS, smem_pix, s>>>(a);
-  CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
+  e = cudaLaunchCooperativeKernel((const void*)dk, dim3(per_dec * sms), dim3(BT_THREADS), args, smem, s);
+  if (e != cudaSuccess) return fail(e, "cjDecodeNoAlloc decode kernel", CUDA_KERNEL_LAUNCH_ERROR);
+  pk<<<std::min(d.nptiles, per_pix * sms), CJ_PIX_THREADS, smem_pix, s>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(e, "cjDecodeNoAlloc pixel kernel", CUDA_KERNEL_LAUNCH_ERROR);
   CJStatus st;
   CJBatchCtl ctl;
-  CJ_CUDA_TRY(cudaMemcpyAsync(&st, base + o_st, sizeof(st), cudaMemcpyDeviceToHost, s), CUDA_MEM_ERROR);
-  CJ_CUDA_TRY(cudaMemcpyAsync(&ctl, base + o_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, s), CUDA_MEM_ERROR);
+  e = cudaMemcpyAsync(&st, base + o_st, sizeof(st), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&ctl, base + o_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return fail(e, "cjDecodeNoAlloc status copy", CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaStreamSynchronize(s), CUDA_KERNEL_LAUNCH_ERROR);
-  if (ctl.timeout || ctl.passes > nwarps + 2) return PROGRAMMER_ERROR;
+  if (ctl.timeout) return CUDA_KERNEL_LAUNCH_ERROR;
+  if (ctl.passes > nwarps + 2) return PROGRAMMER_ERROR;
   return cj_status_error(&st);
 }

@@ -8,8 +8,17 @@
 
 #include "cj_core.h"
 #include "cj_idct.cuh"
+#include "cj_tc.cuh"
 
 #define CJ_PIX_THREADS 256
+
+// iDCT arithmetic of the pixel stage (include/pixelTransformGPU.h CJ_IDCT_*)
+#define CJ_PIX_IDCT_INT 0  // the reference's fixed point: bit-exact
+#define CJ_PIX_IDCT_TC 2   // FP16 hi/lo tensor cores, FP32 accumulation
+// Output formats (include/cudajpeg.h CJ_OUTPUT_*)
+#define CJ_OUT_RGB 0     // interleaved RGB (grey: one plane), the reference's output
+#define CJ_OUT_PLANAR 1  // Y plane, then Cb and Cr planes at chroma resolution
+#define CJ_OUT_NV12 2    // Y plane, then Cb/Cr interleaved at chroma resolution
 
 // ---------------------------------------------------------------- TMA helpers
 __device__ __forceinline__ uint32_t cj_smem_addr(const void* p) {
@@ -57,6 +66,8 @@ struct CJPixGeom {
   int y_stride, c_stride; // tile plane strides (bytes)
   int ipr_shift;          // log2 of 8-pixel items per tile row (T * hmax)
   int sc1_off, tmp_off, y_off, cb_off, cr_off;
+  int a_off, b_off, big_off;  // tensor-core form: A tile, Kronecker basis, range flags
+  int cw, ch;             // chroma plane size (planar outputs)
 };
 
 // Row-pass results of one block: 8 rows of 8 int32, padded to 72 words so
@@ -65,6 +76,7 @@ struct CJPixGeom {
 
 struct alignas(16) CJPixSmemParams {
   int32_t q[4][64];       // dequantisation tables, natural order (int32: no unpacking per row)
+  uint16_t qh[4][64];     // the same as FP16 bit patterns (tensor-core form)
   uint16_t boff[64];      // per block of the tile: smem offset of its 8x8 destination
   uint8_t bc[64];         // per block of the tile: component
   uint8_t bq[64];         // per block of the tile: quantisation table
@@ -93,8 +105,11 @@ CJ_HD int cj_pix_check(const CJScanParams* hp) {
 // the two coefficient buffers sit at fixed offsets 0 and 8 KiB (a tile holds
 // at most 64 blocks), so tiles of different geometry -- consecutive tiles of
 // a batch CTA may come from different images -- never overlap the current
-// tile's working space.
-CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy, int nbuf = 1) {
+// tile's working space.  The tensor-core form (tc) needs no row-pass buffer
+// but a 128-row FP16 A tile (16 KiB), the hi/lo Kronecker basis (16 KiB)
+// and one range flag per block row, at offsets that do not depend on the
+// geometry.
+CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy, int nbuf = 1, bool tc = false) {
   g->y_stride = g->T * 8 * g->hmax;
   g->c_stride = g->nch == 3 ? g->T * 8 * csx : 0;
   g->ipr_shift = 0;
@@ -106,8 +121,19 @@ CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy, int nbuf = 1) {
     g->sc1_off = 8192;
     off = 16384;
   }
-  g->tmp_off = (int)off;
-  off += (size_t)g->T * g->bpm * CJ_TMP_STRIDE * 4;
+  g->a_off = g->b_off = g->big_off = 0;
+  if (tc) {
+    g->a_off = (int)off;
+    off += 16384;
+    g->b_off = (int)off;
+    off += 16384;
+    g->big_off = (int)off;
+    off += 64 * 8;
+    g->tmp_off = g->a_off;  // unused
+  } else {
+    g->tmp_off = (int)off;
+    off += (size_t)g->T * g->bpm * CJ_TMP_STRIDE * 4;
+  }
   g->y_off = (int)off;
   off += (size_t)g->y_stride * 8 * g->vmax;
   off = (off + 15) & ~(size_t)15;
@@ -183,7 +209,11 @@ __device__ __forceinline__ void cj_pixel_setup(const CJScanParams& prmr, const C
   const CJScanParams* prm = &prmr;
   CJPixSmemParams& P = *Pp;
   const int nblk = g.T * g.bpm;
-  for (int k = threadIdx.x; k < 4 * 64; k += blockDim.x) P.q[k >> 6][k & 63] = prm->qnat[k >> 6][k & 63];
+  for (int k = threadIdx.x; k < 4 * 64; k += blockDim.x) {
+    const int q = prm->qnat[k >> 6][k & 63];
+    P.q[k >> 6][k & 63] = q;
+    P.qh[k >> 6][k & 63] = __half_as_ushort(__int2half_rn(q));  // exact: 8-bit tables
+  }
   for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
     const int mi = k / g.bpm, ph = k - mi * g.bpm;
     const int c = prm->phase_comp[ph], bl = prm->phase_blk[ph], sxc = prm->comp_sx[c];
@@ -196,28 +226,12 @@ __device__ __forceinline__ void cj_pixel_setup(const CJScanParams& prmr, const C
   }
 }
 
-// One tile (after cj_pixel_setup for its image), MCU row `mrow`, MCUs
-// [mc0, mc0 + T), whose coefficients arrive
-// in `sc` on phase `parity` of `bar`: dequantise + integer iDCT into plane
-// tiles, then nearest upsampling + YCbCr->RGB (or a grey copy) into `out`.
-// Returns false if the copy did not land within the wait bound (recorded).
-// Ends with a barrier, so `sc` and the plane tiles are free afterwards.
-__device__ __forceinline__ bool cj_pixel_compute(uint8_t* __restrict__ out, CJStatus* st, const CJPixGeom& g,
-                                                 int mrow, int mc0, const int16_t* sc, uint8_t* smem,
-                                                 uint64_t* barp, uint32_t parity, CJPixSmemParams* Pp) {
-  CJPixSmemParams& P = *Pp;
-  const int nm = min(g.T, g.mcux - mc0);
-  const int nblk = nm * g.bpm;
+// Integer iDCT of a tile's blocks (coefficients in `sc`) into the plane
+// tiles: row pass with dequantisation on load, then column pass with level
+// shift and clip.  Ends with a barrier.
+__device__ __forceinline__ void cj_pixel_idct_int(const CJPixGeom& g, int nblk, const int16_t* sc, uint8_t* smem,
+                                                  const CJPixSmemParams& P) {
   int* tmp = reinterpret_cast<int*>(smem + g.tmp_off);
-  uint8_t* py = smem + g.y_off;
-  uint8_t* pcb = smem + g.cb_off;
-  uint8_t* pcr = smem + g.cr_off;
-  bool ok = cj_mbar_wait(barp, parity);
-  if (!__syncthreads_and(ok)) {
-    if (threadIdx.x == 0) atomicMax(&st->dec_err_key, ~((unsigned long long)CJ_DEV_CAPACITY));
-    return false;
-  }
-
   // Row pass: one thread per (block, row); dequantise on load.
   for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
     const int k = t >> 3, r = t & 7;
@@ -254,74 +268,244 @@ __device__ __forceinline__ bool cj_pixel_compute(uint8_t* __restrict__ out, CJSt
     for (int j = 0; j < 8; j++) *reinterpret_cast<uint16_t*>(dst + j * ps) = (uint16_t)cj_level2(o0[j], o1[j]);
   }
   __syncthreads();
+}
 
-  // Upsample + colour (or copy for grey) into the output image.
+// Tensor-memory state of a CTA running the tensor-core form: its 64-column
+// accumulator, the MMA-completion barrier and the phase it waits for next,
+// the float basis [u][x] (range fallback).
+struct CJTcState {
+  uint32_t tmem;
+  uint64_t* bar;
+  uint32_t parity;
+  const float* basis;
+};
+
+// FP32 CUDA-core iDCT rows 4h..4h+3 of one block (its int16 coefficients and
+// int32 dequantisation table): out[8y+x], y = 0..3.  The range fallback of
+// the tensor-core form, for blocks whose dequantised values FP16 cannot hold
+// exactly.
+static __device__ __noinline__ void cj_block_f32_half(const int16_t* blk, const int32_t* q, int h, const float* basis,
+                                               float* out) {
+  float t[64];
+  for (int v = 0; v < 8; v++) {
+    int in[8];
+    for (int u = 0; u < 8; u++) in[u] = (int)blk[8 * v + u] * q[8 * v + u];
+    cj_idct8_f32(in, basis, t + 8 * v);
+  }
+  for (int y = 0; y < 4; y++)
+    for (int x = 0; x < 8; x++) {
+      float s = 0.f;
+      for (int v = 0; v < 8; v++) s = fmaf(t[8 * v + x], basis[v * 8 + 4 * h + y], s);
+      out[8 * y + x] = s;
+    }
+}
+
+// Tensor-core iDCT of a tile's blocks (at most 64, rows of a 128-row A tile)
+// into the plane tiles.  A row kb = block kb's 64 coefficients dequantised in
+// FP16 (exact below 2048; a block row at or above it flags the block, whose
+// pixels then come from the FP32 fallback); thread 0 issues the 8 MMAs of
+// D = A Khi + A Klo; the epilogue reads D row kb (block kb) from tensor
+// memory -- warps w and w + 4 share lanes 32 (w & 3) .. +31 and take pixel
+// rows 0-3 and 4-7 -- rounds, level-shifts, clips and stores the bytes.
+// Returns false if the MMAs did not complete within the wait bound
+// (recorded).  Ends with a barrier.
+__device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, const int16_t* sc, uint8_t* smem,
+                                                 const CJPixSmemParams& P, CJTcState& tc, CJStatus* st) {
+  uint8_t* sA = smem + g.a_off;
+  uint8_t* big = smem + g.big_off;
+  for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
+    const int kb = t >> 3, v = t & 7;
+    const uint4 raw = *reinterpret_cast<const uint4*>(sc + kb * 64 + v * 8);
+    const uint4 qv = *reinterpret_cast<const uint4*>(&P.qh[P.bq[kb]][v * 8]);
+    const uint32_t rw[4] = {raw.x, raw.y, raw.z, raw.w}, qw[4] = {qv.x, qv.y, qv.z, qv.w};
+    uint32_t p[4], acc = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const __half2 c2 = __halves2half2(__short2half_rn((short)(rw[j] & 0xFFFFu)), __short2half_rn((short)(rw[j] >> 16)));
+      const __half2 pr = __hmul2(c2, *reinterpret_cast<const __half2*>(&qw[j]));
+      p[j] = *reinterpret_cast<const uint32_t*>(&pr);
+      // per half: |x| >= 2048 (0x6800, NaN and Inf above) sets bit 15 of
+      // (bits & 0x7FFF) + 0x1800; no carry crosses into the upper half
+      acc |= (p[j] & 0x7FFF7FFFu) + 0x18001800u;
+    }
+    big[t] = (acc & 0x80008000u) != 0;
+    *reinterpret_cast<uint4*>(sA + tc_core_off(kb, v * 8)) = make_uint4(p[0], p[1], p[2], p[3]);
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  if (threadIdx.x == 0)
+    tc_idct_mmas(tc.tmem, cj_smem_addr(sA), cj_smem_addr(smem + g.b_off), cj_smem_addr(tc.bar));
+  const bool ok = cj_mbar_wait(tc.bar, tc.parity);
+  tc.parity ^= 1u;
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) atomicMax(&st->dec_err_key, ~((unsigned long long)CJ_DEV_CAPACITY));
+    cj_mbar_wait(tc.bar, tc.parity ^ 1u);  // a bounded second chance for MMAs still in flight
+    return false;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int kb = 32 * (w & 3) + lane, h = w >> 2;
+  float d[32];
+  tc_ld32(tc.tmem + ((uint32_t)(32 * (w & 3)) << 16) + 32u * h, d);
+  if (kb < nblk) {
+    if (*reinterpret_cast<const uint64_t*>(big + kb * 8))
+      cj_block_f32_half(sc + kb * 64, P.q[P.bq[kb]], h, tc.basis, d);
+    const int ps = P.bc[kb] == 0 ? g.y_stride : g.c_stride;
+    uint8_t* dst = smem + P.boff[kb] + 4 * h * ps;
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+      *reinterpret_cast<uint2*>(dst + y * ps) =
+          make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
+                     tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  return true;
+}
+
+// Nearest upsampling + YCbCr->RGB (or a grey copy) of a tile's plane tiles
+// into the output image (CPUonly/src/pixelTransformCPU.c:110-172).
+__device__ __forceinline__ void cj_pixel_emit_rgb(uint8_t* __restrict__ out, const CJPixGeom& g, int mrow, int mc0,
+                                                  int nm, const uint8_t* smem) {
+  const uint8_t* py = smem + g.y_off;
+  const uint8_t* pcb = smem + g.cb_off;
+  const uint8_t* pcr = smem + g.cr_off;
   const int X0 = mc0 * 8 * g.hmax, Y0 = mrow * 8 * g.vmax;
   const int w = min(nm * 8 * g.hmax, g.width - X0);
   const int h = min(8 * g.vmax, g.height - Y0);
-  if (w > 0 && h > 0) {
-    if ((g.width & 7) == 0 && (((uintptr_t)out) & 7) == 0) {
-      // 8 pixels per item, items laid out (row, 8-pixel column) with a
-      // power-of-two number of items per tile row; 8-byte aligned stores
-      const int ipr = 1 << g.ipr_shift, per_row = w >> 3;
-      for (int t = threadIdx.x; t < (h << g.ipr_shift); t += blockDim.x) {
-        const int y = t >> g.ipr_shift, xi = t & (ipr - 1);
-        if (xi >= per_row) continue;
-        const int x0 = xi * 8;
-        const uint2 yv = *reinterpret_cast<const uint2*>(py + y * g.y_stride + x0);
-        if (g.nch == 3) {
-          const uint8_t* crow_b = pcb + (y >> g.ys) * g.c_stride;
-          const uint8_t* crow_r = pcr + (y >> g.ys) * g.c_stride;
-          CJChromaTerms d[8];
-          int dshift;
-          if (g.xs == 1) {  // 4 chroma samples, 4-byte aligned (x0 / 2 is a multiple of 4)
-            const uint32_t b4 = *reinterpret_cast<const uint32_t*>(crow_b + (x0 >> 1));
-            const uint32_t r4 = *reinterpret_cast<const uint32_t*>(crow_r + (x0 >> 1));
+  if (w <= 0 || h <= 0) return;
+  if ((g.width & 7) == 0 && (((uintptr_t)out) & 7) == 0) {
+    // 8 pixels per item, items laid out (row, 8-pixel column) with a
+    // power-of-two number of items per tile row; 8-byte aligned stores
+    const int ipr = 1 << g.ipr_shift, per_row = w >> 3;
+    for (int t = threadIdx.x; t < (h << g.ipr_shift); t += blockDim.x) {
+      const int y = t >> g.ipr_shift, xi = t & (ipr - 1);
+      if (xi >= per_row) continue;
+      const int x0 = xi * 8;
+      const uint2 yv = *reinterpret_cast<const uint2*>(py + y * g.y_stride + x0);
+      if (g.nch == 3) {
+        const uint8_t* crow_b = pcb + (y >> g.ys) * g.c_stride;
+        const uint8_t* crow_r = pcr + (y >> g.ys) * g.c_stride;
+        CJChromaTerms d[8];
+        int dshift;
+        if (g.xs == 1) {  // 4 chroma samples, 4-byte aligned (x0 / 2 is a multiple of 4)
+          const uint32_t b4 = *reinterpret_cast<const uint32_t*>(crow_b + (x0 >> 1));
+          const uint32_t r4 = *reinterpret_cast<const uint32_t*>(crow_r + (x0 >> 1));
 #pragma unroll
-            for (int j = 0; j < 4; j++) d[j] = cj_chroma_terms((b4 >> (8 * j)) & 0xFF, (r4 >> (8 * j)) & 0xFF);
-            dshift = 1;
-          } else if (g.xs == 0) {  // 8 chroma samples, 8-byte aligned
-            const uint2 b8 = *reinterpret_cast<const uint2*>(crow_b + x0);
-            const uint2 r8 = *reinterpret_cast<const uint2*>(crow_r + x0);
+          for (int j = 0; j < 4; j++) d[j] = cj_chroma_terms((b4 >> (8 * j)) & 0xFF, (r4 >> (8 * j)) & 0xFF);
+          dshift = 1;
+        } else if (g.xs == 0) {  // 8 chroma samples, 8-byte aligned
+          const uint2 b8 = *reinterpret_cast<const uint2*>(crow_b + x0);
+          const uint2 r8 = *reinterpret_cast<const uint2*>(crow_r + x0);
 #pragma unroll
-            for (int j = 0; j < 8; j++)
-              d[j] = cj_chroma_terms(((j < 4 ? b8.x : b8.y) >> (8 * (j & 3))) & 0xFF,
-                                     ((j < 4 ? r8.x : r8.y) >> (8 * (j & 3))) & 0xFF);
-            dshift = 0;
-          } else {  // wider chroma subsampling: per pixel
+          for (int j = 0; j < 8; j++)
+            d[j] = cj_chroma_terms(((j < 4 ? b8.x : b8.y) >> (8 * (j & 3))) & 0xFF,
+                                   ((j < 4 ? r8.x : r8.y) >> (8 * (j & 3))) & 0xFF);
+          dshift = 0;
+        } else {  // wider chroma subsampling: per pixel
 #pragma unroll
-            for (int j = 0; j < 8; j++) d[j] = cj_chroma_terms(crow_b[(x0 + j) >> g.xs], crow_r[(x0 + j) >> g.xs]);
-            dshift = 0;
-          }
-          uint32_t wds[6];
-          if (dshift) cj_rgb8(yv, d, 1, wds);
-          else cj_rgb8(yv, d, 0, wds);
-          uint2* o = reinterpret_cast<uint2*>(out + ((int64_t)(Y0 + y) * g.width + X0 + x0) * 3);
-          o[0] = make_uint2(wds[0], wds[1]);
-          o[1] = make_uint2(wds[2], wds[3]);
-          o[2] = make_uint2(wds[4], wds[5]);
-        } else {
-          *reinterpret_cast<uint2*>(out + (int64_t)(Y0 + y) * g.width + X0 + x0) = yv;
+          for (int j = 0; j < 8; j++) d[j] = cj_chroma_terms(crow_b[(x0 + j) >> g.xs], crow_r[(x0 + j) >> g.xs]);
+          dshift = 0;
         }
-      }
-    } else if (g.nch == 3) {
-      for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
-        int y = t / w, x = t - y * w;
-        int yy = py[y * g.y_stride + x] << 8;
-        int ci = (y >> g.ys) * g.c_stride + (x >> g.xs);
-        int cb = (int)pcb[ci] - 128, cr = (int)pcr[ci] - 128;
-        uint8_t* o = out + ((int64_t)(Y0 + y) * g.width + X0 + x) * 3;
-        o[0] = (uint8_t)cj_rgb_pack(yy, cb, cr, 0);
-        o[1] = (uint8_t)cj_rgb_pack(yy, cb, cr, 1);
-        o[2] = (uint8_t)cj_rgb_pack(yy, cb, cr, 2);
-      }
-    } else {
-      for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
-        int y = t / w, x = t - y * w;
-        out[(int64_t)(Y0 + y) * g.width + X0 + x] = py[y * g.y_stride + x];
+        uint32_t wds[6];
+        if (dshift) cj_rgb8(yv, d, 1, wds);
+        else cj_rgb8(yv, d, 0, wds);
+        uint2* o = reinterpret_cast<uint2*>(out + ((int64_t)(Y0 + y) * g.width + X0 + x0) * 3);
+        o[0] = make_uint2(wds[0], wds[1]);
+        o[1] = make_uint2(wds[2], wds[3]);
+        o[2] = make_uint2(wds[4], wds[5]);
+      } else {
+        *reinterpret_cast<uint2*>(out + (int64_t)(Y0 + y) * g.width + X0 + x0) = yv;
       }
     }
+  } else if (g.nch == 3) {
+    for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
+      int y = t / w, x = t - y * w;
+      int yy = py[y * g.y_stride + x] << 8;
+      int ci = (y >> g.ys) * g.c_stride + (x >> g.xs);
+      int cb = (int)pcb[ci] - 128, cr = (int)pcr[ci] - 128;
+      uint8_t* o = out + ((int64_t)(Y0 + y) * g.width + X0 + x) * 3;
+      o[0] = (uint8_t)cj_rgb_pack(yy, cb, cr, 0);
+      o[1] = (uint8_t)cj_rgb_pack(yy, cb, cr, 1);
+      o[2] = (uint8_t)cj_rgb_pack(yy, cb, cr, 2);
+    }
+  } else {
+    for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
+      int y = t / w, x = t - y * w;
+      out[(int64_t)(Y0 + y) * g.width + X0 + x] = py[y * g.y_stride + x];
+    }
   }
+}
+
+// Planar (Y, Cb, Cr planes) or NV12 (Y plane, then Cb/Cr interleaved) copy
+// of a tile's plane tiles, chroma at its own resolution (no upsampling, no
+// colour transform): the decoded samples themselves.  Chroma planes are
+// g.cw x g.ch (the reference's channel width and height, src/format.cu
+// decodeSOF); grey images have the Y plane only.
+template <int OUT>
+__device__ __forceinline__ void cj_pixel_emit_planes(uint8_t* __restrict__ out, const CJPixGeom& g, int mrow,
+                                                     int mc0, int nm, const uint8_t* smem) {
+  const int X0 = mc0 * 8 * g.hmax, Y0 = mrow * 8 * g.vmax;
+  const int w = min(nm * 8 * g.hmax, g.width - X0);
+  const int h = min(8 * g.vmax, g.height - Y0);
+  const uint8_t* py = smem + g.y_off;
+  for (int t = threadIdx.x; t < w * h; t += blockDim.x) {
+    const int y = t / w, x = t - y * w;
+    out[(int64_t)(Y0 + y) * g.width + X0 + x] = py[y * g.y_stride + x];
+  }
+  if (g.nch != 3) return;
+  const int cs = g.hmax >> g.xs, csy = g.vmax >> g.ys;  // chroma blocks per MCU across / down
+  const int cX0 = mc0 * 8 * cs, cY0 = mrow * 8 * csy;
+  const int cw = min(nm * 8 * cs, g.cw - cX0), ch = min(8 * csy, g.ch - cY0);
+  if (cw <= 0 || ch <= 0) return;
+  uint8_t* cbase = out + (int64_t)g.width * g.height;
+  const uint8_t* pcb = smem + g.cb_off;
+  const uint8_t* pcr = smem + g.cr_off;
+  for (int t = threadIdx.x; t < cw * ch; t += blockDim.x) {
+    const int y = t / cw, x = t - y * cw;
+    const uint8_t b = pcb[y * g.c_stride + x], r = pcr[y * g.c_stride + x];
+    const int64_t o = (int64_t)(cY0 + y) * g.cw + cX0 + x;
+    if (OUT == CJ_OUT_NV12) {
+      cbase[2 * o] = b;
+      cbase[2 * o + 1] = r;
+    } else {
+      cbase[o] = b;
+      cbase[(int64_t)g.cw * g.ch + o] = r;
+    }
+  }
+}
+
+// One tile (after cj_pixel_setup for its image), MCU row `mrow`, MCUs
+// [mc0, mc0 + T), whose coefficients arrive in `sc` on phase `parity` of
+// `bar`: the iDCT (MODE) into plane tiles, then the output (OUT) into `out`.
+// Returns false if the copy or the MMAs did not land within the wait bound
+// (recorded).  Ends with a barrier, so `sc` and the plane tiles are free
+// afterwards.
+template <int MODE, int OUT>
+__device__ __forceinline__ bool cj_pixel_tile(uint8_t* __restrict__ out, CJStatus* st, const CJPixGeom& g, int mrow,
+                                              int mc0, const int16_t* sc, uint8_t* smem, uint64_t* barp,
+                                              uint32_t parity, CJPixSmemParams* Pp, CJTcState* tc) {
+  const int nm = min(g.T, g.mcux - mc0);
+  const int nblk = nm * g.bpm;
+  bool ok = cj_mbar_wait(barp, parity);
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) atomicMax(&st->dec_err_key, ~((unsigned long long)CJ_DEV_CAPACITY));
+    return false;
+  }
+  if (MODE == CJ_PIX_IDCT_TC) {
+    if (!cj_pixel_idct_tc(g, nblk, sc, smem, *Pp, *tc, st)) return false;
+  } else {
+    cj_pixel_idct_int(g, nblk, sc, smem, *Pp);
+  }
+  if (OUT == CJ_OUT_RGB) cj_pixel_emit_rgb(out, g, mrow, mc0, nm, smem);
+  else cj_pixel_emit_planes<OUT>(out, g, mrow, mc0, nm, smem);
   __syncthreads();
   return true;
+}
+
+// The reference output with the reference arithmetic: integer iDCT, RGB.
+__device__ __forceinline__ bool cj_pixel_compute(uint8_t* __restrict__ out, CJStatus* st, const CJPixGeom& g,
+                                                 int mrow, int mc0, const int16_t* sc, uint8_t* smem,
+                                                 uint64_t* barp, uint32_t parity, CJPixSmemParams* Pp) {
+  return cj_pixel_tile<CJ_PIX_IDCT_INT, CJ_OUT_RGB>(out, st, g, mrow, mc0, sc, smem, barp, parity, Pp, nullptr);
 }

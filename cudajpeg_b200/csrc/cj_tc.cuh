@@ -1,0 +1,116 @@
+// cj_tc.cuh -- tensor-core (tcgen05) building blocks of the FP16 hi/lo
+// iDCT, shared by the plane kernel (plane.cu) and the batch pixel kernel.
+//
+// The 2-D iDCT of a block is one linear map on its 64 coefficients:
+//   s[8y+x] = sum_{v,u} F[8v+u] * B[v][y] * B[u][x],
+//   B[u][x] = c(u)/2 cos((2x+1) u pi / 16), c(0) = 1/sqrt(2)  (T.81 A.3.3)
+// so M blocks are one GEMM  D[M x 64] = A[M x 64] * K[64 x 64] with
+// K[8v+u][8y+x] = B[v][y] B[u][x].  A holds dequantised coefficients in FP16
+// (exact while |value| < 2048); K is split into FP16 halves Khi = fp16(K),
+// Klo = fp16(K - Khi) and D = A*Khi + A*Klo accumulates in FP32 in tensor
+// memory (tcgen05.mma kind::f16, M = 128, N = 64, K = 16 per instruction).
+//
+// Shared-memory operands use the K-major no-swizzle canonical layout: 8x8
+// "core matrices" of 8 rows x 16 bytes; core (r8, k8) of a 64-wide K operand
+// sits at ((r8 * 8 + k8) * 128) bytes.  LBO (next core along K) = 128 B,
+// SBO (next 8-row group) = 1024 B.
+#pragma once
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+__device__ __forceinline__ uint32_t tc_core_off(int r, int k) {
+  return (uint32_t)((((r >> 3) * 8 + (k >> 3)) * 128) + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(1024 >> 4) << 32) | (1ull << 46);
+}
+
+// kind::f16, D = F32, A = B = F16, both K-major, N = 64, M = 128
+#define TC_IDESC ((1u << 4) | (0u << 7) | (0u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24))
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"((uint32_t)TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+// The 8 MMAs of one 128-block tile (A at a_addr, Khi at b_addr, Klo at
+// b_addr + 8 KiB) into the accumulator at tmem, then a commit that arrives
+// on `bar` when they are done.  One thread.
+__device__ __forceinline__ void tc_idct_mmas(uint32_t tmem, uint32_t a_addr, uint32_t b_addr, uint32_t bar_addr) {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+  for (int kk = 0; kk < 4; kk++) tc_mma(tmem, tc_smem_desc(a_addr + kk * 256), tc_smem_desc(b_addr + kk * 256), kk > 0);
+#pragma unroll
+  for (int kk = 0; kk < 4; kk++)
+    tc_mma(tmem, tc_smem_desc(a_addr + kk * 256), tc_smem_desc(b_addr + 8192 + kk * 256), 1u);
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_addr)
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
+}
+
+// Tensor-memory columns of one CTA (warp 0 allocates and frees; the address
+// lands in *slot).  A power of two >= 32.
+__device__ __forceinline__ void tc_alloc(uint32_t* slot, uint32_t cols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(slot)),
+               "r"(cols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tc_dealloc(uint32_t tmem, uint32_t cols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols) : "memory");
+}
+
+// The 8x8 basis B[u][x] in float64 (`b64`) and float (`b32`), then Khi and
+// Klo of the Kronecker basis (row n = pixel 8y+x, column k = coefficient
+// 8v+u) in the B operand's core-matrix layout (`dst`, 8192 halves).  All
+// threads of the CTA; ends with a barrier.
+__device__ __forceinline__ void tc_build_basis(uint16_t* dst, double* b64, float* b32) {
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+    const int u = i >> 3, x = i & 7;
+    const double c = (u ? 0.5 : 0.5 * sqrt(0.5)) * cospi((double)((2 * x + 1) * u) / 16.0);
+    b64[i] = c;
+    b32[i] = (float)c;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 4096; e += blockDim.x) {
+    const int n = e >> 6, k = e & 63;
+    const double w = b64[(k >> 3) * 8 + (n >> 3)] * b64[(k & 7) * 8 + (n & 7)];
+    const __half hi = __double2half(w);
+    const __half lo = __double2half(w - (double)__half2float(hi));
+    const uint32_t off = tc_core_off(n, k) >> 1;
+    dst[off] = __half_as_ushort(hi);
+    dst[4096 + off] = __half_as_ushort(lo);
+  }
+  __syncthreads();
+}
+
+// Four iDCT outputs -> the bytes clip(round(v) + 128), v0 in the low byte:
+// signed saturating packs to [-128, 127], then a flip of each top bit
+// (s + 128 == s ^ 0x80 for a signed byte).
+__device__ __forceinline__ uint32_t tc_level4(float a, float b, float c, float d) {
+  uint32_t hi, r;
+  asm("cvt.pack.sat.s8.s32.b32 %0, %1, %2, 0;" : "=r"(hi) : "r"(__float2int_rn(d)), "r"(__float2int_rn(c)));
+  asm("cvt.pack.sat.s8.s32.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(__float2int_rn(b)), "r"(__float2int_rn(a)), "r"(hi));
+  return r ^ 0x80808080u;
+}

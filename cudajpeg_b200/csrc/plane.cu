@@ -1,10 +1,10 @@
 // plane.cu -- per-component plane iDCT (cjIDCTPlane), the C launcher that
 // replaces the reference's __global__ iDCT_GPU (include/pixelTransformGPU.h:6-10,
-// src/pixelTransformGPU.cu:25-142), in two CUDA-core arithmetic forms:
+// src/pixelTransformGPU.cu:25-142), in three arithmetic forms:
 //   CJ_IDCT_INT  the reference's fixed-point separable iDCT, bit-exact;
 //   CJ_IDCT_F32  an FP32 separable iDCT (orthonormal DCT-II basis), rounded
-//                to nearest at the end; the baseline for the tensor-core form
-//                in idct_tc.cu.
+//                to nearest at the end; the baseline for the tensor-core form;
+//   CJ_IDCT_TC   FP16 hi/lo Kronecker basis on tensor cores (k_idct_tc).
 // Input is the quantised int16 block buffer decodeScanGPU leaves on the
 // device; the component's blocks are gathered from the MCU-interleaved order.
 #include <cuda_fp16.h>
@@ -18,6 +18,7 @@
 #include "cj_internal.h"
 #include "cj_idct.cuh"
 #include "cj_pixel.cuh"
+#include "cj_tc.cuh"
 
 #define CJ_PLANE_BLOCKS 32   // 8x8 blocks per CTA
 #define CJ_PLANE_THREADS 256  // one thread per (block, row)
@@ -148,61 +149,15 @@ int cj_upload_basis() {
 
 // ---------------------------------------------------------------- tensor cores
 //
-// The 2-D iDCT of a block is one linear map on its 64 coefficients:
-//   s[8y+x] = sum_{v,u} F[8v+u] * B[v][y] * B[u][x],   B = c_idct_basis
-// so a tile of 128 blocks is one GEMM  D[128 x 64] = A[128 x 64] * K[64 x 64]
-// with K[8v+u][8y+x] = B[v][y] B[u][x].  A holds the dequantised
-// coefficients in FP16 (exact: |value| <= 2048 for every block a real encoder
-// produces; larger blocks are redone on CUDA cores in FP32).  K is split into
-// FP16 halves Khi = fp16(K), Klo = fp16(K - Khi), and D = A*Khi + A*Klo is
-// accumulated in FP32 in tensor memory by tcgen05.mma (M=128, N=64, K=16 per
-// instruction, 8 instructions per tile), issued by one thread.
-//
-// Shared-memory operands use the K-major no-swizzle canonical layout: 8x8
-// "core matrices" of 8 rows x 16 bytes; core (r8, k8) of a 64-wide K operand
-// sits at ((r8 * 8 + k8) * 128) bytes.  LBO (next core along K) = 128 B,
-// SBO (next 8-row group) = 1024 B.
+// The plane iDCT as one GEMM per 128-block tile (cj_tc.cuh): D = A * Khi +
+// A * Klo with A the dequantised coefficients in FP16 (exact: |value| <= 2048
+// for every block a real encoder produces; larger blocks are redone on CUDA
+// cores in FP32), FP32 accumulation in tensor memory, a tcgen05.ld epilogue.
 
 #define TC_M 128
 #define TC_THREADS 128
 
 static uint16_t* g_tc_basis = nullptr;  // device: Khi then Klo, core-matrix layout
-
-__device__ __forceinline__ uint32_t tc_core_off(int r, int k) {
-  return (uint32_t)((((r >> 3) * 8 + (k >> 3)) * 128) + (r & 7) * 16 + (k & 7) * 2);
-}
-
-__device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) |
-         ((uint64_t)(1024 >> 4) << 32) | (1ull << 46);
-}
-
-// kind::f16, D = F32, A = B = F16, both K-major, N = 64, M = 128
-#define TC_IDESC ((1u << 4) | (0u << 7) | (0u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24))
-
-__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"((uint32_t)TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-
-__device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
-        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
-        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
-}
 
 // FP32 CUDA-core iDCT of one block straight from global memory (the range
 // fallback of the tensor-core kernel): out[8y+x].

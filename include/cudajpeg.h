@@ -89,6 +89,13 @@ int cjDebugHuffDecode(const unsigned char counts[16], const unsigned char *symbo
 int cjDebugStepTable(const unsigned char counts[16], const unsigned char *symbols, int ac,
                      unsigned short *out);
 
+/* Which device code the library was built with: archs[0..] receives the
+ * compute capabilities compiled in (1000 = sm_100a), up to max_archs of
+ * them, and the count is returned; *binary_version (may be NULL) receives
+ * the binary version of the device code the current GPU would run (100 on
+ * a B200), or 0 without a GPU. */
+int cjBuildInfo(int *archs, int max_archs, int *binary_version);
+
 /* ---- Batched decoder: many JPEGs in one persistent, cooperative kernel ----
  *
  * The files of a batch lie back to back in one host buffer `blob` (pinned
@@ -113,6 +120,31 @@ int cjBatchSetSubsequenceBits(CJBatch *b, int bits);
  * 128 pixels across). */
 int cjBatchSetTuning(CJBatch *b, int sub_bits, int decode_ctas_per_sm, int pixel_tile_cap);
 void cjBatchGetTuning(const CJBatch *b, int *sub_bits, int *decode_ctas_per_sm, int *pixel_tile_cap);
+/* Output of a batch staged from now on.  format: CJ_OUTPUT_RGB (default:
+ * interleaved RGB, grey as one plane -- the reference's output),
+ * CJ_OUTPUT_PLANAR (the Y plane width*height, then the Cb and Cr planes at
+ * chroma resolution cw*ch, cw = ceil(width * Hc / Hmax), ch = ceil(height *
+ * Vc / Vmax), the reference's channel sizes, src/format.cu:242-354; no
+ * upsampling, no colour transform) or CJ_OUTPUT_NV12 (the Y plane, then Cb
+ * and Cr interleaved at chroma resolution).  Grey images have the Y plane
+ * only in every format.  idct: CJ_IDCT_INT (default: the reference's fixed
+ * point, src/pixelTransformGPU.cu:25-142, bit-exact) or CJ_IDCT_TC (FP16
+ * hi/lo basis on tensor cores, FP32 accumulation: within 0.5 of an exact
+ * iDCT before rounding, samples within +-1 of CJ_IDCT_INT).  Returns
+ * PROGRAMMER_ERROR for anything else. */
+#define CJ_OUTPUT_RGB 0
+#define CJ_OUTPUT_PLANAR 1
+#define CJ_OUTPUT_NV12 2
+int cjBatchSetOutput(CJBatch *b, int format, int idct);
+void cjBatchGetOutput(const CJBatch *b, int *format, int *idct);
+/* Bound on each grid-barrier wait of the decode kernel, in polls of about
+ * 128 ns (0 = the default, 2^24 polls: about 2 s).  A wait that runs out
+ * ends the run early -- every CTA leaves the kernel at its next barrier and
+ * the pixel kernel does nothing -- and cjBatchWait then reports
+ * CUDA_KERNEL_LAUNCH_ERROR for the batch and for every image of it.  The
+ * batch stays usable: the next run (e.g. after restoring the default)
+ * decodes normally.  A tiny limit is a way to test that path. */
+int cjBatchSetWaitLimit(CJBatch *b, unsigned polls);
 /* Autotuner: times the given batch (device time, median of `reps` runs)
  * under every subsequence size in {512, 1024, 2048, 4096} x decode CTAs per
  * SM in {3, 4, 5}, then pixel tile caps {8, 4, 2} at the best of those, and
@@ -133,7 +165,9 @@ int cjBatchRun(CJBatch *b);
 /* Queue the device->host copy of all outputs into the batch's pinned buffer. */
 int cjBatchFetch(CJBatch *b);
 /* Wait for the queued work; errors[i] (may be NULL) gets image i's format.h
- * code.  Returns 0 or a batch-level error. */
+ * code.  Returns 0 or a batch-level error (CUDA_KERNEL_LAUNCH_ERROR when a
+ * grid-barrier wait of the decode kernel timed out; see
+ * cjBatchSetWaitLimit). */
 int cjBatchWait(CJBatch *b, int *errors);
 /* Stage + run + fetch + wait. */
 int cjBatchDecode(CJBatch *b, int n, const unsigned char *blob, const int64_t *offsets,
@@ -145,7 +179,18 @@ const unsigned char *cjBatchDeviceImage(const CJBatch *b, int i);
 /* Width, height and channels of image i of the staged batch (known after
  * cjBatchStage); PROGRAMMER_ERROR if image i was rejected by the host parse. */
 int cjBatchImageGeometry(const CJBatch *b, int i, int *width, int *height, int *channels);
+/* Chroma plane width and height of image i (0 for grey): the Cb / Cr plane
+ * size of the planar and NV12 output formats. */
+int cjBatchChromaGeometry(const CJBatch *b, int i, int *cw, int *ch);
 void *cjBatchStream(const CJBatch *b);
+/* Copy image i's quantised int16 coefficient blocks of the last run to host
+ * memory `dst` (natural order, 64 per block, blocks in MCU scan order with
+ * all components interleaved, DC already predicted -- the reference's
+ * working_space content divided by the quantisation table, before the
+ * split into components, src/decodeScanGPU.cu:435-452).  Waits for the
+ * batch's stream.  Returns the number of blocks, or PROGRAMMER_ERROR when
+ * image i was rejected or max_blocks is too small. */
+long long cjBatchCopyCoefficients(CJBatch *b, int i, short *dst, long long max_blocks);
 /* stats[0..15]: images submitted, images on the device, decode-kernel CTAs,
  * warp items, destuff tiles, pixel tiles, fix-up passes of the last run,
  * input bytes, output bytes, pixel-kernel dynamic shared memory, kernel
@@ -179,10 +224,16 @@ int cjBatchPhaseTimes(const CJBatch *b, float *ms);
  * UNSUPPORTED_ERROR and a message on stderr naming the bytes it needs.
  *
  * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  Every call shares the array, so calls that
- * overlap on the GPU (from different host threads or streams) race: run them
- * one after another.  d_out receives RGB (width*height*3) or grey
+ * (cudaGetSymbolAddress) with that device current and remembers it for the
+ * life of the process; make that first call before any stream capture.  The
+ * remembered address belongs to the device's context: after a
+ * cudaDeviceReset the function must not be called again in this process.
+ * Every call shares the array, so calls that overlap on the GPU (from
+ * different host threads or streams) race: run them one after another.
+ * Before queueing any GPU work the call checks everything it can (header,
+ * output capacity, working-memory size, launch shapes); once work is queued,
+ * every return -- success or error -- comes after the stream has finished
+ * it.  d_out receives RGB (width*height*3) or grey
  * (width*height) bytes and out_capacity is its size in bytes (too small:
  * PROGRAMMER_ERROR).  width/height/channels are filled once the header has
  * been parsed.  The call waits for its own work on `stream` (NULL = the

@@ -114,3 +114,32 @@ def test_autotune_keeps_results(cj, oracle_mod):
                 assert np.array_equal(b.image(k), ref.pixels), k
 
 
+
+
+def test_barrier_timeout_stops_the_batch(cj, oracle_mod):
+    """A grid-barrier wait that runs out (a limit of one poll: the first CTAs
+    at a barrier give up before the last arrive) ends the run with
+    CUDA_KERNEL_LAUNCH_ERROR promptly, without running later phases on
+    unsettled data; the same decoder then decodes the batch exactly."""
+    import time
+
+    files = [s.data for s in W.mixed_batch(n=24, seed=41, max_side=900)]
+    blob, offsets, sizes = cj.Batch.pack(files)
+    with cj.Batch() as b:
+        b.stage(blob.ctypes.data, offsets, sizes)
+        b.set_wait_limit(1)
+        t0 = time.perf_counter()
+        b.run()
+        err, errs = b.wait_status()
+        assert time.perf_counter() - t0 < 5.0
+        assert err == cj.CUDA_KERNEL_LAUNCH_ERROR
+        assert set(errs) == {cj.CUDA_KERNEL_LAUNCH_ERROR}
+        b.set_wait_limit(0)
+        b.run()
+        b.fetch()
+        errs = b.wait()
+        for k, data in enumerate(files):
+            ref = oracle_mod.decode(data)
+            assert errs[k] == ref.error, k
+            if ref.error == 0:
+                assert np.array_equal(b.image(k), ref.pixels), k

@@ -146,3 +146,9 @@ def test_reference_main_dropin(tmp_path, oracle_mod):
         assert raw.startswith(header)
         px = np.frombuffer(raw[len(header):], np.uint8)
         assert np.array_equal(px, oracle_mod.decode(s.data).pixels.reshape(-1))
+
+
+def test_device_code_runs_as_sm100(cj):
+    """The device code the B200 runs is the library's own sm_100 binary (no
+    PTX JIT of another target)."""
+    assert cj.build_info()["binary_version"] == 100
