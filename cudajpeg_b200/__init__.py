@@ -54,7 +54,7 @@ EXPORTED = [
     "cjServerRelease", "cjServerStats", "cjServerReplay", "cjServerSetTuning",
     "cjBatchSetTuning", "cjBatchGetTuning", "cjBatchAutotune", "cjDebugStepTable",
     "cjBatchCopyCoefficients", "cjBuildInfo", "cjBatchSetWaitLimit", "cjBatchSetOutput",
-    "cjBatchGetOutput", "cjBatchChromaGeometry",
+    "cjBatchGetOutput", "cjBatchChromaGeometry", "cjBatchDLPack", "cjServerDLPack", "cjDLPackFree",
 ]
 
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
@@ -148,6 +148,11 @@ def load(build_if_missing: bool = True):
     lib.cjBatchSetOutput.argtypes = [vp, C.c_int, C.c_int]
     lib.cjBatchGetOutput.argtypes = [vp, ip, ip]
     lib.cjBatchChromaGeometry.argtypes = [vp, C.c_int, ip, ip]
+    lib.cjBatchDLPack.restype = vp
+    lib.cjBatchDLPack.argtypes = [vp, C.c_int]
+    lib.cjServerDLPack.restype = vp
+    lib.cjServerDLPack.argtypes = [vp, C.c_longlong]
+    lib.cjDLPackFree.argtypes = [vp]
     lib.cjBatchGetTuning.argtypes = [vp, ip, ip, ip]
     lib.cjBatchAutotune.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, C.POINTER(C.c_float),
                                     C.POINTER(C.c_float), C.c_int]
@@ -412,6 +417,17 @@ class Batch:
         return _image_view(p, w.value, h.value, c.value, getattr(self, "fmt", OUTPUT_RGB),
                            self._chroma_size(i), copy)
 
+    def device_tensor(self, i: int):
+        """Image i of the last run as a torch tensor on the GPU, without a
+        copy (cjBatchDLPack through the DLPack protocol).  A view of the
+        batch's output buffer: valid until the batch is staged again or
+        closed."""
+        import torch
+        p = self.lib.cjBatchDLPack(self.ptr, i)
+        if not p:
+            raise DecodeError(PROGRAMMER_ERROR, f"no device image {i}")
+        return torch.from_dlpack(DLPackView(p, self.lib))
+
     def _chroma_size(self, i: int):
         """(cw, ch) of image i: the reference's channel sizes."""
         cw, ch = C.c_int(0), C.c_int(0)
@@ -550,6 +566,53 @@ def idct_blocks_raw(coef_q: np.ndarray, q_nat: np.ndarray, mode: int) -> np.ndar
         raise DecodeError(err, "cjIDCTBlocksRaw")
     torch.cuda.synchronize()
     return out.cpu().numpy()
+
+
+_DESTRUCTOR = C.CFUNCTYPE(None, C.c_void_p)
+
+
+@_DESTRUCTOR
+def _capsule_destructor(capsule):
+    """Frees a DLPack descriptor no consumer took (its capsule kept the name
+    "dltensor"; a consumer renames it "used_dltensor" and owns it)."""
+    api = C.pythonapi
+    if api.PyCapsule_IsValid(C.c_void_p(capsule), b"dltensor"):
+        p = api.PyCapsule_GetPointer(C.c_void_p(capsule), b"dltensor")
+        load().cjDLPackFree(p)
+
+
+class DLPackView:
+    """One DLManagedTensor* from the library as a DLPack producer
+    (``__dlpack__`` / ``__dlpack_device__``), for torch.from_dlpack and the
+    like.  The decode work that writes the image is ordered on the library's
+    stream; callers synchronise it (cjBatchWait) before consuming."""
+
+    def __init__(self, ptr: int, lib):
+        self.ptr = ptr
+        self.lib = lib
+        t = C.cast(C.c_void_p(ptr), C.POINTER(C.c_int32 * 4))  # data pointer, then DLDevice
+        self.device_id = int(t.contents[3])
+
+    def __dlpack_device__(self):
+        return (2, self.device_id)  # kDLCUDA
+
+    def __dlpack__(self, stream=None, **kwargs):
+        if self.ptr is None:
+            raise RuntimeError("DLPack tensor already exported")
+        api = C.pythonapi
+        api.PyCapsule_New.restype = C.py_object
+        api.PyCapsule_New.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+        api.PyCapsule_IsValid.argtypes = [C.c_void_p, C.c_char_p]
+        api.PyCapsule_GetPointer.restype = C.c_void_p
+        api.PyCapsule_GetPointer.argtypes = [C.c_void_p, C.c_char_p]
+        cap = api.PyCapsule_New(self.ptr, b"dltensor", C.cast(_capsule_destructor, C.c_void_p))
+        self.ptr = None
+        return cap
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            self.lib.cjDLPackFree(self.ptr)
+            self.ptr = None
 
 
 def _image_view(p: int, w: int, h: int, c: int, fmt: int, chroma, copy: bool):

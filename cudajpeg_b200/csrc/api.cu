@@ -1,6 +1,7 @@
 // api.cu -- plain-C accessors and tuning knobs of libcudajpeg (cudajpeg.h).
 #include <stddef.h>
 
+#include "../../include/cj_dlpack.h"
 #include "../../include/cudajpeg.h"
 #include "cj_internal.h"
 #include <new>
@@ -150,4 +151,46 @@ extern "C" int cjBuildInfo(int* archs, int max_archs, int* binary_version) {
     cudaGetLastError();
   }
   return n;
+}
+
+// ---------------------------------------------------------------- DLPack views
+
+// The descriptor and its shape / strides in one allocation.
+struct CJDLTensor {
+  DLManagedTensor t;
+  int64_t shape[3];
+  int64_t strides[3];
+};
+
+static void cj_dl_delete(DLManagedTensor* self) { delete static_cast<CJDLTensor*>(self->manager_ctx); }
+
+// A compact row-major uint8 tensor view of device memory.
+DLManagedTensor* cj_dl_view(void* data, int device, int ndim, const int64_t* shape) {
+  if (!data || ndim < 1 || ndim > 3) return nullptr;
+  CJDLTensor* d = new (std::nothrow) CJDLTensor;
+  if (!d) return nullptr;
+  int64_t stride = 1;
+  for (int k = ndim - 1; k >= 0; k--) {
+    d->shape[k] = shape[k];
+    d->strides[k] = stride;
+    stride *= shape[k];
+  }
+  DLTensor& x = d->t.dl_tensor;
+  x.data = data;
+  x.device.device_type = kDLCUDA;
+  x.device.device_id = device;
+  x.ndim = ndim;
+  x.dtype.code = kDLUInt;
+  x.dtype.bits = 8;
+  x.dtype.lanes = 1;
+  x.shape = d->shape;
+  x.strides = d->strides;
+  x.byte_offset = 0;
+  d->t.manager_ctx = d;
+  d->t.deleter = cj_dl_delete;
+  return &d->t;
+}
+
+extern "C" void cjDLPackFree(DLManagedTensor* t) {
+  if (t && t->deleter) t->deleter(t);
 }

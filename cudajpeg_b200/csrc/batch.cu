@@ -32,6 +32,7 @@
 #include <thread>
 #include <vector>
 
+#include "../../include/cj_dlpack.h"
 #include "../../include/cudajpeg.h"
 #include "cj_entropy.cuh"
 #include "cj_idct.cuh"
@@ -1575,6 +1576,19 @@ const unsigned char* cjBatchDeviceImage(const CJBatch* b, int i) {
 }
 
 void* cjBatchStream(const CJBatch* b) { return (void*)b->stream; }
+
+DLManagedTensor* cjBatchDLPack(CJBatch* b, int i) {
+  if (!b || !b->ready || i < 0 || i >= b->n_in || b->dev_of[i] < 0) return NULL;
+  const int k = b->dev_of[i];
+  const int64_t w = b->dims[5 * k], h = b->dims[5 * k + 1], c = b->dims[5 * k + 2];
+  void* p = (unsigned char*)b->out.p + b->outoff[k];
+  if (c == 3 && b->out_format != CJ_OUT_RGB) {
+    const int64_t n[1] = {w * h + 2 * (int64_t)b->dims[5 * k + 3] * b->dims[5 * k + 4]};
+    return cj_dl_view(p, b->device, 1, n);
+  }
+  const int64_t shape[3] = {h, w, 3};
+  return cj_dl_view(p, b->device, c == 3 ? 3 : 2, shape);
+}
 
 long long cjBatchCopyCoefficients(CJBatch* b, int i, short* dst, long long max_blocks) {
   if (!b || !b->ready || i < 0 || i >= b->n_in || b->dev_of[i] < 0 || !dst) return PROGRAMMER_ERROR;

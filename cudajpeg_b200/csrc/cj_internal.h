@@ -105,3 +105,8 @@ int cj_status_error(const CJStatus* st);
   } while (0)
 
 void cj_note_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+
+// A compact row-major uint8 DLPack view of device memory (api.cu); the
+// descriptor is freed by its deleter.
+struct DLManagedTensor;
+DLManagedTensor* cj_dl_view(void* data, int device, int ndim, const int64_t* shape);

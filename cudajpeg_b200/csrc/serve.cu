@@ -22,6 +22,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "../../include/cj_dlpack.h"
 #include "../../include/cudajpeg.h"
 #include "cj_internal.h"
 
@@ -305,6 +306,13 @@ int cjServerCopyOut(CJServer* s, long long ticket, unsigned char* host_dst, size
   lk.unlock();  // the engine is HELD until this ticket is released
   CJ_CUDA_TRY(cudaMemcpy(host_dst, src, n, cudaMemcpyDeviceToHost), CUDA_MEM_ERROR);
   return 0;
+}
+
+DLManagedTensor* cjServerDLPack(CJServer* s, long long ticket) {
+  std::lock_guard<std::mutex> g(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end() || !it->second.done || it->second.error || !it->second.device_pixels) return NULL;
+  return cjBatchDLPack(s->engines[it->second.engine].batch, it->second.slot);
 }
 
 void cjServerRelease(CJServer* s, long long ticket) {

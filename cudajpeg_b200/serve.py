@@ -22,7 +22,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import DecodeError, load
+from . import PROGRAMMER_ERROR, DecodeError, DLPackView, load
 
 
 class _Result(C.Structure):
@@ -84,6 +84,15 @@ class Server:
         if rc:
             raise DecodeError(rc, f"cjServerCopyOut({ticket})")
         return out
+
+    def device_tensor(self, ticket: int):
+        """A finished request's pixels as a torch tensor on the GPU, without
+        a copy (cjServerDLPack); valid until release(ticket)."""
+        import torch
+        p = self.lib.cjServerDLPack(self.ptr, ticket)
+        if not p:
+            raise DecodeError(PROGRAMMER_ERROR, f"request {ticket} has no device pixels")
+        return torch.from_dlpack(DLPackView(p, self.lib))
 
     def set_tuning(self, sub_bits: int = 0, decode_ctas_per_sm: int = 0, pixel_tile_cap: int = 0):
         err = self.lib.cjServerSetTuning(self.ptr, sub_bits, decode_ctas_per_sm, pixel_tile_cap)

@@ -168,6 +168,9 @@ def _load_ref():
         cpu.refcpu_info.argtypes = [C.c_void_p, C.c_void_p]
         cpu.refcpu_pixels.argtypes = [C.c_void_p, C.c_void_p]
         cpu.refcpu_close.argtypes = [C.c_void_p]
+        cpu.refcpu_open_any.restype = C.c_void_p
+        cpu.refcpu_open_any.argtypes = [C.c_char_p]
+        cpu.refcpu_use_gputree.argtypes = [C.c_char_p]
         cpu.refcpu_bench.restype = C.c_double
         cpu.refcpu_bench.argtypes = [C.POINTER(C.c_char_p), C.c_int, C.c_int, C.c_int,
                                      C.POINTER(C.c_longlong), C.POINTER(C.c_int)]
@@ -177,6 +180,10 @@ def _load_ref():
         gpu.refgpu_open.argtypes = [C.c_void_p, C.c_char_p]
         gpu.refgpu_info.argtypes = [C.c_void_p, C.c_void_p]
         gpu.refgpu_coefs.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        # restart-marker files, which CPUonly rejects, through the reference's
+        # GPU-tree coefficient decoder + CPUonly's iDCT and colour stage
+        if not cpu.refcpu_use_gputree(os.path.join(REF_DIR, "libref_gputree.so").encode()):
+            raise OSError("libref_gputree.so could not be loaded into the CPUonly harness")
         _ref_cpu, _ref_gpu = cpu, gpu
     return _ref_cpu, _ref_gpu
 
@@ -200,11 +207,14 @@ class _QuietStdout:
         os.close(self.null)
 
 
-def ref_cpu_pixels(path: str):
-    """Reference CPUonly decode of a file -> pixels array, or None on failure."""
+def ref_cpu_pixels(path: str, restart: bool = False):
+    """Reference CPUonly decode of a file -> pixels array, or None on failure.
+    restart=True: a file CPUonly rejects (restart markers) goes through the
+    reference's GPU-tree coefficient decoder (src/decodeScanCPU.cu:98-152)
+    and CPUonly's iDCT and colour stage instead."""
     cpu, _ = _load_ref()
     with _QuietStdout():
-        h = cpu.refcpu_open(path.encode())
+        h = (cpu.refcpu_open_any if restart else cpu.refcpu_open)(path.encode())
     if not h:
         return None
     try:
@@ -242,7 +252,9 @@ def ref_gpu_coefs(path: str):
 
 
 def ref_cpu_bench(paths, iters: int, threads: int):
-    """Time the reference CPUonly decoder: (seconds, pixels, failures)."""
+    """Time the reference CPUonly decoder -- restart-marker files through the
+    GPU-tree coefficient decoder + CPUonly pixel stage -- : (seconds, pixels,
+    failures)."""
     cpu, _ = _load_ref()
     arr = (C.c_char_p * len(paths))(*[p.encode() for p in paths])
     px = C.c_longlong(0)

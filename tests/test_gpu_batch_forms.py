@@ -109,3 +109,32 @@ def test_tensor_core_form(cj, oracle_mod, files):
           f"RGB within +-1: {rgb_within / rgb_n:.6f}, max |diff| {rgb_max}")
     assert exact / n > 0.95
     assert rgb_max <= 3 and rgb_within / rgb_n > 0.99
+
+
+def test_device_tensors_through_dlpack(cj, oracle_mod, files):
+    """Decoded images handed to torch without a copy (cjBatchDLPack,
+    cjServerDLPack): same bytes as the host copies and the oracle."""
+    import torch
+
+    from cudajpeg_b200 import serve as sv
+    with cj.Batch() as b:
+        imgs, errs = b.decode(files[:8])
+        for k in range(8):
+            t = b.device_tensor(k)
+            assert t.is_cuda and t.dtype == torch.uint8 and tuple(t.shape) == imgs[k].shape
+            assert t.data_ptr() == b.lib.cjBatchDeviceImage(b.ptr, k)  # a view, not a copy
+            assert np.array_equal(t.cpu().numpy(), imgs[k])
+            assert np.array_equal(imgs[k], oracle_mod.decode(files[k]).pixels)
+        b.set_output(cj.OUTPUT_NV12, cj.IDCT_INT)
+        imgs, errs = b.decode(files[:2])
+        flat = b.device_tensor(0)
+        y, cbcr = imgs[0]
+        assert flat.dim() == 1 and flat.numel() == y.size + cbcr.size
+        assert np.array_equal(flat.cpu().numpy(), np.concatenate([y.ravel(), cbcr.ravel()]))
+    with sv.Server(engines=1) as s:
+        tk = s.submit(files[0])
+        res = s.wait(tk)
+        t = s.device_tensor(tk)
+        assert np.array_equal(t.cpu().numpy(), oracle_mod.decode(files[0]).pixels)
+        del t
+        s.release(tk)

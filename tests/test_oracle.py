@@ -44,6 +44,11 @@ def test_oracle_matches_reference_build(tmp_path, oracle_mod, seed, w, h, mode, 
         assert np.array_equal(px, d.pixels)
     else:
         assert px is None  # CPUonly rejects restart markers (decodeScanCPU.c:41-43)
+    # every file, restart markers included, against the reference's own parts:
+    # GPU-tree coefficients + CPUonly iDCT / upsampling / colour
+    assert np.array_equal(oracle_mod.ref_cpu_pixels(str(p), restart=True), d.pixels)
+    secs, px_count, fails = oracle_mod.ref_cpu_bench([str(p)], 2, 1)
+    assert fails == 0 and px_count == 2 * w * h
 
 
 def test_fp64_idct_within_one_of_integer(golden, oracle_mod):
