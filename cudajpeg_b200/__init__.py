@@ -55,6 +55,8 @@ EXPORTED = [
     "cjBatchSetTuning", "cjBatchGetTuning", "cjBatchAutotune", "cjDebugStepTable",
     "cjBatchCopyCoefficients", "cjBuildInfo", "cjBatchSetWaitLimit", "cjBatchSetOutput",
     "cjBatchGetOutput", "cjBatchChromaGeometry", "cjBatchDLPack", "cjServerDLPack", "cjDLPackFree",
+    "decodeScanCPU", "upsampleAndColourTransformHybrid", "upsampleAndColourTransformGPU",
+    "upsampleAndColourTransformCPU",
 ]
 
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",

@@ -177,3 +177,13 @@ extern "C" void iDCT_resample_colourTransform(JPGReader* jpg) {
   jpg->channels[0].pixels.size = (unsigned int)((size_t)jpg->width * jpg->height);
   jpg->channels[0].pixels.max_size = (unsigned int)d->h_pixels.cap;
 }
+
+// The reference's alternative final stages (include/pixelTransformGPU.h:18-20)
+// map onto the fused pixel stage: run it if the scan's pixels are pending.
+static void cj_pixel_stage_alias(JPGReader* jpg) {
+  if (jpg && jpg->dev && jpg->dev->scan_pending) iDCT_resample_colourTransform(jpg);
+}
+
+extern "C" void upsampleAndColourTransformHybrid(JPGReader* jpg) { cj_pixel_stage_alias(jpg); }
+extern "C" void upsampleAndColourTransformGPU(JPGReader* jpg) { cj_pixel_stage_alias(jpg); }
+extern "C" void upsampleAndColourTransformCPU(JPGReader* jpg) { cj_pixel_stage_alias(jpg); }

@@ -24,6 +24,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include "../../include/decodeScanCPU.h"
 #include "../../include/decodeScanGPU.h"
 #include "cj_internal.h"
 #include "cj_entropy.cuh"
@@ -644,3 +645,7 @@ extern "C" void decodeScanGPU(JPGReader* jpg) {
   jpg->scan_seen = 1;
   jpg->dev->scan_pending = 1;
 }
+
+// include/decodeScanCPU.h: the reference's host scan decoder's name
+// (src/decodeScanCPU.cu:98-152), decoding on the device like decodeScanGPU.
+extern "C" void decodeScanCPU(JPGReader* jpg) { decodeScanGPU(jpg); }

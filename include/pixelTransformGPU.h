@@ -20,6 +20,16 @@ extern "C" {
 
 void iDCT_resample_colourTransform(JPGReader *jpg);
 
+/* The reference's alternative final stages (include/pixelTransformGPU.h:18-20:
+ * upsampling + colour on the GPU, split between GPU and host, or on the
+ * host).  Here each is the same fused GPU pixel stage as
+ * iDCT_resample_colourTransform: it runs that stage if the last scan's
+ * pixels are still pending, and otherwise leaves the decoded image as it is.
+ * There is no host pixel path. */
+void upsampleAndColourTransformHybrid(JPGReader *jpg);
+void upsampleAndColourTransformGPU(JPGReader *jpg);
+void upsampleAndColourTransformCPU(JPGReader *jpg);
+
 /* Arithmetic forms of cjIDCTPlane */
 #define CJ_IDCT_INT 0   /* the reference's fixed-point iDCT: bit-exact */
 #define CJ_IDCT_F32 1   /* FP32 separable iDCT on CUDA cores */

@@ -2,6 +2,8 @@
 coefficients bit-exact with the reference's own decode, pixels bit-exact
 with the reference CPUonly decoder (or the oracle restatement of it for
 restart-marker files, which CPUonly cannot decode)."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -152,3 +154,22 @@ def test_device_code_runs_as_sm100(cj):
     """The device code the B200 runs is the library's own sm_100 binary (no
     PTX JIT of another target)."""
     assert cj.build_info()["binary_version"] == 100
+
+
+def test_reference_alias_entry_points(cj, oracle_mod):
+    """decodeScanCPU (include/decodeScanCPU.h:6) and the reference's
+    alternative pixel stages (include/pixelTransformGPU.h:18-20) are GPU
+    backed: a decode through the marker loop, then any of them, leaves the
+    same image as the oracle's."""
+    s = W.small_case(91, 300, 200, "420", 80, 0, "texture")
+    ref = oracle_mod.decode(s.data)
+    lib = cj.load()
+    with cj.Reader() as r:
+        r.open_bytes(s.data)
+        for name in ("upsampleAndColourTransformGPU", "upsampleAndColourTransformHybrid",
+                     "upsampleAndColourTransformCPU"):
+            getattr(lib, name).argtypes = [ctypes.c_void_p]
+            getattr(lib, name)(r.ptr)
+            assert cj._reader_fields(r.ptr)["error"] == 0
+            assert np.array_equal(r.pixels(), ref.pixels), name
+    assert hasattr(lib, "decodeScanCPU")
