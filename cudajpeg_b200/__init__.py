@@ -35,7 +35,7 @@ ERROR_NAMES = {0: "NO_ERROR", 1: "SYNTAX_ERROR", 2: "UNSUPPORTED_ERROR", 3: "OOM
 
 READER_HOST_COEFFICIENTS = 1
 IDCT_INT, IDCT_F32, IDCT_TC = 0, 1, 2
-OUTPUT_RGB, OUTPUT_PLANAR, OUTPUT_NV12 = 0, 1, 2
+OUTPUT_RGB, OUTPUT_PLANAR, OUTPUT_NV12, OUTPUT_RGB_FANCY = 0, 1, 2, 3
 
 # Every symbol the C headers in include/ declare (checked by the CPU tests).
 EXPORTED = [
@@ -618,7 +618,7 @@ class DLPackView:
 
 
 def _image_view(p: int, w: int, h: int, c: int, fmt: int, chroma, copy: bool):
-    if c != 3 or fmt == OUTPUT_RGB:
+    if c != 3 or fmt not in (OUTPUT_PLANAR, OUTPUT_NV12):
         n = w * h * c
         arr = np.frombuffer((C.c_uint8 * n).from_address(p), np.uint8)
         arr = arr.reshape((h, w, 3) if c == 3 else (h, w))

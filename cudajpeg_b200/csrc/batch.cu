@@ -79,7 +79,9 @@ struct CJImageDesc {
   int32_t ptile0, nptiles;   // pixel tiles
   int32_t T, sub_bits;       // MCUs per pixel tile; bits per subsequence
   int64_t coef0;             // first block in the coefficient buffer
-  int64_t out_off;           // output byte offset
+  int64_t out_off;           // output byte offset (fancy mode: of the planar samples)
+  int64_t rgb_off;           // fancy mode: byte offset of the RGB output
+  int64_t pix0;              // fancy mode: first pixel of the image in the batch's pixel order
 };
 
 #define BT_NPHASE 10
@@ -131,6 +133,8 @@ struct CJBatchArgs {
   CJWarpAgg* carry;
   int16_t* coef;
   uint8_t* out;
+  uint8_t* rgb;   // fancy mode: the RGB output (out then holds planar samples)
+  int64_t npix;   // fancy mode: pixels of the batch
   CJBatchCtl* ctl;
   int n, ntiles, nwarps, nptiles, max_passes;
   unsigned wait_limit;  // grid-barrier polls before a timeout (0 = default)
@@ -1024,7 +1028,46 @@ static cudaError_t bt_pixel_attrs() {
   return cudaSuccess;
 }
 
-// Output bytes of one image in a format.
+// Fancy mode, after the pixel kernel left each image's planar samples at
+// out + out_off: one thread per output pixel upsamples Cb and Cr with the
+// triangle filter (cj_fancy_at) and applies the reference's colour
+// transform (CPUonly/src/pixelTransformCPU.c:147-158) into rgb + rgb_off;
+// grey images are copied.
+__global__ void __launch_bounds__(256) k_fancy_rgb(CJBatchArgs a) {
+  if (__ldcg(&a.ctl->timeout)) return;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < a.npix;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = a.n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.desc[mid].pix0 <= p) lo = mid;
+      else hi = mid - 1;
+    }
+    const CJImageDesc& d = a.desc[lo];
+    const CJScanParams& prm = a.prm[lo];
+    const int W = prm.width, H = prm.height;
+    const int64_t k = p - d.pix0;
+    const uint8_t* pl = a.out + d.out_off;
+    if (prm.nch != 3) {
+      a.rgb[d.rgb_off + k] = pl[k];
+      continue;
+    }
+    const int y = (int)(k / W), x = (int)(k - (int64_t)y * W);
+    const int cw = (W * prm.comp_sx[1] + prm.hmax - 1) / prm.hmax;
+    const int ch = (H * prm.comp_sy[1] + prm.vmax - 1) / prm.vmax;
+    const uint8_t* cbp = pl + (int64_t)W * H;
+    const int cb = cj_fancy_at(cbp, cw, ch, prm.xshift, prm.yshift, x, y);
+    const int cr = cj_fancy_at(cbp + (int64_t)cw * ch, cw, ch, prm.xshift, prm.yshift, x, y);
+    const int yy = pl[k] << 8;
+    uint8_t* o = a.rgb + d.rgb_off + 3 * k;
+    o[0] = (uint8_t)cj_rgb_pack(yy, cb - 128, cr - 128, 0);
+    o[1] = (uint8_t)cj_rgb_pack(yy, cb - 128, cr - 128, 1);
+    o[2] = (uint8_t)cj_rgb_pack(yy, cb - 128, cr - 128, 2);
+  }
+}
+
+// Output bytes of one image in a format (fancy mode: its planar samples;
+// the RGB output is counted apart).
 static int64_t bt_out_bytes(const CJImageHeader& h, int out) {
   const int64_t y = (int64_t)h.width * h.height;
   if (h.nch != 3) return y;
@@ -1051,7 +1094,7 @@ struct CJBatch {
   JPGReader* parser = nullptr;  // host marker parse, one image at a time
   // device buffers (grow-only)
   CJDevBuf hdr, desc, prm, st, blob, data, tile_keep, tile_mark, mpos, mcode, segs, recs, ckpt, snap,
-      wagg, carry, coef, out, ctl;
+      wagg, carry, coef, out, ctl, fancy;  // fancy: planar samples of the fancy mode
   // pinned host staging
   CJHostBuf h_hdr, h_desc, h_out, h_st, h_ctl;
   // plan of the staged batch
@@ -1061,7 +1104,7 @@ struct CJBatch {
   std::vector<int> dims;       // width, height, channels, chroma width, chroma height per device slot
   std::vector<int64_t> outoff; // output offset per device slot
   int ntiles = 0, nwarps = 0, nptiles = 0;
-  int64_t blob_bytes = 0, out_total = 0, blocks = 0, scan_bytes = 0;
+  int64_t blob_bytes = 0, out_total = 0, blocks = 0, scan_bytes = 0, planar_total = 0, npix = 0;
   size_t smem = 0, smem_pix = 0;
   int grid = 0, grid_pix = 0;
   long long launches = 0;
@@ -1090,6 +1133,11 @@ static int bt_ensure(CJBatch* b, CJDevBuf& d, size_t bytes) {
   }
   d.cap = cap;
   return 0;
+}
+
+// The pixel kernel's output format (fancy mode: planar samples for k_fancy_rgb).
+static int bt_pix_format(const CJBatch* b) {
+  return b->out_format == CJ_OUT_RGB_FANCY ? CJ_OUT_PLANAR : b->out_format;
 }
 
 static int bt_init(CJBatch* b) {
@@ -1177,7 +1225,8 @@ void cjBatchDestroy(CJBatch* b) {
     cudaStreamSynchronize(b->stream);
     CJDevBuf* bufs[] = {&b->hdr,  &b->desc, &b->prm,   &b->st,   &b->blob,  &b->data,
                         &b->tile_keep, &b->tile_mark, &b->mpos, &b->mcode, &b->segs,
-                        &b->recs, &b->ckpt, &b->snap, &b->wagg, &b->carry, &b->coef, &b->out, &b->ctl};
+                        &b->recs, &b->ckpt, &b->snap, &b->wagg, &b->carry, &b->coef, &b->out, &b->ctl,
+                        &b->fancy};
     for (CJDevBuf* d : bufs)
       if (d->p) cudaFree(d->p);
     CJHostBuf* hb[] = {&b->h_hdr, &b->h_desc, &b->h_out, &b->h_st, &b->h_ctl};
@@ -1213,7 +1262,8 @@ int cjBatchSetTuning(CJBatch* b, int sub_bits, int decode_ctas_per_sm, int pixel
 
 int cjBatchSetOutput(CJBatch* b, int format, int idct) {
   if (!b) return PROGRAMMER_ERROR;
-  if (format != CJ_OUT_RGB && format != CJ_OUT_PLANAR && format != CJ_OUT_NV12) return PROGRAMMER_ERROR;
+  if (format != CJ_OUT_RGB && format != CJ_OUT_PLANAR && format != CJ_OUT_NV12 && format != CJ_OUT_RGB_FANCY)
+    return PROGRAMMER_ERROR;
   if (idct != CJ_PIX_IDCT_INT && idct != CJ_PIX_IDCT_TC) return PROGRAMMER_ERROR;
   b->out_format = format;
   b->idct = idct;
@@ -1257,7 +1307,10 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   CJImageHeader* hh = (CJImageHeader*)b->h_hdr.p;
   CJImageDesc* dd = (CJImageDesc*)b->h_desc.p;
   int nd = 0, ntiles = 0, nsubw = 0, nptiles = 0, nmark = 0, nseg = 0;
-  int64_t data_bytes = 0, blocks = 0, out_total = 0;
+  int64_t data_bytes = 0, blocks = 0, out_total = 0, planar_total = 0, npix = 0;
+  const bool fancy = b->out_format == CJ_OUT_RGB_FANCY;
+  // the pixel kernel's format: fancy mode writes planar samples for k_fancy_rgb
+  const int pix_format = fancy ? CJ_OUT_PLANAR : b->out_format;
   size_t smem = 0;
   for (int i = 0; i < n; i++) {
     int64_t so = 0, sl = 0;
@@ -1298,9 +1351,18 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
     nptiles += d.nptiles;
     d.coef0 = blocks;
     blocks += h.total_blocks;
-    d.out_off = out_total;
     int ch = h.nch == 3 ? 3 : 1;
-    out_total += (bt_out_bytes(h, b->out_format) + 15) & ~(int64_t)15;  // 16-byte aligned starts
+    if (fancy) {
+      d.out_off = planar_total;
+      planar_total += (bt_out_bytes(h, CJ_OUT_PLANAR) + 15) & ~(int64_t)15;
+      d.rgb_off = out_total;
+      out_total += ((int64_t)h.width * h.height * ch + 15) & ~(int64_t)15;
+      d.pix0 = npix;
+      npix += (int64_t)h.width * h.height;
+    } else {
+      d.out_off = out_total;
+      out_total += (bt_out_bytes(h, pix_format) + 15) & ~(int64_t)15;  // 16-byte aligned starts
+    }
     CJPixGeom g;
     g.nch = h.nch;
     g.bpm = bpm;
@@ -1314,7 +1376,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
     b->dims.push_back(ch);
     b->dims.push_back(h.nch == 3 ? (h.width * h.comp_sx[1] + h.hmax - 1) / h.hmax : 0);
     b->dims.push_back(h.nch == 3 ? (h.height * h.comp_sy[1] + h.vmax - 1) / h.vmax : 0);
-    b->outoff.push_back(d.out_off);
+    b->outoff.push_back(fancy ? d.rgb_off : d.out_off);
     nd++;
   }
   b->n_dev = nd;
@@ -1323,6 +1385,8 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   b->nptiles = nptiles;
   b->blob_bytes = blob_bytes;
   b->out_total = out_total;
+  b->planar_total = planar_total;
+  b->npix = npix;
   b->blocks = blocks;
   b->scan_bytes = data_bytes;
   b->smem = BT_DECODE_SMEM;
@@ -1341,6 +1405,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
       bt_ensure(b, b->wagg, (size_t)nsubw * sizeof(CJWarpAgg)) ||
       bt_ensure(b, b->carry, (size_t)nsubw * sizeof(CJWarpAgg)) ||
       bt_ensure(b, b->coef, (size_t)blocks * 128 + 128) || bt_ensure(b, b->out, (size_t)out_total + 64) ||
+      (fancy && bt_ensure(b, b->fancy, (size_t)planar_total + 64)) ||
       bt_ensure(b, b->ctl, sizeof(CJBatchCtl)))
     return CUDA_MEM_ERROR;
   if (cj_host_ensure(b->h_st, nd_ * sizeof(CJStatus)) || cj_host_ensure(b->h_ctl, sizeof(CJBatchCtl)))
@@ -1359,7 +1424,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   if (per_sm < 1) return UNSUPPORTED_ERROR;
   b->grid = std::min(per_sm, b->decode_ctas) * b->sm_count;
   CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                  &per_sm, (const void*)bt_pixel_kernel(b->idct, b->out_format), CJ_PIX_THREADS, b->smem_pix),
+                  &per_sm, (const void*)bt_pixel_kernel(b->idct, bt_pix_format(b)), CJ_PIX_THREADS, b->smem_pix),
               CUDA_KERNEL_LAUNCH_ERROR);
   if (per_sm < 1) return UNSUPPORTED_ERROR;
   b->grid_pix = std::min(nptiles, per_sm * b->sm_count);
@@ -1386,7 +1451,10 @@ static CJBatchArgs bt_args(const CJBatch* b) {
   a.wagg = (CJWarpAgg*)b->wagg.p;
   a.carry = (CJWarpAgg*)b->carry.p;
   a.coef = (int16_t*)b->coef.p;
-  a.out = (uint8_t*)b->out.p;
+  const bool fancy = b->out_format == CJ_OUT_RGB_FANCY;
+  a.out = (uint8_t*)(fancy ? b->fancy.p : b->out.p);
+  a.rgb = fancy ? (uint8_t*)b->out.p : nullptr;
+  a.npix = fancy ? b->npix : 0;
   a.ctl = (CJBatchCtl*)b->ctl.p;
   a.n = b->n_dev;
   a.ntiles = b->ntiles;
@@ -1444,11 +1512,20 @@ static bool bt_build_graph(CJBatch* b) {
   }
   if (ok && b->grid_pix > 0) {
     cudaKernelNodeParams pp = kp;
-    pp.func = (void*)bt_pixel_kernel(b->idct, b->out_format);
+    pp.func = (void*)bt_pixel_kernel(b->idct, bt_pix_format(b));
     pp.gridDim = dim3(b->grid_pix);
     pp.blockDim = dim3(CJ_PIX_THREADS);
     pp.sharedMemBytes = (unsigned)b->smem_pix;
     ok = cudaGraphAddKernelNode(&n_pix, g, &n_dec, 1, &pp) == cudaSuccess;
+  }
+  if (ok && n_pix && b->out_format == CJ_OUT_RGB_FANCY && b->npix > 0) {
+    cudaGraphNode_t n_fancy = nullptr;
+    cudaKernelNodeParams fp = kp;
+    fp.func = (void*)k_fancy_rgb;
+    fp.gridDim = dim3(b->sm_count * 8);
+    fp.blockDim = dim3(256);
+    fp.sharedMemBytes = 0;
+    ok = cudaGraphAddKernelNode(&n_fancy, g, &n_pix, 1, &fp) == cudaSuccess;
   }
   if (ok && b->gexec) {
     // same topology as the instantiated graph: update its nodes in place
@@ -1480,7 +1557,7 @@ int cjBatchRun(CJBatch* b) {
     CJ_CUDA_TRY(cudaEventRecord(b->ev0, s), CUDA_KERNEL_LAUNCH_ERROR);
     CJ_CUDA_TRY(cudaGraphLaunch(b->gexec, s), CUDA_KERNEL_LAUNCH_ERROR);
     CJ_CUDA_TRY(cudaEventRecord(b->ev1, s), CUDA_KERNEL_LAUNCH_ERROR);
-    b->launches += b->grid_pix > 0 ? 2 : 1;
+    b->launches += (b->grid_pix > 0 ? 2 : 1) + (b->out_format == CJ_OUT_RGB_FANCY && b->grid_pix > 0 && b->npix > 0);
     b->graph_launches++;
     return 0;
   }
@@ -1493,9 +1570,14 @@ int cjBatchRun(CJBatch* b) {
               CUDA_KERNEL_LAUNCH_ERROR);
   b->launches++;
   if (b->grid_pix > 0) {
-    bt_pixel_kernel(b->idct, b->out_format)<<<b->grid_pix, CJ_PIX_THREADS, b->smem_pix, s>>>(a);
+    bt_pixel_kernel(b->idct, bt_pix_format(b))<<<b->grid_pix, CJ_PIX_THREADS, b->smem_pix, s>>>(a);
     CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
     b->launches++;
+    if (b->out_format == CJ_OUT_RGB_FANCY && b->npix > 0) {
+      k_fancy_rgb<<<b->sm_count * 8, 256, 0, s>>>(a);
+      CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
+      b->launches++;
+    }
   }
   CJ_CUDA_TRY(cudaEventRecord(b->ev1, s), CUDA_KERNEL_LAUNCH_ERROR);
   return 0;
@@ -1582,7 +1664,7 @@ DLManagedTensor* cjBatchDLPack(CJBatch* b, int i) {
   const int k = b->dev_of[i];
   const int64_t w = b->dims[5 * k], h = b->dims[5 * k + 1], c = b->dims[5 * k + 2];
   void* p = (unsigned char*)b->out.p + b->outoff[k];
-  if (c == 3 && b->out_format != CJ_OUT_RGB) {
+  if (c == 3 && (b->out_format == CJ_OUT_PLANAR || b->out_format == CJ_OUT_NV12)) {
     const int64_t n[1] = {w * h + 2 * (int64_t)b->dims[5 * k + 3] * b->dims[5 * k + 4]};
     return cj_dl_view(p, b->device, 1, n);
   }

@@ -19,6 +19,7 @@
 #define CJ_OUT_RGB 0     // interleaved RGB (grey: one plane), the reference's output
 #define CJ_OUT_PLANAR 1  // Y plane, then Cb and Cr planes at chroma resolution
 #define CJ_OUT_NV12 2    // Y plane, then Cb/Cr interleaved at chroma resolution
+#define CJ_OUT_RGB_FANCY 3  // interleaved RGB with fancy (triangle) chroma upsampling
 
 // ---------------------------------------------------------------- TMA helpers
 __device__ __forceinline__ uint32_t cj_smem_addr(const void* p) {
@@ -508,4 +509,30 @@ __device__ __forceinline__ bool cj_pixel_compute(uint8_t* __restrict__ out, CJSt
                                                  int mrow, int mc0, const int16_t* sc, uint8_t* smem,
                                                  uint64_t* barp, uint32_t parity, CJPixSmemParams* Pp) {
   return cj_pixel_tile<CJ_PIX_IDCT_INT, CJ_OUT_RGB>(out, st, g, mrow, mc0, sc, smem, barp, parity, Pp, nullptr);
+}
+
+// Fancy (triangle) upsampling of a cw x ch chroma plane by 2^xs x 2^ys: the
+// sample at output (x, y), as the IJG decoder's h2v1 / h1v2 / h2v2 fancy
+// upsamplers give it (weights 3/4 and 1/4 toward the nearer and the farther
+// sample, alternating rounding biases, edge samples alone at the first and
+// last column, the first and last rows repeated above and below); other
+// factors replicate.  An optional output mode: the reference upsamples by
+// nearest replication (CPUonly/src/pixelTransformCPU.c:110-127).
+__device__ __forceinline__ int cj_fancy_at(const uint8_t* __restrict__ pl, int cw, int ch, int xs, int ys, int x,
+                                           int y) {
+  const int r = min(y >> ys, ch - 1), i = min(x >> xs, cw - 1);
+  const bool fancy = (xs == 1 && ys <= 1) || (xs == 0 && ys == 1);
+  const uint8_t* row = pl + (int64_t)r * cw;
+  if (!fancy) return row[i];
+  int nb = r;
+  if (ys == 1) nb = (y & 1) ? min(r + 1, ch - 1) : max(r - 1, 0);
+  const uint8_t* nrow = pl + (int64_t)nb * cw;
+  if (xs == 0) return (3 * row[i] + nrow[i] + ((y & 1) ? 2 : 1)) >> 2;
+  if (ys == 0) {
+    if (x & 1) return i == cw - 1 ? row[i] : (3 * row[i] + row[i + 1] + 2) >> 2;
+    return i == 0 ? row[i] : (3 * row[i] + row[i - 1] + 1) >> 2;
+  }
+  const int cs = 3 * row[i] + nrow[i];
+  if (x & 1) return i == cw - 1 ? (4 * cs + 7) >> 4 : (3 * cs + 3 * row[i + 1] + nrow[i + 1] + 7) >> 4;
+  return i == 0 ? (4 * cs + 8) >> 4 : (3 * cs + 3 * row[i - 1] + nrow[i - 1] + 8) >> 4;
 }

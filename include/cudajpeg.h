@@ -126,8 +126,12 @@ void cjBatchGetTuning(const CJBatch *b, int *sub_bits, int *decode_ctas_per_sm, 
  * chroma resolution cw*ch, cw = ceil(width * Hc / Hmax), ch = ceil(height *
  * Vc / Vmax), the reference's channel sizes, src/format.cu:242-354; no
  * upsampling, no colour transform) or CJ_OUTPUT_NV12 (the Y plane, then Cb
- * and Cr interleaved at chroma resolution).  Grey images have the Y plane
- * only in every format.  idct: CJ_IDCT_INT (default: the reference's fixed
+ * and Cr interleaved at chroma resolution) or CJ_OUTPUT_RGB_FANCY (interleaved
+ * RGB like CJ_OUTPUT_RGB, but chroma upsampled by the IJG decoder's "fancy"
+ * triangle filter -- weights 3/4 and 1/4 toward the nearer and the farther
+ * chroma sample, for factor-2 directions -- instead of the reference's
+ * nearest replication; the colour transform is the reference's).  Grey
+ * images have the Y plane only in every format.  idct: CJ_IDCT_INT (default: the reference's fixed
  * point, src/pixelTransformGPU.cu:25-142, bit-exact) or CJ_IDCT_TC (FP16
  * hi/lo basis on tensor cores, FP32 accumulation: within 0.5 of an exact
  * iDCT before rounding, samples within +-1 of CJ_IDCT_INT).  Returns
@@ -135,6 +139,7 @@ void cjBatchGetTuning(const CJBatch *b, int *sub_bits, int *decode_ctas_per_sm, 
 #define CJ_OUTPUT_RGB 0
 #define CJ_OUTPUT_PLANAR 1
 #define CJ_OUTPUT_NV12 2
+#define CJ_OUTPUT_RGB_FANCY 3
 int cjBatchSetOutput(CJBatch *b, int format, int idct);
 void cjBatchGetOutput(const CJBatch *b, int *format, int *idct);
 /* Bound on each grid-barrier wait of the decode kernel, in polls of about

@@ -578,3 +578,77 @@ void oracle_idct_f64(const int32_t *coef, int64_t n, double *out) {
       }
   }
 }
+
+/* ---------------- fancy (triangle) chroma upsampling ----------------
+ *
+ * Not part of the reference path (its upsampling is nearest replication,
+ * CPUonly/src/pixelTransformCPU.c:110-127); this restates the published IJG
+ * decoder's "fancy" upsampling (libjpeg jdsample.c: h2v1, h1v2 and h2v2
+ * fancy upsamplers) as the checker of the decoder's optional fancy mode.
+ * A factor-2 direction interpolates with weights 3/4 and 1/4 between the
+ * nearer and the farther sample; each output pair alternates its rounding
+ * bias (h2v1 / h1v2: +1 then +2, >> 2; h2v2: +8 then +7, >> 4 after the
+ * vertical 3:1 column sums); the first and last column of a row use the
+ * edge sample alone (h2v2: 4 x the column sum), the rows above the first
+ * and below the last repeat them.  Other factors replicate (IJG
+ * int_upsample).  `in` is a cw x ch plane (stride in_stride); `out` gets the
+ * ow x oh upsampled plane (cropped from 2cw x 2ch).  A one-sample-wide
+ * plane uses its sample for both neighbours. */
+void oracle_fancy_upsample(const uint8_t *in, int cw, int ch, int in_stride, int xs, int ys,
+                           uint8_t *out, int ow, int oh) {
+  const int fancy = (xs == 1 && ys <= 1) || (xs == 0 && ys == 1);
+  for (int y = 0; y < oh; y++) {
+    const int r = y >> ys;
+    const uint8_t *row = in + (size_t)(r < ch ? r : ch - 1) * in_stride;
+    int nb = r;
+    if (fancy && ys == 1) nb = (y & 1) ? (r + 1 < ch ? r + 1 : ch - 1) : (r > 0 ? r - 1 : 0);
+    const uint8_t *nrow = in + (size_t)(nb < ch ? nb : ch - 1) * in_stride;
+    for (int x = 0; x < ow; x++) {
+      const int i = x >> xs;
+      int v;
+      if (!fancy) {
+        v = row[i < cw ? i : cw - 1];
+      } else if (xs == 0) { /* h1v2 */
+        v = (3 * row[i] + nrow[i] + ((y & 1) ? 2 : 1)) >> 2;
+      } else if (ys == 0) { /* h2v1 */
+        if (x & 1) v = (i == cw - 1) ? row[i] : (3 * row[i] + row[i + 1] + 2) >> 2;
+        else v = (i == 0) ? row[i] : (3 * row[i] + row[i - 1] + 1) >> 2;
+      } else { /* h2v2 */
+        const int cs = 3 * row[i] + nrow[i];
+        if (x & 1) v = (i == cw - 1) ? (4 * cs + 7) >> 4 : (3 * cs + 3 * row[i + 1] + nrow[i + 1] + 7) >> 4;
+        else v = (i == 0) ? (4 * cs + 8) >> 4 : (3 * cs + 3 * row[i - 1] + nrow[i - 1] + 8) >> 4;
+      }
+      out[(size_t)y * ow + x] = (uint8_t)v;
+    }
+  }
+}
+
+/* The decoded image with fancy chroma upsampling: upsampled Y, Cb, Cr
+ * interleaved (ycc, may be NULL) and RGB through the reference's colour
+ * transform (CPUonly/src/pixelTransformCPU.c:147-158; rgb, may be NULL).
+ * Colour images only. */
+void oracle_fancy(const OracleImage *im, uint8_t *ycc, uint8_t *rgb) {
+  const int W = im->width, H = im->height;
+  int xs = 0, ys = 0;
+  while ((im->comp[1].width << xs) < W) xs++;
+  while ((im->comp[1].height << ys) < H) ys++;
+  uint8_t *cb = (uint8_t *)malloc((size_t)W * H), *cr = (uint8_t *)malloc((size_t)W * H);
+  if (!cb || !cr) { free(cb); free(cr); return; }
+  oracle_fancy_upsample(im->comp[1].plane, im->comp[1].width, im->comp[1].height, im->comp[1].stride, xs, ys, cb, W, H);
+  oracle_fancy_upsample(im->comp[2].plane, im->comp[2].width, im->comp[2].height, im->comp[2].stride, xs, ys, cr, W, H);
+  const OracleComp *Y = &im->comp[0];
+  for (int y = 0; y < H; y++)
+    for (int x = 0; x < W; x++) {
+      const size_t k = (size_t)y * W + x;
+      const int yv = Y->plane[(size_t)y * Y->stride + x];
+      if (ycc) { ycc[3 * k] = (uint8_t)yv; ycc[3 * k + 1] = cb[k]; ycc[3 * k + 2] = cr[k]; }
+      if (rgb) {
+        const int yy = yv << 8, b = cb[k] - 128, r = cr[k] - 128;
+        rgb[3 * k] = clip8((yy + 359 * r + 128) >> 8);
+        rgb[3 * k + 1] = clip8((yy - 88 * b - 183 * r + 128) >> 8);
+        rgb[3 * k + 2] = clip8((yy + 454 * b + 128) >> 8);
+      }
+    }
+  free(cb);
+  free(cr);
+}

@@ -56,6 +56,9 @@ def _load():
         lib.oracle_dq.argtypes = [C.c_void_p, C.c_void_p]
         lib.oracle_idct_blocks.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
         lib.oracle_idct_f64.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        lib.oracle_fancy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.oracle_fancy_upsample.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                              C.c_void_p, C.c_int, C.c_int]
         _lib = lib
     return _lib
 
@@ -86,10 +89,14 @@ class Decoded:
     planes: list = field(default_factory=list)  # uint8 [rows, stride] per component
     pixels: np.ndarray | None = None            # uint8 [H, W, 3] or [H, W]
     dq: np.ndarray | None = None                # uint8 [4, 64] zig-zag order
+    fancy_ycc: np.ndarray | None = None         # uint8 [H, W, 3], fancy=True only
+    fancy_rgb: np.ndarray | None = None         # uint8 [H, W, 3], fancy=True only
 
 
-def decode(data: bytes) -> Decoded:
-    """Decode a JPEG held in memory with the C restatement."""
+def decode(data: bytes, fancy: bool = False) -> Decoded:
+    """Decode a JPEG held in memory with the C restatement.  fancy=True also
+    gives colour images with fancy (triangle) chroma upsampling: upsampled
+    YCbCr and RGB through the reference's colour transform."""
     lib = _load()
     err = C.c_int(0)
     h = lib.oracle_decode(data, len(data), C.byref(err))
@@ -114,10 +121,24 @@ def decode(data: bytes) -> Decoded:
         lib.oracle_pixels(h, out.pixels.ctypes.data)
         out.dq = np.empty((4, 64), np.uint8)
         lib.oracle_dq(h, out.dq.ctypes.data)
+        if fancy and out.nch == 3:
+            out.fancy_ycc = np.empty((out.height, out.width, 3), np.uint8)
+            out.fancy_rgb = np.empty((out.height, out.width, 3), np.uint8)
+            lib.oracle_fancy(h, out.fancy_ycc.ctypes.data, out.fancy_rgb.ctypes.data)
         return out
     finally:
         if h:
             lib.oracle_free(h)
+
+
+def fancy_upsample(plane: np.ndarray, xs: int, ys: int, ow: int, oh: int) -> np.ndarray:
+    """Fancy (triangle) upsampling of a 2-D uint8 plane by 2^xs x 2^ys,
+    cropped to oh x ow (oracle_fancy_upsample)."""
+    lib = _load()
+    p = np.ascontiguousarray(plane, np.uint8)
+    out = np.empty((oh, ow), np.uint8)
+    lib.oracle_fancy_upsample(p.ctypes.data, p.shape[1], p.shape[0], p.shape[1], xs, ys, out.ctypes.data, ow, oh)
+    return out
 
 
 def idct_int(coefs: np.ndarray) -> np.ndarray:

@@ -138,3 +138,21 @@ def test_device_tensors_through_dlpack(cj, oracle_mod, files):
         assert np.array_equal(t.cpu().numpy(), oracle_mod.decode(files[0]).pixels)
         del t
         s.release(tk)
+
+
+def test_fancy_upsampling_equals_oracle(cj, oracle_mod, files):
+    """CJ_OUTPUT_RGB_FANCY: the triangle-filter chroma upsampling (the
+    oracle's restatement, pinned to libjpeg by tests/test_oracle.py) with the
+    reference's iDCT and colour transform, bit-exact for every image; grey
+    images are their plane."""
+    rgb, errs = decode_forms(cj, files, cj.OUTPUT_RGB_FANCY, cj.IDCT_INT)
+    fancy_differs = 0
+    for k, data in enumerate(files):
+        ref = oracle_mod.decode(data, fancy=True)
+        assert errs[k] == ref.error, k
+        if ref.error:
+            continue
+        want = ref.fancy_rgb if ref.nch == 3 else ref.pixels
+        assert np.array_equal(rgb[k], want), k
+        fancy_differs += int(not np.array_equal(want, ref.pixels))
+    assert fancy_differs >= 10

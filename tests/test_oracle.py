@@ -69,3 +69,27 @@ def test_workloads_are_seeded():
     batch = W.mixed_batch(n=24, seed=9, max_side=256)
     assert len(batch) == 24
     assert all(s.width % 8 == 0 and s.height % 8 == 0 for s in batch)
+
+
+@pytest.mark.parametrize("mode,h,w", [("420", 64, 96), ("422", 48, 80), ("420", 40, 104), ("422", 24, 136)])
+def test_fancy_upsampling_matches_libjpeg(oracle_mod, mode, h, w):
+    """The oracle's fancy upsampler against Pillow's libjpeg decoding to
+    YCbCr, on images whose blocks are all DC-only (content constant over
+    each chroma block's footprint): there both decoders' iDCTs give
+    round(DC / 8) + 128, so only the upsampling can differ."""
+    import io
+
+    from PIL import Image
+    rng = np.random.default_rng(len(mode) + h + w)
+    tile = (16, 16) if mode == "420" else (8, 16)
+    t = rng.integers(30, 226, (h // tile[0], w // tile[1], 3)).astype(np.uint8)
+    arr = np.kron(t, np.ones(tile + (1,), np.uint8))
+    data = W.encode(arr, mode, 92)
+    d = oracle_mod.decode(data, fancy=True)
+    assert d.error == 0
+    im = Image.open(io.BytesIO(data))
+    im.draft("YCbCr", im.size)
+    want = np.asarray(im)
+    assert im.mode == "YCbCr" and want.shape == d.fancy_ycc.shape
+    assert np.array_equal(d.fancy_ycc[..., 0], want[..., 0])  # luma: the DC-only iDCTs agree
+    assert np.array_equal(d.fancy_ycc, want)
