@@ -58,17 +58,14 @@ sys.path.insert(0, ROOT)
 METRIC = "decoded MPix/s"
 FLUSH_BYTES = 256 << 20
 
-# Algorithmic bytes of each kernel, per launch, as a function of the image:
-# B = entropy-coded bytes, Bd = destuffed bytes, n = 8x8 blocks, P = output bytes.
+# Minimum bytes of each kernel of the single-image path, per launch, as a
+# function of the image: B = entropy-coded bytes, Bd = destuffed bytes,
+# n = 8x8 blocks, P = output bytes.  k_decode_batch reads the compressed
+# scan, writes the destuffed copy, reads it twice (speculative sync and
+# write-out) and writes the int16 blocks; k_pixel reads the blocks and
+# writes the image.
 KERNEL_BYTES = {
-    "k_destuff_count": lambda g: g["B"],
-    "k_scan_tiles": lambda g: 0,
-    "k_destuff_scatter": lambda g: g["B"] + g["Bd"],
-    "k_build_segments": lambda g: 0,
-    "k_sync_intra": lambda g: g["Bd"],
-    "k_sync_inter": lambda g: g["Bd"],
-    "k_scan_warps": lambda g: 0,
-    "k_decode_write": lambda g: g["Bd"] + 128 * g["n"],
+    "k_decode_batch": lambda g: g["B"] + 3 * g["Bd"] + 128 * g["n"],
     "k_pixel": lambda g: 128 * g["n"] + g["P"],
 }
 

@@ -62,8 +62,7 @@ EXPORTED = [
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
                 "fixup", "warp_scan", "write", "pixel", "launch"]
 
-KERNEL_NAMES = ["k_destuff_count", "k_scan_tiles", "k_destuff_scatter", "k_build_segments",
-                "k_sync_intra", "k_sync_inter", "k_scan_warps", "k_decode_write", "k_pixel"]
+KERNEL_NAMES = ["k_decode_batch", "k_pixel", "k_prog_scan"]
 
 
 class DecodeError(RuntimeError):

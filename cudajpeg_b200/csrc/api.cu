@@ -24,7 +24,7 @@ void cjReaderInfo(const JPGReader* r, int64_t* info) {
   info[8] = st ? st->destuffed : 0;
   info[9] = st ? st->nmarkers : 0;
   info[10] = d ? (int64_t)d->raw_len : 0;
-  info[11] = (int64_t)sizeof(CJScanParams);
+  info[11] = d ? (int64_t)d->param_bytes : 0;
 }
 
 const unsigned char* cjReaderPixels(const JPGReader* r) { return r->pixels; }
@@ -60,8 +60,9 @@ void* cjReaderStream(const JPGReader* r) { return (void*)r->dev->stream; }
 
 int cjReaderRedecodeDevice(JPGReader* r) {
   CJReaderDevice* d = r->dev;
-  if (!d->gpu_ready || !d->raw.p || !d->total_blocks) return PROGRAMMER_ERROR;
-  int err = cj_scan_device(r);
+  // (baseline frames: a progressive frame's scans are not kept for a re-run)
+  if (!d->gpu_ready || !d->raw.p || !d->total_blocks || !d->b_grid || d->progressive) return PROGRAMMER_ERROR;
+  int err = cj_reader_decode(r, false);
   if (!err) err = cj_pixel_launch(r, false);
   return err;
 }
@@ -73,17 +74,8 @@ int cjReaderSync(JPGReader* r) {
                               d->stream),
               CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaStreamSynchronize(d->stream), CUDA_KERNEL_LAUNCH_ERROR);
-  const CJStatus* st = (const CJStatus*)d->h_status.p;
-  if (st->unstable) {
-    int err = cj_scan_resync(r);
-    if (!err) err = cj_pixel_launch(r, false);
-    if (err) return err;
-    CJ_CUDA_TRY(cudaMemcpyAsync(d->h_status.p, d->status.p, sizeof(CJStatus),
-                                cudaMemcpyDeviceToHost, d->stream),
-                CUDA_MEM_ERROR);
-    CJ_CUDA_TRY(cudaStreamSynchronize(d->stream), CUDA_KERNEL_LAUNCH_ERROR);
-  }
-  return cj_status_error(st);
+  int err = cj_reader_decode_status(r);
+  return err ? err : cj_status_error((const CJStatus*)d->h_status.p);
 }
 
 const unsigned char* cjReaderDevicePixels(const JPGReader* r) {

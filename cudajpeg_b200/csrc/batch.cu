@@ -1165,20 +1165,17 @@ static int bt_init(CJBatch* b) {
   return 0;
 }
 
-// Host parse of one file up to its scan; fills the device header.
-static int bt_parse(CJBatch* b, const unsigned char* data, size_t size, CJImageHeader* h,
-                    int64_t* scan_off, int64_t* scan_len) {
-  JPGReader* r = b->parser;
-  r->huff_defined = 0;  // images of a batch are independent
-  int e = cj_parse_to_scan(r, data, size);
-  if (e) return e;
+// The device header of a reader parsed up to its scan (tables as parsed,
+// geometry); UNSUPPORTED_ERROR for a geometry the pixel tiles do not cover
+// (cj_pix_check).
+static int bt_fill_header(const JPGReader* r, CJImageHeader* h) {
   memset(h, 0, sizeof(*h));
   for (int s = 0; s < 4; s++) {
     memcpy(h->counts[s], r->dev->huff[s].counts, 16);
     memcpy(h->symbols[s], r->dev->huff[s].symbols, 256);
   }
   h->huff_mask = (uint8_t)r->huff_defined;
-  memcpy(h->dq, r->dq_tables, sizeof(h->dq));
+  memcpy(h->dq, r->dev->dq16, sizeof(h->dq));
   h->nch = r->num_channels;
   for (int c = 0; c < r->num_channels; c++) {
     h->comp_dc[c] = (uint8_t)r->channels[c].dc_id;
@@ -1210,9 +1207,37 @@ static int bt_parse(CJBatch* b, const unsigned char* data, size_t size, CJImageH
   if (h->comp_sx[0] != h->hmax || h->comp_sy[0] != h->vmax) return UNSUPPORTED_ERROR;
   if (h->nch == 3 && ((h->comp_sx[1] << xs) != h->hmax || (h->comp_sy[1] << ys) != h->vmax))
     return UNSUPPORTED_ERROR;
+  return 0;
+}
+
+// Host parse of one file up to its scan; fills the device header.
+static int bt_parse(CJBatch* b, const unsigned char* data, size_t size, CJImageHeader* h,
+                    int64_t* scan_off, int64_t* scan_len) {
+  JPGReader* r = b->parser;
+  r->huff_defined = 0;  // images of a batch are independent
+  int e = cj_parse_to_scan(r, data, size);
+  if (e) return e;
+  e = bt_fill_header(r, h);
+  if (e) return e;
   *scan_off = (int64_t)(r->pos - data);
   *scan_len = (int64_t)(r->end - r->pos);
   return 0;
+}
+
+// The plan of one image alone at the start of every buffer: destuff tiles,
+// markers, segments, subsequences of `sub_bits`, pixel tiles.
+static void bt_plan_one(const CJImageHeader& h, int64_t scan_len, int sub_bits, CJImageDesc* d) {
+  memset(d, 0, sizeof(*d));
+  int bpm = 0;
+  for (int c = 0; c < h.nch; c++) bpm += h.comp_sx[c] * h.comp_sy[c];
+  d->raw_len = scan_len;
+  d->ntiles = (int)std::max<int64_t>(1, (scan_len + BT_TILE_BYTES - 1) / BT_TILE_BYTES);
+  d->mark_cap = h.nseg_expected + 1;
+  d->seg_cap = h.nseg_expected;
+  d->sub_bits = sub_bits;
+  d->sub_cap = ((int)((scan_len * 8 + sub_bits - 1) / sub_bits) + h.nseg_expected + 1 + 31) & ~31;
+  d->T = cj_pix_tile_mcus(h.hmax, bpm);
+  d->nptiles = h.mcuy * ((h.mcux + d->T - 1) / d->T);
 }
 
 extern "C" {
@@ -1792,6 +1817,114 @@ int cjBatchAutotune(CJBatch* b, int n, const unsigned char* blob, const int64_t*
 
 }  // extern "C"
 
+// ---------------------------------------------------------------- the drop-in reader
+
+// decodeScanGPU's device decode (and cjReaderRedecodeDevice's): the batch
+// decode kernel on the reader's one image, in the reader's grow-only
+// buffers -- one cooperative launch, Huffman tables built on the device,
+// fix-up passes looped on the device.  The grid is the co-resident maximum,
+// cut to the image's work (destuff tiles, warp groups) for small images so
+// that idle CTAs do not lengthen the grid barriers.
+int cj_reader_decode(JPGReader* jpg, bool stage) {
+  CJReaderDevice* d = jpg->dev;
+  cudaStream_t s = d->stream;
+  if (stage) {
+    CJImageHeader h;
+    int e = bt_fill_header(jpg, &h);
+    if (e) return e;
+    const int64_t n = (int64_t)(jpg->end - jpg->pos);
+    CJImageDesc desc;
+    bt_plan_one(h, n, d->sub_bits, &desc);
+    const int nwarps = desc.sub_cap / 32;
+    if (cj_dev_ensure(d->bhdr, sizeof(CJImageHeader)) || cj_dev_ensure(d->bdesc, sizeof(CJImageDesc)) ||
+        cj_dev_ensure(d->params, sizeof(CJScanParams)) || cj_dev_ensure(d->status, sizeof(CJStatus)) ||
+        cj_dev_ensure(d->raw, (size_t)n + 64) || cj_dev_ensure(d->data, (size_t)n + 64) ||
+        cj_dev_ensure(d->tile_keep, (size_t)desc.ntiles * 4) || cj_dev_ensure(d->tile_mark, (size_t)desc.ntiles * 4) ||
+        cj_dev_ensure(d->mpos, (size_t)desc.mark_cap * 4) || cj_dev_ensure(d->mcode, (size_t)desc.mark_cap) ||
+        cj_dev_ensure(d->segs, (size_t)desc.seg_cap * sizeof(CJSegment)) ||
+        cj_dev_ensure(d->recs, (size_t)desc.sub_cap * sizeof(CJSubRec)) ||
+        cj_dev_ensure(d->ckpt, (size_t)desc.sub_cap * CJ_CKPTS * sizeof(CJCkpt)) ||
+        cj_dev_ensure(d->snap, (size_t)2 * nwarps * sizeof(uint64_t)) ||
+        cj_dev_ensure(d->wagg, (size_t)nwarps * sizeof(CJWarpAgg)) ||
+        cj_dev_ensure(d->carry, (size_t)nwarps * sizeof(CJWarpAgg)) ||
+        cj_dev_ensure(d->coef, (size_t)h.total_blocks * 128 + 128) || cj_dev_ensure(d->bctl, sizeof(CJBatchCtl)))
+      return CUDA_MEM_ERROR;
+    if (cj_host_ensure(d->h_bctl, sizeof(CJBatchCtl))) return OOM_ERROR;
+    static bool attrs = false;  // per process: the attribute is per function, not per device
+    if (!attrs) {
+      CJ_CUDA_TRY(bt_decode_attrs(), CUDA_MEM_ERROR);
+      attrs = true;
+    }
+    int sms = 0, per_sm = 0;
+    CJ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device), CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &per_sm, (const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT), BT_THREADS, BT_DECODE_SMEM),
+                CUDA_KERNEL_LAUNCH_ERROR);
+    if (per_sm < 1) return UNSUPPORTED_ERROR;
+    const int work = std::max(desc.ntiles, (nwarps + BT_WARPS - 1) / BT_WARPS);
+    d->b_grid = std::max(1, std::min(std::min(per_sm, BT_DECODE_CTAS_DEFAULT) * sms, work));
+    d->b_ntiles = desc.ntiles;
+    d->b_nwarps = nwarps;
+    d->b_nptiles = desc.nptiles;
+    d->raw_len = (size_t)n;
+    d->total_blocks = h.total_blocks;
+    d->param_bytes = sizeof(CJImageHeader) + sizeof(CJImageDesc);
+    CJ_CUDA_TRY(cudaEventRecord(d->ev_begin, s), CUDA_KERNEL_LAUNCH_ERROR);
+    CJ_CUDA_TRY(cudaMemcpyAsync(d->bhdr.p, &h, sizeof(h), cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaMemcpyAsync(d->bdesc.p, &desc, sizeof(desc), cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
+    // (a copy from pageable memory returns once its source has been staged,
+    // so the header and plan may live on this stack frame)
+    if (n) CJ_CUDA_TRY(cudaMemcpyAsync(d->raw.p, jpg->pos, (size_t)n, cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
+  } else {
+    CJ_CUDA_TRY(cudaEventRecord(d->ev_begin, s), CUDA_KERNEL_LAUNCH_ERROR);
+  }
+  CJBatchArgs a;
+  memset(&a, 0, sizeof(a));
+  a.hdr = (const CJImageHeader*)d->bhdr.p;
+  a.desc = (const CJImageDesc*)d->bdesc.p;
+  a.prm = (CJScanParams*)d->params.p;
+  a.st = (CJStatus*)d->status.p;
+  a.blob = (const uint8_t*)d->raw.p;
+  a.data = (uint8_t*)d->data.p;
+  a.tile_keep = (int32_t*)d->tile_keep.p;
+  a.tile_mark = (int32_t*)d->tile_mark.p;
+  a.mpos = (uint32_t*)d->mpos.p;
+  a.mcode = (uint8_t*)d->mcode.p;
+  a.segs = (CJSegment*)d->segs.p;
+  a.recs = (CJSubRec*)d->recs.p;
+  a.ckpt = (CJCkpt*)d->ckpt.p;
+  a.snap0 = (uint64_t*)d->snap.p;
+  a.snap1 = a.snap0 + d->b_nwarps;
+  a.wagg = (CJWarpAgg*)d->wagg.p;
+  a.carry = (CJWarpAgg*)d->carry.p;
+  a.coef = (int16_t*)d->coef.p;
+  a.ctl = (CJBatchCtl*)d->bctl.p;
+  a.n = 1;
+  a.ntiles = d->b_ntiles;
+  a.nwarps = d->b_nwarps;
+  a.nptiles = d->b_nptiles;
+  a.max_passes = d->b_nwarps + 2;
+  cj_profile_begin(d);
+  CJ_CUDA_TRY(cudaMemsetAsync(d->bctl.p, 0, sizeof(CJBatchCtl), s), CUDA_MEM_ERROR);
+  void* args[] = {&a};
+  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT), dim3(d->b_grid),
+                                          dim3(BT_THREADS), args, BT_DECODE_SMEM, s),
+              CUDA_KERNEL_LAUNCH_ERROR);
+  cj_after_launch(d, CJ_K_DECODE_BATCH);
+  CJ_CUDA_TRY(cudaEventRecord(d->ev_scan, s), CUDA_KERNEL_LAUNCH_ERROR);
+  CJ_CUDA_TRY(cudaMemcpyAsync(d->h_bctl.p, d->bctl.p, sizeof(CJBatchCtl), cudaMemcpyDeviceToHost, s),
+              CUDA_MEM_ERROR);
+  return 0;
+}
+
+int cj_reader_decode_status(const JPGReader* jpg) {
+  const CJBatchCtl* ctl = (const CJBatchCtl*)jpg->dev->h_bctl.p;
+  if (!ctl || jpg->dev->progressive) return 0;  // progressive scans have no grid barriers
+  if (ctl->timeout) return CUDA_KERNEL_LAUNCH_ERROR;
+  if (ctl->passes > jpg->dev->b_nwarps + 2) return PROGRAMMER_ERROR;
+  return 0;
+}
+
 // ---------------------------------------------------------------- no-allocation decode
 //
 // cjDecodeNoAlloc: the batch kernel above run on one image whose every piece
@@ -1857,44 +1990,10 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   if (err) return err;
   CJImageHeader h;
   CJImageDesc d;
-  memset(&h, 0, sizeof(h));
-  memset(&d, 0, sizeof(d));
-  for (int s = 0; s < 4; s++) {
-    memcpy(h.counts[s], rd.huff[s].counts, 16);
-    memcpy(h.symbols[s], rd.huff[s].symbols, 256);
-  }
-  h.huff_mask = (uint8_t)r.huff_defined;
-  memcpy(h.dq, r.dq_tables, sizeof(h.dq));
-  h.nch = r.num_channels;
+  err = bt_fill_header(&r, &h);
+  if (err) return err;
   int bpm = 0;
-  for (int c = 0; c < r.num_channels; c++) {
-    h.comp_dc[c] = (uint8_t)r.channels[c].dc_id;
-    h.comp_ac[c] = (uint8_t)r.channels[c].ac_id;
-    h.comp_q[c] = (uint8_t)r.channels[c].dq_id;
-    h.comp_sx[c] = (uint8_t)r.channels[c].samples_x;
-    h.comp_sy[c] = (uint8_t)r.channels[c].samples_y;
-    bpm += h.comp_sx[c] * h.comp_sy[c];
-  }
-  h.mcux = r.num_blocks_x;
-  h.mcuy = r.num_blocks_y;
-  h.width = r.width;
-  h.height = r.height;
-  h.hmax = r.block_size_x >> 3;
-  h.vmax = r.block_size_y >> 3;
-  int xs = 0, ys = 0;
-  if (r.num_channels == 3) {
-    while ((r.channels[1].width << xs) < r.width) xs++;
-    while ((r.channels[1].height << ys) < r.height) ys++;
-  }
-  h.xshift = (uint8_t)xs;
-  h.yshift = (uint8_t)ys;
-  h.restart_interval = r.restart_interval;
-  const int64_t mcus = (int64_t)h.mcux * h.mcuy;
-  h.nseg_expected = r.restart_interval ? (int)((mcus + r.restart_interval - 1) / r.restart_interval) : 1;
-  h.total_blocks = mcus * bpm;
-  if (h.comp_sx[0] != h.hmax || h.comp_sy[0] != h.vmax) return UNSUPPORTED_ERROR;
-  if (h.nch == 3 && ((h.comp_sx[1] << xs) != h.hmax || (h.comp_sy[1] << ys) != h.vmax))
-    return UNSUPPORTED_ERROR;
+  for (int c = 0; c < h.nch; c++) bpm += h.comp_sx[c] * h.comp_sy[c];
   const int ch = h.nch == 3 ? 3 : 1;
   const size_t out_bytes = (size_t)h.width * h.height * ch;
   if (width) *width = h.width;
@@ -1908,24 +2007,8 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   // alone spreads over the whole GPU only with more, shorter subsequences
   // than a batch uses: the single-image paths' 1024 bits (as openJPG), with
   // the batch's full-width pixel tiles.
-  const int S = CJ_SUB_BITS_DEFAULT;
+  bt_plan_one(h, scan_len, CJ_SUB_BITS_DEFAULT, &d);
   d.src_off = scan_off;
-  d.raw_len = scan_len;
-  d.data_off = 0;
-  d.tile0 = 0;
-  d.ntiles = (int)std::max<int64_t>(1, (scan_len + BT_TILE_BYTES - 1) / BT_TILE_BYTES);
-  d.mark0 = 0;
-  d.mark_cap = h.nseg_expected + 1;
-  d.seg0 = 0;
-  d.seg_cap = h.nseg_expected;
-  d.sub_bits = S;
-  d.sub0 = 0;
-  d.sub_cap = ((int)((scan_len * 8 + S - 1) / S) + h.nseg_expected + 1 + 31) & ~31;
-  d.T = cj_pix_tile_mcus(h.hmax, bpm);
-  d.ptile0 = 0;
-  d.nptiles = h.mcuy * ((h.mcux + d.T - 1) / d.T);
-  d.coef0 = 0;
-  d.out_off = 0;
   const int nwarps = d.sub_cap / 32;
   size_t off = 0;
   auto carve = [&](size_t bytes) {

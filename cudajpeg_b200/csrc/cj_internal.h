@@ -32,22 +32,27 @@ struct CJHostHuff {
 struct CJReaderDevice {
   // host-side tables (valid without a GPU)
   CJHostHuff huff[4];
+  uint16_t dq16[4][64];   // quantisation tables as parsed (8- or 16-bit), zig-zag order
+  bool progressive = false;  // the frame is SOF2
+  int prog_scans = 0;        // progressive scans queued for this frame
   // GPU resources, created on the first scan
   bool gpu_ready = false;
   int device = -1;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_begin = nullptr, ev_scan = nullptr, ev_end = nullptr;
   CJDevBuf raw, data, tile_keep, tile_mark, mpos, mcode, segs, recs, ckpt, snap, wagg, carry, coef,
-      pix, params, status, wcoef;
-  CJHostBuf h_params, h_status, h_pixels, h_file;
+      pix, params, status, wcoef, bhdr, bdesc, bctl, pscan;
+  CJHostBuf h_params, h_status, h_pixels, h_file, h_bctl;
   // per-scan bookkeeping
   int sub_bits = CJ_SUB_BITS_DEFAULT;
   size_t raw_len = 0;
   int64_t total_blocks = 0;
   int nsub_cap = 0, nwarp_cap = 0, nseg_exp = 0, mark_cap = 0;
   int scan_pending = 0;   // a scan was launched and its status is not yet checked
-  int snap_parity = 0;    // which last-exit snapshot the next fix-up pass reads
   int comp_first[3];      // first block of each component inside an MCU
+  // the scan as one image of the batch decode kernel (cj_reader_decode)
+  int b_grid = 0, b_ntiles = 0, b_nwarps = 0, b_nptiles = 0;
+  size_t param_bytes = 0;  // header + plan bytes copied to the device per scan
   // kernel accounting: launches since reader creation, and (when profiling)
   // one event after each kernel of the last decode
   long long launches = 0;
@@ -58,10 +63,7 @@ struct CJReaderDevice {
 };
 
 // Kernel ids for per-kernel timing (cjReaderKernelTimes)
-enum {
-  CJ_K_DESTUFF_COUNT = 0, CJ_K_SCAN_TILES, CJ_K_DESTUFF_SCATTER, CJ_K_SEGMENTS, CJ_K_SYNC_INTRA,
-  CJ_K_SYNC_INTER, CJ_K_SCAN_WARPS, CJ_K_DECODE_WRITE, CJ_K_PIXEL, CJ_K_COUNT
-};
+enum { CJ_K_DECODE_BATCH = 0, CJ_K_PIXEL, CJ_K_PROG_SCAN, CJ_K_COUNT };
 
 // Count a kernel launch and, when profiling, timestamp its end.
 void cj_after_launch(CJReaderDevice* d, int kernel_id);
@@ -73,15 +75,37 @@ int cj_host_ensure(CJHostBuf& b, size_t bytes);
 int cj_gpu_init(JPGReader* jpg);
 void cj_dev_release(CJReaderDevice* d);
 
-// Scan stages (scan.cu).  cj_scan_launch stages the scan parameters and the
-// entropy-coded data [jpg->pos, jpg->end) on the device and enqueues the
-// device decode (cj_scan_device) on the reader's stream.
+// Scan stage (scan.cu).  cj_scan_launch fills the reader's host-side scan
+// geometry and enqueues cj_reader_decode(stage = true) on its stream.
 int cj_scan_launch(JPGReader* jpg);
-int cj_scan_device(JPGReader* jpg);
-// Re-runs fix-up passes until stable and re-decodes (rare path).
-int cj_scan_resync(JPGReader* jpg);
-// Launch the coefficient write-out pass only (used by the rare path).
-int cj_scan_write(JPGReader* jpg);
+// The scan's geometry and quantisation tables on the host (scan.cu).
+void cj_fill_params(JPGReader* jpg, CJScanParams* hp);
+// One scan of a progressive frame, as its kernel sees it.
+struct CJProgScan {
+  int32_t ns, ss, se, ah, al;
+  int32_t dc_slot[3], ac_slot[3];
+  int32_t first[3];  // first block of the scan component inside an MCU
+  int32_t sx[3], sy[3];
+  int32_t bpm, mcux;
+  int32_t bw, bh;    // one-component scans: the component's block grid
+  int32_t ri;        // units (MCUs, or blocks of a one-component scan) per interval; 0 = none
+  int32_t nunits, nint;
+};
+// Check a progressive frame's SOS header at jpg->pos (0 or a format.h code).
+int cj_parse_prog_sos(JPGReader* jpg, CJProgScan* s);
+// Progressive frames (progressive.cu): queue one SOS's scan; at EOI, the
+// pixel stage's parameters.
+int cj_prog_scan(JPGReader* jpg);
+int cj_prog_finish(JPGReader* jpg);
+// The scan's entropy decode as one image of the batch decode kernel
+// (batch.cu): with stage = true, plan the image and copy its header and
+// entropy-coded bytes [jpg->pos, jpg->end) to the device first; otherwise
+// re-run the decode over what is already there.  Asynchronous on the
+// reader's stream.
+int cj_reader_decode(JPGReader* jpg, bool stage);
+// After the reader's stream has been synchronised: CUDA_KERNEL_LAUNCH_ERROR
+// when a grid-barrier wait of the last decode timed out, else 0.
+int cj_reader_decode_status(const JPGReader* jpg);
 
 // Pixel stage (pixel.cu): enqueue the fused kernel + D2H of the output.
 int cj_pixel_launch(JPGReader* jpg, bool copy_out);

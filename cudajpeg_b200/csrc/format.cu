@@ -196,17 +196,28 @@ void decodeDRI(JPGReader* jpg) {
 }
 
 void decodeDQT(JPGReader* jpg) {
-  // src/format.cu:424-442: 8-bit tables (a 16-bit table fails the id check)
+  // src/format.cu:424-442 for 8-bit tables.  16-bit tables (Pq = 1, ITU
+  // T.81 B.2.4.1: 64 big-endian values), which the reference rejects through
+  // its id check, are read as well; their values must stay below 2^15 (the
+  // largest step the IJG encoder writes).  dq_tables keeps the reference's
+  // 8-bit view (a 16-bit value saturates there); the decoder uses the
+  // tables as parsed.
   if (!seg_len_ok(jpg)) THROW(SYNTAX_ERROR);
   unsigned int block_len = read16(jpg->pos);
   unsigned char* block_end = jpg->pos + block_len;
   if (block_end > jpg->end) THROW(SYNTAX_ERROR);
   unsigned char* pos = jpg->pos + 2;
-  while (pos + 65 <= block_end) {
-    unsigned char id = pos[0];
-    if (id & 0xFC) THROW(SYNTAX_ERROR);
-    memcpy(&jpg->dq_tables[id][0], pos + 1, 64);
-    pos += 65;
+  while (pos < block_end) {
+    const int pq = pos[0] >> 4, id = pos[0] & 15;
+    const int n = pq ? 129 : 65;
+    if (pq > 1 || id > 3 || pos + n > block_end) THROW(SYNTAX_ERROR);
+    for (int k = 0; k < 64; k++) {
+      const unsigned v = pq ? read16(pos + 1 + 2 * k) : pos[1 + k];
+      if (v > 32767) THROW(UNSUPPORTED_ERROR);
+      jpg->dev->dq16[id][k] = (uint16_t)v;
+      jpg->dq_tables[id][k] = (unsigned char)(v > 255 ? 255 : v);
+    }
+    pos += n;
   }
   if (pos != block_end) THROW(SYNTAX_ERROR);
   jpg->pos = block_end;
@@ -232,6 +243,8 @@ static int cj_marker_loop(JPGReader* r, unsigned char* buf, size_t size, bool st
   r->num_channels = 0;
   r->time = 0;
   r->scan_seen = 0;
+  r->dev->progressive = false;
+  r->dev->prog_scans = 0;
   while (!r->error) {
     if (r->pos > r->end || r->pos[0] != 0xFF) {
       r->error = SYNTAX_ERROR;
@@ -240,11 +253,23 @@ static int cj_marker_loop(JPGReader* r, unsigned char* buf, size_t size, bool st
     r->pos += 2;
     switch (r->pos[-1]) {
       case 0xC0: decodeSOF(r); break;
+      case 0xC2:  // progressive (ITU T.81 Annex G; the reference rejects it)
+        r->dev->progressive = true;
+        decodeSOF(r);
+        break;
       case 0xC4: decodeDHT(r); break;
       case 0xDB: decodeDQT(r); break;
       case 0xDD: decodeDRI(r); break;
       case 0xDA:
         if (stop_at_scan) {
+          if (r->dev->progressive) {
+            // the batch decoder takes baseline frames only: a valid
+            // progressive scan is unsupported there, an invalid one a
+            // syntax error as for the marker loop
+            CJProgScan ps;
+            int e = cj_parse_prog_sos(r, &ps);
+            return r->error = e ? e : UNSUPPORTED_ERROR;
+          }
           int e = cj_parse_sos(r);
           if (!e) r->scan_seen = 1;
           return r->error = e;

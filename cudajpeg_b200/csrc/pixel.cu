@@ -142,7 +142,8 @@ extern "C" void iDCT_resample_colourTransform(JPGReader* jpg) {
   CJReaderDevice* d = jpg->dev;
   if (!d || !d->scan_pending) THROW(PROGRAMMER_ERROR);
   d->scan_pending = 0;
-  int err = cj_pixel_launch(jpg, true);
+  int err = d->progressive ? cj_prog_finish(jpg) : 0;
+  if (!err) err = cj_pixel_launch(jpg, true);
   if (err) THROW(err);
   CJStatus* hs = (CJStatus*)d->h_status.p;
   cudaError_t e = cudaStreamSynchronize(d->stream);
@@ -150,12 +151,8 @@ extern "C" void iDCT_resample_colourTransform(JPGReader* jpg) {
     cj_note_cuda_error(e, "cudaStreamSynchronize", __FILE__, __LINE__);
     THROW(CUDA_KERNEL_LAUNCH_ERROR);
   }
-  if (hs->unstable) {
-    // rare: re-run the fix-up passes to a fixed point, then redo the output
-    if ((err = cj_scan_resync(jpg)) || (err = cj_pixel_launch(jpg, true))) THROW(err);
-    if (cudaStreamSynchronize(d->stream) != cudaSuccess) THROW(CUDA_KERNEL_LAUNCH_ERROR);
-  }
-  err = cj_status_error(hs);
+  err = cj_reader_decode_status(jpg);
+  if (!err) err = cj_status_error(hs);
   if (err) {
     jpg->error = err;
     jpg->error_line = 0;

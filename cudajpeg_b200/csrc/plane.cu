@@ -159,134 +159,122 @@ int cj_upload_basis() {
 
 static uint16_t* g_tc_basis = nullptr;  // device: Khi then Klo, core-matrix layout
 
-// FP32 CUDA-core iDCT of one block straight from global memory (the range
-// fallback of the tensor-core kernel): out[8y+x].
-__device__ void tc_block_f32(const int16_t* blk, const int16_t* q, float* out) {
-  float tmp[64];
-  for (int v = 0; v < 8; v++) {
-    int in[8];
-    for (int u = 0; u < 8; u++) in[u] = (int)blk[8 * v + u] * q[8 * v + u];
-    cj_idct8_f32(in, c_idct_basis, tmp + 8 * v);
-  }
-  for (int x = 0; x < 8; x++) {
-    float col[8], s[8];
-    for (int v = 0; v < 8; v++) col[v] = tmp[8 * v + x];
-    cj_idct8_f32f(col, c_idct_basis, s);
-    for (int y = 0; y < 8; y++) out[8 * y + x] = s[y];
-  }
+// One thread's block of a 128-block tile: its 8 coefficient rows as loaded
+// (quantised int16), where it lives and where its pixels go.
+struct TcRows {
+  uint4 r[8];
+  int64_t gb;  // block index in the coefficient buffer
+  int bx, by;  // block position in the plane
+  bool live;
+};
+
+template <bool RAW>
+__device__ __forceinline__ void tc_fetch(const CJPlaneArgs& a, int64_t t, TcRows& x) {
+  const int64_t kb = t * TC_M + threadIdx.x;
+  x.live = kb < a.nblocks;
+  x.bx = x.by = 0;
+  x.gb = 0;
+  if (x.live) x.gb = RAW ? kb : cj_plane_src(a, kb, &x.bx, &x.by);
+#pragma unroll
+  for (int k8 = 0; k8 < 8; k8++)
+    x.r[k8] = x.live ? __ldg(reinterpret_cast<const uint4*>(a.coef + x.gb * 64 + k8 * 8)) : make_uint4(0, 0, 0, 0);
 }
 
 // RAW = true: write the FP32 values (before +128 / rounding / clip) of block
 // list entries to raw_out; RAW = false: write pixels into the plane.
+//
+// Per 128-block tile: each of the 128 threads dequantises its block into the
+// FP16 A tile (a block whose values FP16 cannot hold exactly is flagged),
+// thread 0 issues the 8 MMAs, and -- while they run and during the epilogue
+// -- every thread already has the loads of its block of the CTA's next tile
+// in flight (register prefetch).  The epilogue reads the block's row of D
+// from tensor memory in two halves of 32 values (pixel rows 0-3, 4-7);
+// flagged blocks take the FP32 CUDA-core fallback for those rows.
 template <bool RAW>
-__global__ void __launch_bounds__(TC_THREADS) k_idct_tc(CJPlaneArgs a, const uint16_t* __restrict__ basis,
-                                                       float* raw_out, int* status) {
+__global__ void __launch_bounds__(TC_THREADS, 5) k_idct_tc(CJPlaneArgs a, const uint16_t* __restrict__ basis,
+                                                          float* raw_out, int* status) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tmem_base;
   __shared__ int16_t q[64];
+  __shared__ int32_t q32[64];
+  __shared__ float sbasis[64];
   uint8_t* sA = smem;               // 128 x 64 fp16 = 16 KiB
   uint8_t* sB = smem + 16384;       // Khi, Klo: 2 x 64 x 64 fp16 = 16 KiB
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x, warp = tid >> 5;
   for (int k = tid; k < 16384 / 16; k += TC_THREADS)
     reinterpret_cast<uint4*>(sB)[k] = __ldg(reinterpret_cast<const uint4*>(basis) + k);
-  if (tid < 64) q[tid] = a.qnat[tid];
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     cj_smem_addr(&tmem_base)),
-                 "r"(64u)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  if (tid < 64) {
+    q[tid] = a.qnat[tid];
+    q32[tid] = a.qnat[tid];
+    sbasis[tid] = c_idct_basis[tid];
   }
+  if (warp == 0) tc_alloc(&tmem_base, 64);
   if (tid == 0) cj_mbar_init(&bar, 1);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
   const uint32_t aaddr = cj_smem_addr(sA), baddr = cj_smem_addr(sB);
   const int64_t ntiles = (a.nblocks + TC_M - 1) / TC_M;
   uint32_t parity = 0;
-  bool failed = false;
-  for (int64_t t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
+  TcRows nx;
+  if ((int64_t)blockIdx.x < ntiles) tc_fetch<RAW>(a, blockIdx.x, nx);
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     // ---- A tile: thread m owns block m; dequantise, check range, FP16
-    const int m = tid;
-    const int64_t kb = t * TC_M + m;
-    const bool live = kb < a.nblocks;
-    int bx = 0, by = 0;
-    int64_t gb = 0;
+    const TcRows cur = nx;
     bool big = false;
-    if (live) gb = RAW ? kb : cj_plane_src(a, kb, &bx, &by);
 #pragma unroll
     for (int k8 = 0; k8 < 8; k8++) {
-      uint4 packed = make_uint4(0, 0, 0, 0);
-      if (live) {
-        uint4 raw = __ldg(reinterpret_cast<const uint4*>(a.coef + gb * 64 + k8 * 8));
-        int v[8];
-        cj_unpack_dequant(raw, q + k8 * 8, v);
-        uint32_t h[4];
+      int v[8];
+      cj_unpack_dequant(cur.r[k8], q + k8 * 8, v);
+      uint32_t h[4];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          big |= (v[2 * j] > 2048 || v[2 * j] < -2048 || v[2 * j + 1] > 2048 || v[2 * j + 1] < -2048);
-          __half2 p2 = __floats2half2_rn((float)v[2 * j], (float)v[2 * j + 1]);
-          h[j] = *reinterpret_cast<uint32_t*>(&p2);
-        }
-        packed = make_uint4(h[0], h[1], h[2], h[3]);
+      for (int j = 0; j < 4; j++) {
+        big |= (v[2 * j] > 2048 || v[2 * j] < -2048 || v[2 * j + 1] > 2048 || v[2 * j + 1] < -2048);
+        __half2 p2 = __floats2half2_rn((float)v[2 * j], (float)v[2 * j + 1]);
+        h[j] = *reinterpret_cast<uint32_t*>(&p2);
       }
-      *reinterpret_cast<uint4*>(sA + tc_core_off(m, k8 * 8)) = packed;
+      *reinterpret_cast<uint4*>(sA + tc_core_off(tid, k8 * 8)) = make_uint4(h[0], h[1], h[2], h[3]);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    // ---- 8 MMAs: A * Khi then A * Klo, K = 16 per instruction
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++)
-        tc_mma(tmem, tc_smem_desc(aaddr + kk * 256), tc_smem_desc(baddr + kk * 256), kk > 0);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++)
-        tc_mma(tmem, tc_smem_desc(aaddr + kk * 256), tc_smem_desc(baddr + 8192 + kk * 256), 1u);
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       cj_smem_addr(&bar))
-                   : "memory");
-    }
-    bool ok = cj_mbar_wait(&bar, parity);
+    if (tid == 0) tc_idct_mmas(tmem, aaddr, baddr, cj_smem_addr(&bar));
+    // ---- the next tile's loads fly while the MMAs run and the epilogue works
+    if (t + gridDim.x < ntiles) tc_fetch<RAW>(a, t + gridDim.x, nx);
+    const bool ok = cj_mbar_wait(&bar, parity);
     parity ^= 1;
     if (!__syncthreads_and(ok)) {
       if (tid == 0) atomicExch(status, 1);
       cj_mbar_wait(&bar, parity ^ 1);  // give an in-flight MMA a bounded chance to land
-      failed = true;
       break;
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // ---- D row m = block m: 64 FP32 values, lanes 32*warp .. 32*warp+31
-    float d[64];
-    tc_ld32(tmem + ((uint32_t)(32 * warp) << 16), d);
-    tc_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 32, d + 32);
-    if (live) {
-      if (big) tc_block_f32(a.coef + gb * 64, q, d);
+    // ---- D row m = block m: two halves of 32 FP32 values (pixel rows 0-3, 4-7)
+#pragma unroll 1
+    for (int h = 0; h < 2; h++) {
+      float d[32];
+      tc_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 32u * h, d);
+      if (!cur.live) continue;
+      if (big) cj_block_f32_half(a.coef + cur.gb * 64, q32, h, sbasis, d);
       if (RAW) {
-        float4* o = reinterpret_cast<float4*>(raw_out + kb * 64);
+        float4* o = reinterpret_cast<float4*>(raw_out + (cur.gb * 64 + 32 * h));
 #pragma unroll
-        for (int k = 0; k < 16; k++) o[k] = make_float4(d[4 * k], d[4 * k + 1], d[4 * k + 2], d[4 * k + 3]);
+        for (int k = 0; k < 8; k++) o[k] = make_float4(d[4 * k], d[4 * k + 1], d[4 * k + 2], d[4 * k + 3]);
       } else {
 #pragma unroll
-        for (int y = 0; y < 8; y++) {
-          uint32_t lo = 0, hi = 0;
-#pragma unroll
-          for (int x = 0; x < 4; x++) lo |= cj_clip8(__float2int_rn(d[8 * y + x]) + 128) << (8 * x);
-#pragma unroll
-          for (int x = 0; x < 4; x++) hi |= cj_clip8(__float2int_rn(d[8 * y + 4 + x]) + 128) << (8 * x);
-          *reinterpret_cast<uint2*>(a.plane + (int64_t)(by * 8 + y) * a.stride + bx * 8) = make_uint2(lo, hi);
-        }
+        for (int y = 0; y < 4; y++)
+          *reinterpret_cast<uint2*>(a.plane + (int64_t)(cur.by * 8 + 4 * h + y) * a.stride + cur.bx * 8) =
+              make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
+                         tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();  // TMEM and the A tile are free for the next tile
   }
-  (void)lane;
   __syncthreads();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64u) : "memory");
+  if (warp == 0) tc_dealloc(tmem, 64);
 }
 
 // Khi / Klo of the Kronecker basis in the K-major core-matrix layout of B
@@ -332,7 +320,15 @@ static int cj_idct_tc_launch(const CJPlaneArgs& a, float* raw, bool is_raw, cuda
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int64_t ntiles = (a.nblocks + TC_M - 1) / TC_M;
-  unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)sms * 4);
+  // CTAs per SM: as many as shared memory and registers allow, at most 7 so
+  // that their tensor-memory columns (64 each) stay within the SM's 512
+  int per_sm = 0;
+  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, is_raw ? (const void*)k_idct_tc<true>
+                                                                              : (const void*)k_idct_tc<false>,
+                                                            TC_THREADS, smem),
+              CUDA_KERNEL_LAUNCH_ERROR);
+  per_sm = std::max(1, std::min(per_sm, 7));
+  unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)sms * per_sm);
   if (grid < 1) grid = 1;
   if (is_raw)
     k_idct_tc<true><<<grid, TC_THREADS, smem, s>>>(a, g_tc_basis, raw, g_tc_status);

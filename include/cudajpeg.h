@@ -18,7 +18,8 @@ extern "C" {
 /* info[0..11]: width, height, channels, MCUs across, MCUs down, restart
  * interval, blocks per MCU, subsequences of the last scan, destuffed scan
  * bytes, markers found, entropy-coded bytes copied to the device, parameter
- * bytes copied to the device (Huffman / quantisation tables, geometry). */
+ * bytes copied to the device (the raw Huffman / quantisation tables and
+ * geometry, and the work plan; the decode tables are built on the GPU). */
 void cjReaderInfo(const JPGReader *r, int64_t *info);
 
 /* The decoded image of the last successful openJPG / openJPGMem: RGB
@@ -47,7 +48,8 @@ const short *cjReaderDeviceQuantTable(const JPGReader *r, int t);
 /* The reader's CUDA stream (cudaStream_t). */
 void *cjReaderStream(const JPGReader *r);
 
-/* Re-run the whole device decode of the last successfully decoded file from
+/* Re-run the whole device decode of the last successfully decoded baseline
+ * file (PROGRAMMER_ERROR after a progressive one) from
  * its compressed bytes already resident on the GPU (destuff .. pixel
  * kernel), leaving the image in device memory and skipping every host<->
  * device copy.  Asynchronous on the reader's stream; check the result with
@@ -64,9 +66,9 @@ const unsigned char *cjReaderDevicePixels(const JPGReader *r);
 /* Per-kernel timing: when on, every kernel launch is followed by a CUDA event
  * on the reader's stream; cjReaderKernelTimes then returns, for the last
  * decode, up to `max` (kernel id, milliseconds) pairs in launch order and
- * their count.  Kernel ids: 0 destuff-count, 1 tile-scan, 2 destuff-scatter,
- * 3 segments, 4 sync-intra, 5 sync-inter, 6 warp-scan, 7 decode-write,
- * 8 pixel. */
+ * their count.  Kernel ids: 0 the entropy decode (the batch decoder's
+ * cooperative kernel on this one image), 1 the pixel kernel, 2 one scan of a
+ * progressive frame. */
 void cjReaderSetProfile(JPGReader *r, int on);
 int cjReaderKernelTimes(const JPGReader *r, int *ids, float *ms, int max);
 

@@ -15,7 +15,12 @@
  *   - scan loop incl. restart markers . src/decodeScanGPU.cu:435-490
  *   - integer iDCT (row / column) ..... CPUonly/src/pixelTransformCPU.c:14-107
  *   - nearest upsample + YCbCr->RGB ... CPUonly/src/pixelTransformCPU.c:110-172
- * and adds an FP64 separable iDCT used to measure iDCT error.
+ * and adds an FP64 separable iDCT used to measure iDCT error.  Beyond the
+ * reference (which rejects both, src/format.cu:191-200 and :432) it also
+ * decodes progressive frames (SOF2, ITU T.81 Annex G) and 16-bit
+ * quantisation tables (Pq = 1): the checker of the decoder's extensions,
+ * pinned by files whose baseline twin (the same coefficients written as one
+ * baseline scan) the reference decodes.
  *
  * Parity is pinned against the reference itself: oracle/Makefile compiles the
  * reference's own sources into oracle/_ref/, and tests/golden/ holds vectors
@@ -51,6 +56,7 @@ typedef struct {
   int nblocks;
   int32_t *coef; /* dequantised, natural order, 64 per block, scan order */
   int32_t *coef_pos;
+  int32_t *qcoef; /* progressive frames: quantised values built up scan by scan */
   uint8_t *plane; /* stride x rows */
 } OracleComp;
 
@@ -64,7 +70,9 @@ typedef struct {
   int restart_interval;
   OracleComp comp[3];
   OracleVlc *vlc[4]; /* DC0, DC1, AC0, AC1 (table_id = (Tc<<1 | Th)) */
-  uint8_t dq[4][64]; /* zig-zag order, as stored in the DQT segment */
+  uint16_t dq[4][64]; /* zig-zag order, as stored in the DQT segment */
+  int progressive;    /* SOF2 */
+  int eobrun;         /* progressive AC scans: blocks left in the current end-of-band run */
   uint8_t *pixels; /* RGB W*H*3, or grey W*H */
   int error;
   int scan_done;
@@ -126,6 +134,12 @@ static void parse_sof(OracleImage *im) {
     k->coef = (int32_t *)calloc((size_t)k->nblocks * 64, sizeof(int32_t));
     k->plane = (uint8_t *)malloc((size_t)k->stride * k->rows);
     if (!k->coef || !k->plane) { im->error = OR_OOM_ERROR; return; }
+    free(k->qcoef);
+    k->qcoef = NULL;
+    if (im->progressive) {
+      k->qcoef = (int32_t *)calloc((size_t)k->nblocks * 64, sizeof(int32_t));
+      if (!k->qcoef) { im->error = OR_OOM_ERROR; return; }
+    }
     k->coef_pos = k->coef;
   }
   if (im->nch == 3) {
@@ -179,14 +193,22 @@ static void parse_dht(OracleImage *im) {
 }
 
 static void parse_dqt(OracleImage *im) {
-  /* src/format.cu:424-442: 8-bit tables only (Pq=1 fails the id check) */
+  /* src/format.cu:424-442 for 8-bit tables; 16-bit tables (Pq = 1, T.81
+   * B.2.4.1: 64 big-endian values), which the reference rejects, are read
+   * too -- their values must stay below 2^15 */
   uint8_t *seg_end = im->pos + read16(im->pos);
   if (seg_end > im->end) { im->error = OR_SYNTAX_ERROR; return; }
   uint8_t *p = im->pos + 2;
-  while (p + 65 <= seg_end) {
-    if (p[0] & 0xFC) { im->error = OR_SYNTAX_ERROR; return; }
-    memcpy(im->dq[p[0]], p + 1, 64);
-    p += 65;
+  while (p < seg_end) {
+    const int pq = p[0] >> 4, id = p[0] & 15;
+    const int n = pq ? 129 : 65;
+    if (pq > 1 || id > 3 || p + n > seg_end) { im->error = OR_SYNTAX_ERROR; return; }
+    for (int k = 0; k < 64; k++) {
+      const unsigned v = pq ? read16(p + 1 + 2 * k) : p[1 + k];
+      if (v > 32767) { im->error = OR_UNSUPPORTED_ERROR; return; }
+      im->dq[id][k] = (uint16_t)v;
+    }
+    p += n;
   }
   if (p != seg_end) { im->error = OR_SYNTAX_ERROR; return; }
   im->pos = seg_end;
@@ -254,7 +276,7 @@ static void decode_block(OracleImage *im, OracleComp *k) {
   /* src/decodeScanGPU.cu:78-100 */
   uint8_t sym = 0;
   int32_t *blk = k->coef_pos;
-  const uint8_t *q = im->dq[k->dq_id];
+  const uint16_t *q = im->dq[k->dq_id];
   k->dc_pred += get_vlc(im, im->vlc[k->dc_id], NULL);
   blk[0] = k->dc_pred * q[0];
   int z = 0;
@@ -319,6 +341,231 @@ static void decode_scan(OracleImage *im) {
       }
     }
   im->scan_done = 1;
+}
+
+/* ---------------- progressive scans (ITU T.81 Annex G) ----------------
+ *
+ * Not in the reference (it rejects SOF2, src/format.cu:191-200).  Each
+ * scan's entropy-coded data runs to the next marker that is not RSTn; the
+ * bit reader below reads it with the FF 00 stuffing removed.  Coefficients
+ * are built up in qcoef (quantised, natural order) and dequantised at EOI. */
+
+typedef struct {
+  const uint8_t *p, *end; /* stuffed bytes of the scan */
+  uint32_t bits;
+  int nbits;
+} ProgBits;
+
+static int pb_bit(ProgBits *b) {
+  if (!b->nbits) {
+    uint8_t v = 0;
+    if (b->p < b->end) {
+      v = *b->p++;
+      if (v == 0xFF && b->p < b->end && *b->p == 0x00) b->p++;
+    }
+    b->bits = v;
+    b->nbits = 8;
+  }
+  b->nbits--;
+  return (b->bits >> b->nbits) & 1;
+}
+
+static int pb_bits(ProgBits *b, int n) {
+  int v = 0;
+  while (n--) v = (v << 1) | pb_bit(b);
+  return v;
+}
+
+/* Huffman decode with the 16-bit table: bit by bit against the code lengths
+ * (the table gives {len, symbol} of the code that prefixes a window). */
+static int pb_huff(ProgBits *b, const OracleVlc *t, int *err) {
+  int code = 0;
+  for (int l = 1; l <= 16; l++) {
+    code = (code << 1) | pb_bit(b);
+    const OracleVlc e = t[code << (16 - l)];
+    if (e.len == l) return e.sym;
+  }
+  *err = OR_SYNTAX_ERROR;
+  return 0;
+}
+
+static int pb_extend(int v, int s) { return v < (1 << (s - 1)) ? v - (1 << s) + 1 : v; }
+
+/* After a restart interval: skip to the byte boundary and the RSTn marker. */
+static int pb_restart(ProgBits *b, int expect) {
+  b->nbits = 0;
+  if (b->p + 1 >= b->end || b->p[0] != 0xFF || b->p[1] != (0xD0 | expect)) return OR_SYNTAX_ERROR;
+  b->p += 2;
+  return 0;
+}
+
+/* One block of a progressive scan (T.81 G.1.2.1-3; the decoding procedures
+ * DECODE_DC_FIRST / DC refinement / DECODE_AC_FIRST / AC refinement with
+ * end-of-band runs). */
+static int prog_block(OracleImage *im, ProgBits *b, OracleComp *k, int32_t *q, int ss, int se, int ah, int al) {
+  int err = 0;
+  if (ss == 0) {
+    if (!ah) {
+      const int s = pb_huff(b, im->vlc[k->dc_id], &err);
+      if (err) return err;
+      if (s > 11) return OR_SYNTAX_ERROR;
+      k->dc_pred += s ? pb_extend(pb_bits(b, s), s) : 0;
+      q[0] = k->dc_pred * (1 << al);
+    } else if (pb_bit(b)) {
+      q[0] |= 1 << al;
+    }
+    return 0;
+  }
+  const OracleVlc *t = im->vlc[k->ac_id];
+  int kk = ss;
+  if (!ah) {
+    if (im->eobrun > 0) { im->eobrun--; return 0; }
+    while (kk <= se) {
+      const int rs = pb_huff(b, t, &err);
+      if (err) return err;
+      const int r = rs >> 4, s = rs & 15;
+      if (s) {
+        kk += r;
+        if (kk > se) return OR_SYNTAX_ERROR;
+        q[kZigZagToNatural[kk]] = pb_extend(pb_bits(b, s), s) * (1 << al);
+        kk++;
+      } else if (r == 15) {
+        kk += 16;
+      } else {
+        im->eobrun = (1 << r) - 1;
+        if (r) im->eobrun += pb_bits(b, r);
+        break;
+      }
+    }
+    return 0;
+  }
+  const int p1 = 1 << al, m1 = -(1 << al);
+  if (im->eobrun == 0) {
+    for (; kk <= se; kk++) {
+      const int rs = pb_huff(b, t, &err);
+      if (err) return err;
+      int r = rs >> 4, s = rs & 15, val = 0;
+      if (s) {
+        if (s != 1) return OR_SYNTAX_ERROR;
+        val = pb_bit(b) ? p1 : m1;
+      } else if (r != 15) {
+        im->eobrun = 1 << r;
+        if (r) im->eobrun += pb_bits(b, r);
+        break;
+      }
+      /* pass r zero-history coefficients, refining the nonzero ones met */
+      while (kk <= se) {
+        int32_t *c = &q[kZigZagToNatural[kk]];
+        if (*c) {
+          if (pb_bit(b) && !(*c & p1)) *c += *c >= 0 ? p1 : m1;
+        } else if (--r < 0) {
+          break;
+        }
+        kk++;
+      }
+      if (val) {
+        if (kk > se) return OR_SYNTAX_ERROR;
+        q[kZigZagToNatural[kk]] = val;
+      }
+    }
+  }
+  if (im->eobrun > 0) {
+    /* inside an end-of-band run: correction bits of the nonzero coefficients */
+    for (; kk <= se; kk++) {
+      int32_t *c = &q[kZigZagToNatural[kk]];
+      if (*c && pb_bit(b) && !(*c & p1)) *c += *c >= 0 ? p1 : m1;
+    }
+    im->eobrun--;
+  }
+  return 0;
+}
+
+static void decode_prog_scan(OracleImage *im) {
+  /* SOS of a progressive frame (T.81 B.2.3, G.1.1.1.1) */
+  uint8_t *p = im->pos;
+  unsigned hlen = read16(p);
+  if (p + hlen > im->end || hlen < 6) { im->error = OR_SYNTAX_ERROR; return; }
+  const int ns = p[2];
+  if (ns < 1 || ns > im->nch || hlen != 6u + 2u * ns) { im->error = OR_SYNTAX_ERROR; return; }
+  int comps[3];
+  for (int j = 0; j < ns; j++) {
+    const uint8_t *d = p + 3 + 2 * j;
+    int c = 0;
+    while (c < im->nch && im->comp[c].id != d[0]) c++;
+    if (c == im->nch || (j && c <= comps[j - 1]) || (d[1] & 0xEE)) { im->error = OR_SYNTAX_ERROR; return; }
+    comps[j] = c;
+    im->comp[c].dc_id = d[1] >> 4;
+    im->comp[c].ac_id = (d[1] & 1) | 2;
+  }
+  const uint8_t *t = p + 3 + 2 * ns;
+  const int ss = t[0], se = t[1], ah = t[2] >> 4, al = t[2] & 15;
+  if ((ss == 0) != (se == 0) || se > 63 || ss > se || (ss && ns != 1) || al > 13 || (ah && ah != al + 1)) {
+    im->error = OR_SYNTAX_ERROR;
+    return;
+  }
+  for (int j = 0; j < ns; j++) {
+    const OracleComp *k = &im->comp[comps[j]];
+    if ((ss == 0 && !ah && !im->vlc[k->dc_id]) || (ss && !im->vlc[k->ac_id])) { im->error = OR_SYNTAX_ERROR; return; }
+  }
+  im->pos += hlen;
+  /* the scan's data: up to the next marker other than RSTn */
+  const uint8_t *e = im->pos;
+  while (e + 1 < im->end + 2 && !(e[0] == 0xFF && e[1] != 0x00 && (e[1] & 0xF8) != 0xD0)) e++;
+  ProgBits b = {im->pos, e, 0, 0};
+  im->eobrun = 0;
+  for (int c = 0; c < 3; c++) im->comp[c].dc_pred = 0;
+  const int ri = im->restart_interval;
+  int left = ri, expect = 0, err = 0;
+  if (ns > 1) { /* interleaved (DC scans only): MCU order */
+    for (int my = 0; my < im->mcuy && !err; my++)
+      for (int mx = 0; mx < im->mcux && !err; mx++) {
+        for (int j = 0; j < ns && !err; j++) {
+          OracleComp *k = &im->comp[comps[j]];
+          const int per = k->sx * k->sy;
+          for (int w = 0; w < per && !err; w++)
+            err = prog_block(im, &b, k, k->qcoef + 64 * ((size_t)(my * im->mcux + mx) * per + w), ss, se, ah, al);
+        }
+        if (!err && ri && !(--left) && !(my == im->mcuy - 1 && mx == im->mcux - 1)) {
+          err = pb_restart(&b, expect);
+          expect = (expect + 1) & 7;
+          left = ri;
+          im->eobrun = 0;
+          for (int c = 0; c < 3; c++) im->comp[c].dc_pred = 0;
+        }
+      }
+  } else { /* one component: its blocks in raster order, not padded to MCUs */
+    OracleComp *k = &im->comp[comps[0]];
+    const int bw = (k->width + 7) / 8, bh = (k->height + 7) / 8, per = k->sx * k->sy;
+    for (int by = 0; by < bh && !err; by++)
+      for (int bx = 0; bx < bw && !err; bx++) {
+        const size_t mcu = (size_t)(by / k->sy) * im->mcux + bx / k->sx;
+        const size_t blk = mcu * per + (by % k->sy) * k->sx + bx % k->sx;
+        err = prog_block(im, &b, k, k->qcoef + 64 * blk, ss, se, ah, al);
+        if (!err && ri && !(--left) && !(by == bh - 1 && bx == bw - 1)) {
+          err = pb_restart(&b, expect);
+          expect = (expect + 1) & 7;
+          left = ri;
+          im->eobrun = 0;
+          k->dc_pred = 0;
+        }
+      }
+  }
+  if (err) { im->error = err; return; }
+  im->pos = (uint8_t *)e;
+  im->scan_done = 1;
+}
+
+/* Progressive frames at EOI: dequantise the built-up coefficients. */
+static void prog_dequantise(OracleImage *im) {
+  for (int c = 0; c < im->nch; c++) {
+    OracleComp *k = &im->comp[c];
+    const uint16_t *dq = im->dq[k->dq_id];
+    for (size_t b = 0; b < (size_t)k->nblocks; b++)
+      for (int z = 0; z < 64; z++) {
+        const int n = kZigZagToNatural[z];
+        k->coef[64 * b + n] = k->qcoef[64 * b + n] * dq[z];
+      }
+  }
 }
 
 /* ---------------- pixel stage (CPUonly/src/pixelTransformCPU.c) ---------------- */
@@ -466,7 +713,7 @@ void oracle_free(OracleImage *im) {
   if (!im) return;
   free(im->buf);
   for (int i = 0; i < 4; i++) free(im->vlc[i]);
-  for (int c = 0; c < 3; c++) { free(im->comp[c].coef); free(im->comp[c].plane); }
+  for (int c = 0; c < 3; c++) { free(im->comp[c].coef); free(im->comp[c].plane); free(im->comp[c].qcoef); }
   free(im->pixels);
   free(im);
 }
@@ -495,12 +742,14 @@ OracleImage *oracle_decode(const uint8_t *data, size_t size, int *err) {
     uint8_t m = im->pos[-1];
     switch (m) {
       case 0xC0: parse_sof(im); break;
+      case 0xC2: im->progressive = 1; parse_sof(im); break;
       case 0xC4: parse_dht(im); break;
       case 0xDB: parse_dqt(im); break;
       case 0xDD: parse_dri(im); break;
       case 0xDA:
         if (!im->nch) { im->error = OR_SYNTAX_ERROR; break; }
-        decode_scan(im);
+        if (im->progressive) decode_prog_scan(im);
+        else decode_scan(im);
         break;
       case 0xFE: skip_segment(im); break;
       case 0xD9: break;
@@ -511,6 +760,7 @@ OracleImage *oracle_decode(const uint8_t *data, size_t size, int *err) {
     if (im->error) break;
     if (im->pos[-1] == 0xD9) {
       if (!im->scan_done) { im->error = OR_SYNTAX_ERROR; break; }
+      if (im->progressive) prog_dequantise(im);
       pixel_stage(im);
       break;
     }
@@ -545,7 +795,7 @@ void oracle_pixels(const OracleImage *im, uint8_t *out) {
   memcpy(out, im->pixels, (size_t)im->width * im->height * (im->nch == 3 ? 3 : 1));
 }
 
-void oracle_dq(const OracleImage *im, uint8_t *out) { memcpy(out, im->dq, sizeof(im->dq)); }
+void oracle_dq(const OracleImage *im, uint16_t *out) { memcpy(out, im->dq, sizeof(im->dq)); }
 
 /* Integer iDCT of n natural-order blocks (int32 dequantised) into n separate
  * 8x8 uint8 tiles: used to test the plane kernels block by block. */

@@ -88,7 +88,7 @@ class Decoded:
     coefs: list = field(default_factory=list)   # int32 [nblocks, 64] per component
     planes: list = field(default_factory=list)  # uint8 [rows, stride] per component
     pixels: np.ndarray | None = None            # uint8 [H, W, 3] or [H, W]
-    dq: np.ndarray | None = None                # uint8 [4, 64] zig-zag order
+    dq: np.ndarray | None = None                # uint16 [4, 64] zig-zag order
     fancy_ycc: np.ndarray | None = None         # uint8 [H, W, 3], fancy=True only
     fancy_rgb: np.ndarray | None = None         # uint8 [H, W, 3], fancy=True only
 
@@ -119,7 +119,7 @@ def decode(data: bytes, fancy: bool = False) -> Decoded:
         shape = (out.height, out.width, 3) if out.nch == 3 else (out.height, out.width)
         out.pixels = np.empty(shape, np.uint8)
         lib.oracle_pixels(h, out.pixels.ctypes.data)
-        out.dq = np.empty((4, 64), np.uint8)
+        out.dq = np.empty((4, 64), np.uint16)
         lib.oracle_dq(h, out.dq.ctypes.data)
         if fancy and out.nch == 3:
             out.fancy_ycc = np.empty((out.height, out.width, 3), np.uint8)

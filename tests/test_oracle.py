@@ -93,3 +93,71 @@ def test_fancy_upsampling_matches_libjpeg(oracle_mod, mode, h, w):
     assert im.mode == "YCbCr" and want.shape == d.fancy_ycc.shape
     assert np.array_equal(d.fancy_ycc[..., 0], want[..., 0])  # luma: the DC-only iDCTs agree
     assert np.array_equal(d.fancy_ycc, want)
+
+
+def progressive_twins(mode, w, h, q, ri, seed):
+    """The same pixels encoded baseline and progressive by Pillow's libjpeg:
+    same quantisation, same coefficients, different scans."""
+    import io
+
+    from PIL import Image
+    rng = np.random.default_rng(seed)
+    arr = W.smooth_content(rng, w, h, 1 if mode == "gray" else 3)
+    if mode == "gray":
+        arr = arr[..., 0]
+    out = []
+    for prog in (False, True):
+        buf = io.BytesIO()
+        kw = dict(quality=q, optimize=False, progressive=prog)
+        if mode != "gray":
+            kw["subsampling"] = W.SUBSAMPLING[mode]
+        if ri:
+            kw["restart_marker_blocks"] = ri
+        Image.fromarray(arr, "L" if mode == "gray" else "RGB").save(buf, "JPEG", **kw)
+        out.append(buf.getvalue())
+    return out
+
+
+PROGRESSIVE_CASES = [("420", 200, 136, 85, 0), ("422", 333, 200, 92, 0), ("444", 96, 80, 75, 0),
+                     ("gray", 150, 90, 90, 0), ("420", 257, 131, 60, 0), ("420", 128, 96, 80, 2),
+                     ("444", 64, 64, 95, 3), ("420", 17, 9, 70, 0)]
+
+
+@pytest.mark.parametrize("mode,w,h,q,ri", PROGRESSIVE_CASES)
+def test_oracle_progressive_equals_baseline_twin(oracle_mod, mode, w, h, q, ri):
+    """The oracle's progressive decode (T.81 Annex G) gives the coefficients
+    and pixels of the baseline twin, which the reference decodes."""
+    base, prog = progressive_twins(mode, w, h, q, ri, seed=w + h)
+    assert prog.count(b"\xff\xda") > 1 and b"\xff\xc2" in prog
+    a, b = oracle_mod.decode(base), oracle_mod.decode(prog)
+    assert a.error == b.error == 0
+    for x, y in zip(a.coefs, b.coefs):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.pixels, b.pixels)
+
+
+def dqt_to_16bit(data: bytes, scale: int = 1) -> bytes:
+    """Rewrite every 8-bit DQT table of a file as a 16-bit table (Pq = 1)
+    holding the same values times `scale`."""
+    out, i = bytearray(), 0
+    while True:
+        j = data.find(b"\xff\xdb", i)
+        if j < 0 or j > data.find(b"\xff\xda"):
+            out += data[i:]
+            return bytes(out)
+        n = (data[j + 2] << 8) | data[j + 3]
+        seg, body = data[j + 4: j + 2 + n], bytearray()
+        for k in range(0, len(seg), 65):
+            body.append(0x10 | seg[k])
+            for v in seg[k + 1: k + 65]:
+                body += (v * scale).to_bytes(2, "big")
+        out += data[i:j] + b"\xff\xdb" + (len(body) + 2).to_bytes(2, "big") + body
+        i = j + 2 + n
+
+
+def test_oracle_16bit_dqt(oracle_mod):
+    s = W.small_case(51, 120, 88, "420", 80, 0, "texture")
+    d8, d16 = oracle_mod.decode(s.data), oracle_mod.decode(dqt_to_16bit(s.data))
+    assert d8.error == d16.error == 0 and np.array_equal(d8.pixels, d16.pixels)
+    big = oracle_mod.decode(dqt_to_16bit(s.data, scale=12))  # steps above 255
+    assert big.error == 0 and int(big.dq.max()) > 255
