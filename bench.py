@@ -90,6 +90,11 @@ def parse_args():
                     help="under torchrun: partition one batch across ranks (strong scaling) "
                          "instead of one batch per rank (weak scaling)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default batch tuning")
+    ap.add_argument("--idct", default="int", choices=["int", "tc"],
+                    help="pixel-stage iDCT of the batch: the reference's integer iDCT (bit-exact) or tensor cores")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="time the batch run only (no end-to-end, plain path, serving or other configurations): "
+                         "the short command the profiles are captured with")
     ap.add_argument("--tuning", default="",
                     help="fixed batch tuning SUB_BITS,CTAS_PER_SM,TILE_CAP instead of the autotuner")
     ap.add_argument("--serve-seconds", type=float, default=1.5,
@@ -409,7 +414,9 @@ def run_batch(args, wl, world, rank, local, dist):
     blob, offsets, sizes = cj.Batch.pack(wl.files)
     src = torch.empty(len(blob), dtype=torch.uint8, pin_memory=True)
     src.numpy()[:] = blob
+    idct = cj.IDCT_TC if args.idct == "tc" else cj.IDCT_INT
     b = cj.Batch()
+    b.set_output(cj.OUTPUT_RGB, idct)
     b.stage(src.data_ptr(), offsets, sizes)
     b.run()
     b.fetch()
@@ -460,6 +467,15 @@ def run_batch(args, wl, world, rank, local, dist):
     job_pixels = R.sum_over_ranks(wl.pixels, dist, "cuda")
     job_file_bytes = R.sum_over_ranks(wl.file_bytes, dist, "cuda")
     value = job_pixels * args.steps / (total_ms / 1e3) / 1e6
+    if args.kernels_only:
+        b.close()
+        return {"metric": METRIC, "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int16/int32",
+                "data": "synthetic", "config": dict(wl.config, idct=args.idct, kernels_only=True,
+                                                   tuning=tune),
+                "phase_ms": {k: round(statistics.mean(v), 4) for k, v in phases.items()},
+                "gpu_launches": int(launches), "clocks": clocks.summary()}
 
     # end to end through the public C API: every step parses the files on the
     # host, copies them from pinned memory to the device, decodes, and copies
@@ -468,6 +484,7 @@ def run_batch(args, wl, world, rank, local, dist):
     # next step's host parse, host->device copy and kernels.
     b2 = cj.Batch()
     b2.set_tuning(tune["sub_bits"], tune["decode_ctas_per_sm"], tune["pixel_tile_cap"])
+    b2.set_output(cj.OUTPUT_RGB, idct)
     pair = [b, b2]
     e2e_lat = []
     for x in pair:  # one sequential step each: latency of a lone step, and buffers warm
@@ -843,9 +860,10 @@ def run_gpu(args):
         line = run_batch(args, wl, world, rank, local, dist)
     else:
         line = run_single(args, wl, world, rank, local, dist)
-    if rank == 0 and world == 1 and args.workload == "mixed_batch" and not args.no_other_configs:
+    if rank == 0 and world == 1 and args.workload == "mixed_batch" and not args.no_other_configs \
+            and not args.kernels_only:
         line["other_configs"] = other_configs(args)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.kernels_only:
         line["cpu_baseline"] = cpu_baseline(wl, os.cpu_count() or 1, args.cpu_seconds)
     if dist:
         dist.destroy_process_group()

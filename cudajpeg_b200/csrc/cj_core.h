@@ -1,7 +1,7 @@
-// cj_core.h -- data layouts and the per-lane Huffman block decoder shared by
-// the entropy kernels.  Everything here is plain C++ marked __host__
-// __device__ so the same code is compiled for sm_100a kernels and for host
-// unit checks of the table builder.
+// cj_core.h -- data layouts, Huffman tables and decode steps shared by the
+// entropy kernels.  Everything here is plain C++ marked __host__ __device__
+// so the same code is compiled for sm_100a kernels and for host checks of
+// the table builder.
 #pragma once
 #include <stdint.h>
 
@@ -164,16 +164,6 @@ CJ_HD uint32_t cj_word(const uint32_t* words, uint64_t w, uint64_t end_byte) {
   return v;
 }
 
-// 32 bits starting at bit `p` (MSB first).
-CJ_HD uint32_t cj_peek32(const uint32_t* words, uint64_t p, uint64_t end_byte) {
-  uint64_t w = p >> 5;
-  uint32_t s = (uint32_t)(p & 31);
-  uint32_t hi = cj_word(words, w, end_byte);
-  if (!s) return hi;
-  uint32_t lo = cj_word(words, w + 1, end_byte);
-  return (hi << s) | (lo >> (32 - s));
-}
-
 // Decode one Huffman code from a left-aligned 16-bit window.  Returns
 // (len << 8) | symbol, or 0 when no code of length 1..16 matches.
 // Codes longer than CJ_FAST_BITS: canonical search by length.
@@ -256,116 +246,3 @@ CJ_HD int32_t cj_extend(uint32_t bits, uint32_t size) {
   {0,  1,  8,  16, 9,  2,  3,  10, 17, 24, 32, 25, 18, 11, 4,  5,  12, 19, 26, 33, 40, 48, \
    41, 34, 27, 20, 13, 6,  7,  14, 21, 28, 35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, \
    30, 37, 44, 51, 58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63}
-
-// MSB-first bit reader over the destuffed buffer with a 64-bit register
-// window and one word of prefetch, so the load feeding the next refill is in
-// flight while the current symbols decode.  Bytes at or past `end_byte` read
-// as 0xFF (the padding the reference's bit reader supplies).  Word indices are
-// 32-bit (a scan is at most CJ_MAX_SCAN_BYTES); the bit position is not kept
-// but derived: pos() = 32 * w - n.
-struct CJBits {
-  const uint32_t* words;
-  uint64_t buf;        // unread bits, MSB-aligned
-  uint32_t w;          // index of the word in `nxt`
-  uint32_t wfull;      // words below this index lie wholly before end_byte
-  uint32_t end_byte;
-  uint32_t nxt;        // the next word to append, already loaded
-  int n;               // valid bits in buf (32..63 after a refill)
-
-  CJ_HD uint32_t word(uint32_t i) const {
-    if (i < wfull) return cj_bswap(words[i]);
-    return cj_word(words, i, end_byte);  // the partial last word, or past the end
-  }
-  CJ_HD void init(const uint32_t* wd, uint64_t eb, uint64_t p) {
-    words = wd;
-    end_byte = (uint32_t)eb;
-    wfull = (uint32_t)(eb >> 2);
-    uint32_t w0 = (uint32_t)(p >> 5);
-    uint32_t s = (uint32_t)(p & 31);
-    buf = ((uint64_t)word(w0) << 32) << s;
-    n = 32 - (int)s;
-    w = w0 + 1;
-    nxt = word(w);
-    refill();
-  }
-  CJ_HD void refill() {
-    if (n < 32) {
-      buf |= (uint64_t)nxt << (32 - n);
-      n += 32;
-      w++;
-      nxt = word(w);
-    }
-  }
-  CJ_HD uint64_t pos() const { return ((uint64_t)w << 5) - (uint64_t)n; }
-  CJ_HD uint32_t peek32() const { return (uint32_t)(buf >> 32); }
-  CJ_HD void skip(uint32_t k) {
-    buf <<= k;
-    n -= (int)k;
-    refill();
-  }
-};
-
-// Decode one block at the reader's position with the given tables.
-//   Sink receives (natural index, value) for every nonzero AC coefficient.
-//   *dc_diff gets the DC difference.  Returns CJ_DEV_* (0 ok).  On an error
-//   the block is cut short at the failing symbol, consuming at least one bit,
-//   so a speculative decode keeps moving.
-template <class Sink>
-CJ_HD int cj_block(CJBits& br, const CJHuff& dc, const CJHuff& ac, const uint8_t* zz,
-                   int32_t* dc_diff, Sink& sink) {
-  uint32_t v = br.peek32();
-  uint32_t e = cj_huff_decode(dc, v >> 16);
-  if (!e) {
-    *dc_diff = 0;
-    br.skip(1);
-    return CJ_DEV_BAD_CODE;
-  }
-  uint32_t len = e >> 8, size = e & 15;
-  *dc_diff = size ? cj_extend((v << len) >> (32 - size), size) : 0;
-  br.skip(len + size);
-  int k = 0;
-  for (;;) {
-    v = br.peek32();
-    e = cj_huff_decode(ac, v >> 16);
-    if (!e) {
-      br.skip(1);
-      return CJ_DEV_BAD_CODE;
-    }
-    len = e >> 8;
-    uint32_t sym = e & 255;
-    size = sym & 15;
-    if (!size) {
-      br.skip(len);
-      if (sym == 0) return 0;             // EOB
-      if (sym != 0xF0) return CJ_DEV_BAD_AC;
-      k += 16;                            // ZRL
-      if (k > 63) return CJ_DEV_BAD_AC;
-      if (k == 63) return 0;
-      continue;
-    }
-    k += (int)(sym >> 4) + 1;
-    if (k > 63) {
-      br.skip(len);
-      return CJ_DEV_BAD_AC;
-    }
-    sink(zz[k], cj_extend((v << len) >> (32 - size), size));
-    br.skip(len + size);
-    if (k == 63) return 0;
-  }
-}
-
-// Reference-style wrapper used by host tools: decode the block at bit `p`.
-template <class Sink>
-CJ_HD uint64_t cj_decode_block(const uint32_t* words, uint64_t end_byte, uint64_t p,
-                               const CJHuff& dc, const CJHuff& ac, const uint8_t* zz,
-                               int32_t* dc_diff, int* err, Sink& sink, uint64_t* last_sym) {
-  CJBits br;
-  br.init(words, end_byte, p);
-  *err = cj_block(br, dc, ac, zz, dc_diff, sink);
-  *last_sym = p;
-  return br.pos();
-}
-
-struct CJNullSink {
-  CJ_HD void operator()(int, int32_t) const {}
-};

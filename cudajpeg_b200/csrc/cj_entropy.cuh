@@ -1,7 +1,7 @@
-// cj_entropy.cuh -- device building blocks of the entropy decode shared by
-// the per-image kernels (scan.cu) and the persistent batch kernel
-// (batch.cu): destuff classification, subsequence lanes, speculative block
-// decode and the warp settle loop.
+// cj_entropy.cuh -- device building blocks of the entropy decode in the
+// persistent batch kernel (batch.cu): destuff classification, subsequence
+// lanes, speculative block decode, the warp settle loop and the cooperative
+// coefficient write-out.
 #pragma once
 #include <limits.h>
 #include <stdint.h>
@@ -105,10 +105,6 @@ __device__ __forceinline__ CJChunk cj_classify_in(const CJChunkIn& x, int64_t n,
   return c;
 }
 
-__device__ __forceinline__ CJChunk cj_classify(const uint8_t* raw, int64_t n, int64_t base) {
-  return cj_classify_in(cj_chunk_load(raw, n, base), n, base);
-}
-
 struct CJLane {
   uint64_t begin, end;   // this subsequence's bits
   uint64_t end_byte;     // its segment's end (bytes)
@@ -148,7 +144,8 @@ __device__ __forceinline__ CJLane cj_lane(const CJSegment* segs, int nseg, int n
 // One more word is loaded a crossing ahead and kept as read from memory
 // (byte-swapped only when it becomes the next word), so a load has several
 // symbols to arrive before the window needs it.
-// Bytes at or past `end_byte` read as 0xFF, as in CJBits.
+// Bytes at or past `end_byte` read as 0xFF (the padding the reference's bit
+// reader supplies).
 struct CJFBits {
   const uint32_t* words;
   uint32_t wfull, end_byte, cur, nxt, raw2, wi, off;
@@ -219,7 +216,8 @@ struct CJCkpt {
 // DC and AC symbols of all lanes take the same instructions; a block ends
 // when the position passes 62 (EOB and invalid symbols advance by >= 64).
 // The DC symbol's window is kept and its difference added when the block
-// ends.  Symbol for symbol this is cj_block: a failing block is counted and
+// ends.  Symbol for symbol this is the serial T.81 block decode
+// (src/decodeScanGPU.cu:78-100): a failing block is counted and
 // decoding goes on after the bits the failing symbol consumed.
 //
 // Checkpoints (`ck`, CJ_CKPTS of them) are written for every decode.  A
@@ -373,13 +371,6 @@ __device__ __forceinline__ CJAgg5 cj_op(const CJAgg5& x, const CJAgg5& y) {
   return r;
 }
 
-struct CJCoefSink {
-  int16_t* blk;
-  __device__ __forceinline__ void operator()(int idx, int32_t v) const {
-    if (idx) blk[idx] = (int16_t)v;
-  }
-};
-
 // Segmented exclusive prefix, over the lanes of a warp, of each lane's blocks
 // and DC sums: from the last segment head at or before the lane, plus the
 // carry from earlier warps (cn, c0..c2) when the segment began before this warp.
@@ -415,31 +406,6 @@ __device__ __forceinline__ void cj_warp_prefix(const CJSubRec& r, const CJLane& 
   *d2 = e3;
 }
 
-// Zero, with coalesced 16-byte stores, the int16 blocks [first, end) that
-// each lane of this warp is about to write (inactive lanes pass active =
-// false); in a valid stream these ranges are contiguous across the warp.
-// Callers clamp every range to its segment, so a corrupt stream cannot reach
-// past the image.  All 32 lanes call this; the writes are visible to the warp
-// after it.
-__device__ __forceinline__ void cj_warp_zero_range(int16_t* __restrict__ coef, bool active, int64_t first,
-                                                   int64_t end) {
-  const int lane = threadIdx.x & 31;
-  const bool any = active && first < end;
-  long long lo = any ? first : LLONG_MAX, hi = any ? end : LLONG_MIN;
-#pragma unroll
-  for (int d = 16; d; d >>= 1) {
-    lo = min(lo, __shfl_xor_sync(CJ_FULL, lo, d));
-    hi = max(hi, __shfl_xor_sync(CJ_FULL, hi, d));
-  }
-  // no range at all: lo and hi keep their sentinels (lo * 8 would wrap)
-  if (lo < hi) {
-    uint4* p = reinterpret_cast<uint4*>(coef);
-    const uint4 z = make_uint4(0, 0, 0, 0);
-    for (long long q = lo * 8 + lane; q < hi * 8; q += 32) p[q] = z;
-  }
-  __syncwarp();
-}
-
 // Blocks lane `ln` writes from block `first`: to its block count, or to its
 // segment's last block for the segment's last lane; clamped to the segment.
 __device__ __forceinline__ int64_t cj_lane_write_end(const CJLane& ln, const CJSegment& seg, const CJSubRec& r,
@@ -450,7 +416,7 @@ __device__ __forceinline__ int64_t cj_lane_write_end(const CJLane& ln, const CJS
 }
 
 // Warp-cooperative write-out of 32 units (one per lane; `active` = false for
-// lanes without one), symbol for symbol the decode of cj_write_lane with the
+// lanes without one), symbol for symbol the serial block decode with the
 // same structural checks.  Each lane builds its current block in its own
 // 64-entry int16 buffer in shared memory (`wbuf` + lane * 64, all zero on
 // entry and on return).  After every symbol the warp stores the blocks its
@@ -458,7 +424,7 @@ __device__ __forceinline__ int64_t cj_lane_write_end(const CJLane& ln, const CJS
 // 16-byte store each -- a whole 128-byte line per block instead of one
 // scattered 2-byte store per coefficient -- and clears those buffers.  Blocks
 // go to memory whole, so the range needs no zero fill; a unit that stops at
-// an error stores its partial block (as cj_write_lane leaves it) and zeroes
+// an error stores its partial block (as the serial decode leaves it) and zeroes
 // the rest of its range, up to `zero_end`.
 __device__ __forceinline__ void cj_write_units_warp(const CJScanParams& sp, const CJSteps& T, const uint32_t* words,
                                                     const CJLane& ln, const CJSegment& seg, uint64_t start,
@@ -577,94 +543,5 @@ __device__ __forceinline__ void cj_write_units_warp(const CJScanParams& sp, cons
     uint4* p = reinterpret_cast<uint4*>(coef + x * 64);
 #pragma unroll
     for (int i = 0; i < 8; i++) p[i] = make_uint4(0, 0, 0, 0);
-  }
-}
-
-// Final decode of one lane from its settled start: writes quantised int16
-// coefficients (natural order) of its blocks, DC predicted per component,
-// and records structural errors of its restart interval.  `zz` is the
-// zig-zag -> natural index table (64 entries, in shared memory).  A part of
-// a lane (a unit) starts at one of its checkpoints (`start`, its first block
-// and DC predictors) and stops at the block boundary `stop`, the next
-// checkpoint; stop = ~0 runs to the lane's end.
-__device__ __forceinline__ void cj_write_lane(const CJScanParams& sp, const CJSteps& T, const uint32_t* words,
-                                              const CJLane& ln, const CJSegment& seg,
-                                              uint64_t start, int64_t first_block, int dc0,
-                                              int dc1, int dc2, int16_t* __restrict__ coef,
-                                              CJStatus* st, const uint8_t* zz, uint64_t stop) {
-  int64_t b = first_block;
-  const int64_t bend = seg.first_block + seg.nblocks;
-  const uint64_t seg_end = seg.bit_end;
-  CJFBits br;
-  br.init(words, ln.end_byte, cj_state_bit(start));
-  uint32_t m = cj_state_phase(start);
-  const int bpm = sp.bpm;
-  const uint64_t pack = sp.phase_pack;
-  int c;
-  uint32_t aslot, slot;
-  cj_phase(sp, bpm, pack, m, c, slot, aslot);
-  int k = -1;
-  int32_t dd = 0;
-  int16_t* blk = coef;
-  // the structural checks made before every block; false = stop here
-  auto block_start = [&]() -> bool {
-    const uint64_t p = br.pos();
-    if (p >= stop) return false;  // the next unit's first block
-    if (!ln.last && p >= ln.end) return false;
-    if (b >= bend) {
-      if (!ln.last) cj_raise_dec(st, b, CJ_DEV_EXTRA);
-      else if (seg.marker_follows) {
-        if (((p + 7) >> 3) != ln.end_byte) cj_raise_dec(st, b, CJ_DEV_TRAILING);
-      } else if (ln.end_byte > ((p + 7) >> 3) + 2) {
-        cj_raise_dec(st, b, CJ_DEV_TRAILING);
-      }
-      return false;
-    }
-    if (seg.marker_follows && p >= seg_end) {
-      cj_raise_dec(st, b, CJ_DEV_OVERRUN);
-      return false;
-    }
-    blk = coef + b * 64;  // zeroed beforehand by cj_warp_zero_range
-    return true;
-  };
-  if (!block_start()) return;
-  for (;;) {
-    const uint32_t v = br.peek();
-    const uint32_t stp = cj_step(T, sp, slot, v);
-    const uint32_t dk = (stp >> 5) & 127, size = stp >> 12, total = stp & 31;
-    const int kn = k + (int)dk;
-    const uint32_t len = total - size;
-    const int32_t val = size ? cj_extend((v << len) >> (32 - size), size) : 0;
-    if (k < 0) dd = val;
-    else if (size && kn <= 63) blk[zz[kn]] = (int16_t)val;
-    br.skip(total - (kn > 63 ? size : 0u));
-    slot = aslot;
-    if (kn < 63) {
-      k = kn;
-      continue;
-    }
-    if (kn > 63 && dk != CJ_STEP_EOB) {  // failing symbol: the block is cut here
-      cj_raise_dec(st, b, dk == CJ_STEP_NO_CODE ? CJ_DEV_BAD_CODE : CJ_DEV_BAD_AC);
-      return;
-    }
-    // block complete
-    if (seg.marker_follows && br.pos() > seg_end) {
-      cj_raise_dec(st, b, CJ_DEV_OVERRUN);
-      return;
-    }
-    int dcv;
-    if (c == 0) dcv = dc0 += dd;
-    else if (c == 1) dcv = dc1 += dd;
-    else dcv = dc2 += dd;
-    if (dcv < -32768 || dcv > 32767) {
-      cj_raise_dec(st, b, CJ_DEV_DC_RANGE);
-      return;
-    }
-    blk[0] = (int16_t)dcv;
-    b++;
-    m = (m + 1 == (uint32_t)bpm) ? 0 : m + 1;
-    cj_phase(sp, bpm, pack, m, c, slot, aslot);
-    k = -1;
-    if (!block_start()) return;
   }
 }
