@@ -61,7 +61,7 @@
 struct CJImageHeader {
   uint8_t counts[4][16];    // DHT BITS per table slot
   uint8_t symbols[4][256];  // DHT HUFFVAL per table slot
-  uint8_t dq[4][64];        // DQT, zig-zag order
+  uint16_t dq[4][64];       // DQT (8- or 16-bit values), zig-zag order
   uint8_t comp_dc[3], comp_ac[3], comp_q[3], comp_sx[3], comp_sy[3];
   uint8_t nch, huff_mask, xshift, yshift, pad[4];
   int32_t mcux, mcuy, width, height, hmax, vmax, restart_interval, nseg_expected;

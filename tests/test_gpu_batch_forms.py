@@ -36,7 +36,7 @@ def f64_plane(oracle_mod, ref, c):
     plane = np.zeros((comp.rows, comp.stride), np.float64)
     blocks = s.reshape(-1, 8, 8)
     for y in range(8):
-        plane[by * 8 + y, bx[:, None] * 8 + np.arange(8)[None, :]] = blocks[:, y, :]
+        plane[(by * 8 + y)[:, None], bx[:, None] * 8 + np.arange(8)[None, :]] = blocks[:, y, :]
     return plane[: comp.height, : comp.width]
 
 
