@@ -281,33 +281,15 @@ struct CJTcState {
   const float* basis;
 };
 
-// FP32 CUDA-core iDCT rows 4h..4h+3 of one block (its int16 coefficients and
-// int32 dequantisation table): out[8y+x], y = 0..3.  The range fallback of
-// the tensor-core form, for blocks whose dequantised values FP16 cannot hold
-// exactly.
-static __device__ __noinline__ void cj_block_f32_half(const int16_t* blk, const int32_t* q, int h, const float* basis,
-                                               float* out) {
-  float t[64];
-  for (int v = 0; v < 8; v++) {
-    int in[8];
-    for (int u = 0; u < 8; u++) in[u] = (int)blk[8 * v + u] * q[8 * v + u];
-    cj_idct8_f32(in, basis, t + 8 * v);
-  }
-  for (int y = 0; y < 4; y++)
-    for (int x = 0; x < 8; x++) {
-      float s = 0.f;
-      for (int v = 0; v < 8; v++) s = fmaf(t[8 * v + x], basis[v * 8 + 4 * h + y], s);
-      out[8 * y + x] = s;
-    }
-}
-
 // Tensor-core iDCT of a tile's blocks (at most 64, rows of a 128-row A tile)
 // into the plane tiles.  A row kb = block kb's 64 coefficients dequantised in
-// FP16 (exact below 2048; a block row at or above it flags the block, whose
-// pixels then come from the FP32 fallback); thread 0 issues the 8 MMAs of
-// D = A Khi + A Klo; the epilogue reads D row kb (block kb) from tensor
-// memory -- warps w and w + 4 share lanes 32 (w & 3) .. +31 and take pixel
-// rows 0-3 and 4-7 -- rounds, level-shifts, clips and stores the bytes.
+// FP16 (exact below 2048; a block row at or above it flags the block);
+// thread 0 issues the 8 MMAs of D = A Khi + A Klo; the epilogue reads D row
+// kb (block kb) from tensor memory -- warps w and w + 4 share lanes
+// 32 (w & 3) .. +31 and take pixel rows 0-3 and 4-7 -- rounds,
+// level-shifts, clips and stores the bytes.  Flagged blocks are then redone
+// on CUDA cores in FP32 by the whole CTA (one thread per pixel), a branch
+// the CTA takes together, so the common path carries no call and no spills.
 // Returns false if the MMAs did not complete within the wait bound
 // (recorded).  Ends with a barrier.
 __device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, const int16_t* sc, uint8_t* smem,
@@ -349,8 +331,6 @@ __device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, c
   float d[32];
   tc_ld32(tc.tmem + ((uint32_t)(32 * (w & 3)) << 16) + 32u * h, d);
   if (kb < nblk) {
-    if (*reinterpret_cast<const uint64_t*>(big + kb * 8))
-      cj_block_f32_half(sc + kb * 64, P.q[P.bq[kb]], h, tc.basis, d);
     const int ps = P.bc[kb] == 0 ? g.y_stride : g.c_stride;
     uint8_t* dst = smem + P.boff[kb] + 4 * h * ps;
 #pragma unroll
@@ -360,7 +340,26 @@ __device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, c
                      tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
+  const bool flagged = kb < nblk && h == 0 && *reinterpret_cast<const uint64_t*>(big + kb * 8) != 0;
+  if (__syncthreads_or(flagged)) {  // rare: FP32 redo of the flagged blocks
+    for (int k = 0; k < nblk; k++) {
+      if (!*reinterpret_cast<const uint64_t*>(big + k * 8)) continue;  // the same for every thread
+      if (threadIdx.x < 64) {
+        const int y = threadIdx.x >> 3, x = threadIdx.x & 7;
+        const int16_t* blk = sc + k * 64;
+        const int32_t* q = P.q[P.bq[k]];
+        float acc = 0.f;
+        for (int v = 0; v < 8; v++) {
+          float row = 0.f;
+          for (int u = 0; u < 8; u++) row = fmaf((float)(blk[8 * v + u] * q[8 * v + u]), tc.basis[u * 8 + x], row);
+          acc = fmaf(row, tc.basis[v * 8 + y], acc);
+        }
+        const int ps = P.bc[k] == 0 ? g.y_stride : g.c_stride;
+        smem[P.boff[k] + y * ps + x] = (uint8_t)cj_clip8(__float2int_rn(acc) + 128);
+      }
+    }
+    __syncthreads();
+  }
   return true;
 }
 

@@ -188,10 +188,12 @@ __device__ __forceinline__ void tc_fetch(const CJPlaneArgs& a, int64_t t, TcRows
 // thread 0 issues the 8 MMAs, and -- while they run and during the epilogue
 // -- every thread already has the loads of its block of the CTA's next tile
 // in flight (register prefetch).  The epilogue reads the block's row of D
-// from tensor memory in two halves of 32 values (pixel rows 0-3, 4-7);
-// flagged blocks take the FP32 CUDA-core fallback for those rows.
+// from tensor memory in two halves of 32 values (pixel rows 0-3, 4-7).
+// Flagged blocks are listed in shared memory and redone afterwards by the
+// whole CTA on CUDA cores in FP32 (one thread per output pixel), a branch the
+// CTA takes together, so the common path carries no call and no spills.
 template <bool RAW>
-__global__ void __launch_bounds__(TC_THREADS, 5) k_idct_tc(CJPlaneArgs a, const uint16_t* __restrict__ basis,
+__global__ void __launch_bounds__(TC_THREADS, 4) k_idct_tc(CJPlaneArgs a, const uint16_t* __restrict__ basis,
                                                           float* raw_out, int* status) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t bar;
@@ -199,6 +201,7 @@ __global__ void __launch_bounds__(TC_THREADS, 5) k_idct_tc(CJPlaneArgs a, const 
   __shared__ int16_t q[64];
   __shared__ int32_t q32[64];
   __shared__ float sbasis[64];
+  __shared__ int s_nbig, s_big[TC_M];
   uint8_t* sA = smem;               // 128 x 64 fp16 = 16 KiB
   uint8_t* sB = smem + 16384;       // Khi, Klo: 2 x 64 x 64 fp16 = 16 KiB
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -217,6 +220,7 @@ __global__ void __launch_bounds__(TC_THREADS, 5) k_idct_tc(CJPlaneArgs a, const 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
   const uint32_t aaddr = cj_smem_addr(sA), baddr = cj_smem_addr(sB);
+  if (tid == 0) s_nbig = 0;
   const int64_t ntiles = (a.nblocks + TC_M - 1) / TC_M;
   uint32_t parity = 0;
   TcRows nx;
@@ -238,6 +242,7 @@ __global__ void __launch_bounds__(TC_THREADS, 5) k_idct_tc(CJPlaneArgs a, const 
       }
       *reinterpret_cast<uint4*>(sA + tc_core_off(tid, k8 * 8)) = make_uint4(h[0], h[1], h[2], h[3]);
     }
+    if (big && cur.live) s_big[atomicAdd(&s_nbig, 1)] = tid;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) tc_idct_mmas(tmem, aaddr, baddr, cj_smem_addr(&bar));
@@ -257,7 +262,6 @@ __global__ void __launch_bounds__(TC_THREADS, 5) k_idct_tc(CJPlaneArgs a, const 
       float d[32];
       tc_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 32u * h, d);
       if (!cur.live) continue;
-      if (big) cj_block_f32_half(a.coef + cur.gb * 64, q32, h, sbasis, d);
       if (RAW) {
         float4* o = reinterpret_cast<float4*>(raw_out + (cur.gb * 64 + 32 * h));
 #pragma unroll
@@ -272,6 +276,29 @@ __global__ void __launch_bounds__(TC_THREADS, 5) k_idct_tc(CJPlaneArgs a, const 
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();  // TMEM and the A tile are free for the next tile
+    const int nbig = s_nbig;
+    if (nbig) {  // CTA-uniform, rare: FP32 redo of the flagged blocks
+      for (int bi = 0; bi < nbig; bi++) {
+        const int64_t kb = t * TC_M + s_big[bi];
+        int bx = 0, by = 0;
+        const int64_t gb = RAW ? kb : cj_plane_src(a, kb, &bx, &by);
+        if (tid < 64) {
+          const int y = tid >> 3, x = tid & 7;
+          const int16_t* blk = a.coef + gb * 64;
+          float acc = 0.f;
+          for (int v = 0; v < 8; v++) {
+            float row = 0.f;
+            for (int u = 0; u < 8; u++) row = fmaf((float)(blk[8 * v + u] * q32[8 * v + u]), sbasis[u * 8 + x], row);
+            acc = fmaf(row, sbasis[v * 8 + y], acc);
+          }
+          if (RAW) raw_out[gb * 64 + tid] = acc;
+          else a.plane[(int64_t)(by * 8 + y) * a.stride + bx * 8 + x] = (uint8_t)cj_clip8(__float2int_rn(acc) + 128);
+        }
+      }
+      __syncthreads();
+      if (tid == 0) s_nbig = 0;
+      __syncthreads();
+    }
   }
   __syncthreads();
   if (warp == 0) tc_dealloc(tmem, 64);
