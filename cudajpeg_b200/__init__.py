@@ -36,6 +36,9 @@ ERROR_NAMES = {0: "NO_ERROR", 1: "SYNTAX_ERROR", 2: "UNSUPPORTED_ERROR", 3: "OOM
 READER_HOST_COEFFICIENTS = 1
 IDCT_INT, IDCT_F32, IDCT_TC = 0, 1, 2
 OUTPUT_RGB, OUTPUT_PLANAR, OUTPUT_NV12, OUTPUT_RGB_FANCY = 0, 1, 2, 3
+# chroma sampling classes (per-class subsequence sizes)
+SAMPLING_420, SAMPLING_422, SAMPLING_444, SAMPLING_GRAY, SAMPLING_OTHER = 0, 1, 2, 3, 4
+SAMPLING_CLASSES = 5
 
 # Every symbol the C headers in include/ declare (checked by the CPU tests).
 EXPORTED = [
@@ -54,6 +57,7 @@ EXPORTED = [
     "cjServerRelease", "cjServerStats", "cjServerReplay", "cjServerSetTuning",
     "cjBatchSetTuning", "cjBatchGetTuning", "cjBatchAutotune", "cjDebugStepTable",
     "cjBatchCopyCoefficients", "cjBuildInfo", "cjBatchSetWaitLimit", "cjBatchSetOutput",
+    "cjBatchSetSubsequenceBitsFor", "cjBatchGetSubsequenceBitsFor",
     "cjBatchGetOutput", "cjBatchChromaGeometry", "cjBatchDLPack", "cjServerDLPack", "cjDLPackFree",
     "decodeScanCPU", "upsampleAndColourTransformHybrid", "upsampleAndColourTransformGPU",
     "upsampleAndColourTransformCPU",
@@ -146,6 +150,8 @@ def load(build_if_missing: bool = True):
     lib.cjBatchImageGeometry.argtypes = [vp, C.c_int, ip, ip, ip]
     lib.cjBatchSetTuning.argtypes = [vp, C.c_int, C.c_int, C.c_int]
     lib.cjBatchSetWaitLimit.argtypes = [vp, C.c_uint]
+    lib.cjBatchSetSubsequenceBitsFor.argtypes = [vp, C.c_int, C.c_int]
+    lib.cjBatchGetSubsequenceBitsFor.argtypes = [vp, C.c_int]
     lib.cjBatchSetOutput.argtypes = [vp, C.c_int, C.c_int]
     lib.cjBatchGetOutput.argtypes = [vp, ip, ip]
     lib.cjBatchChromaGeometry.argtypes = [vp, C.c_int, ip, ip]
@@ -475,6 +481,12 @@ class Batch:
         if err:
             raise ValueError(f"bad tuning {(sub_bits, decode_ctas_per_sm, pixel_tile_cap)}")
 
+    def set_sub_bits_for(self, sampling_class: int, bits: int):
+        """Subsequence size for one sampling class (SAMPLING_*; 0 = follow
+        the batch-wide size), for batches staged from now on."""
+        if self.lib.cjBatchSetSubsequenceBitsFor(self.ptr, sampling_class, bits):
+            raise ValueError(f"bad subsequence size {bits} for class {sampling_class}")
+
     def set_wait_limit(self, polls: int):
         """Bound each grid-barrier wait of the decode kernel (0 = default)."""
         if self.lib.cjBatchSetWaitLimit(self.ptr, polls):
@@ -490,7 +502,9 @@ class Batch:
     def tuning(self) -> dict:
         a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
         self.lib.cjBatchGetTuning(self.ptr, C.byref(a), C.byref(b), C.byref(c))
-        return {"sub_bits": a.value, "decode_ctas_per_sm": b.value, "pixel_tile_cap": c.value}
+        return {"sub_bits": a.value, "decode_ctas_per_sm": b.value, "pixel_tile_cap": c.value,
+                "sub_bits_class": [self.lib.cjBatchGetSubsequenceBitsFor(self.ptr, k)
+                                   for k in range(SAMPLING_CLASSES)]}
 
     def autotune(self, blob_ptr: int, offsets: np.ndarray, sizes: np.ndarray, reps: int = 3) -> dict:
         """Time the batch under every candidate tuning (cjBatchAutotune) and
@@ -500,14 +514,14 @@ class Batch:
         self._keep = (offsets, sizes)
         self.n = len(sizes)
         best = C.c_float(0.0)
-        trials = (C.c_float * 32)()
+        trials = (C.c_float * 64)()
         err = self.lib.cjBatchAutotune(self.ptr, self.n, C.c_void_p(blob_ptr), offsets.ctypes.data,
-                                       sizes.ctypes.data, reps, C.byref(best), trials, 32)
+                                       sizes.ctypes.data, reps, C.byref(best), trials, 64)
         if err:
             raise DecodeError(err, "cjBatchAutotune")
         out = self.tuning()
         out["best_ms"] = round(best.value, 4)
-        out["trials_ms"] = [round(trials[k], 4) for k in range(15)]
+        out["trials_ms"] = [round(trials[k], 4) for k in range(64) if trials[k] > 0]
         return out
 
 

@@ -1086,6 +1086,7 @@ struct CJBatch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // tuning (cjBatchSetTuning / cjBatchAutotune)
   int sub_bits = BT_SUB_BITS_DEFAULT;
+  int sub_bits_class[CJ_SAMPLING_CLASSES] = {0, 0, 0, 0, 0};  // 0: sub_bits
   int decode_ctas = BT_DECODE_CTAS_DEFAULT;  // decode-kernel CTAs per SM (3, 4 or 5)
   int tile_cap = 0;                          // max MCUs per pixel tile (0 = layout maximum)
   unsigned wait_limit = 0;                   // grid-barrier polls before a timeout (0 = default)
@@ -1266,9 +1267,42 @@ void cjBatchDestroy(CJBatch* b) {
   delete b;
 }
 
+}  // extern "C"
+
+// Sampling class of an image (CJ_SAMPLING_*).
+static int bt_sampling_class(const CJImageHeader& h) {
+  if (h.nch == 1) return CJ_SAMPLING_GRAY;
+  if (h.comp_sx[1] != 1 || h.comp_sy[1] != 1 || h.comp_sx[2] != 1 || h.comp_sy[2] != 1) return CJ_SAMPLING_OTHER;
+  if (h.comp_sx[0] == 2 && h.comp_sy[0] == 2) return CJ_SAMPLING_420;
+  if (h.comp_sx[0] == 2 && h.comp_sy[0] == 1) return CJ_SAMPLING_422;
+  if (h.comp_sx[0] == 1 && h.comp_sy[0] == 1) return CJ_SAMPLING_444;
+  return CJ_SAMPLING_OTHER;
+}
+
+static int bt_sub_bits_for(const CJBatch* b, const CJImageHeader& h) {
+  const int c = b->sub_bits_class[bt_sampling_class(h)];
+  return c ? c : b->sub_bits;
+}
+
+static bool bt_sub_bits_ok(int bits) { return bits >= 128 && bits <= 65536 && !(bits & 31); }
+
+extern "C" {
+
+int cjBatchSetSubsequenceBitsFor(CJBatch* b, int sampling_class, int bits) {
+  if (!b || sampling_class < 0 || sampling_class >= CJ_SAMPLING_CLASSES) return PROGRAMMER_ERROR;
+  if (bits && !bt_sub_bits_ok(bits)) return PROGRAMMER_ERROR;
+  b->sub_bits_class[sampling_class] = bits;
+  return 0;
+}
+
+int cjBatchGetSubsequenceBitsFor(const CJBatch* b, int sampling_class) {
+  if (!b || sampling_class < 0 || sampling_class >= CJ_SAMPLING_CLASSES) return PROGRAMMER_ERROR;
+  return b->sub_bits_class[sampling_class] ? b->sub_bits_class[sampling_class] : b->sub_bits;
+}
+
 int cjBatchSetSubsequenceBits(CJBatch* b, int bits) {
   if (bits == 0) bits = BT_SUB_BITS_DEFAULT;
-  if (bits < 128 || bits > 65536 || (bits & 31)) return PROGRAMMER_ERROR;
+  if (!b || !bt_sub_bits_ok(bits)) return PROGRAMMER_ERROR;
   b->sub_bits = bits;
   return 0;
 }
@@ -1362,8 +1396,8 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
     d.seg0 = nseg;
     d.seg_cap = h.nseg_expected;
     nseg += d.seg_cap;
-    d.sub_bits = b->sub_bits;
-    int sub_cap = (int)((sl * 8 + b->sub_bits - 1) / b->sub_bits) + h.nseg_expected + 1;
+    d.sub_bits = bt_sub_bits_for(b, h);
+    int sub_cap = (int)((sl * 8 + d.sub_bits - 1) / d.sub_bits) + h.nseg_expected + 1;
     sub_cap = (sub_cap + 31) & ~31;
     d.sub0 = nsubw * 32;
     d.sub_cap = sub_cap;
@@ -1457,7 +1491,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
 }
 
 static CJBatchArgs bt_args(const CJBatch* b) {
-  CJBatchArgs a;
+  CJBatchArgs a{};
   a.hdr = (const CJImageHeader*)b->hdr.p;
   a.desc = (const CJImageDesc*)b->desc.p;
   a.prm = (CJScanParams*)b->prm.p;
@@ -1779,7 +1813,8 @@ int cjBatchAutotune(CJBatch* b, int n, const unsigned char* blob, const int64_t*
     if (trials_ms && trial < max_trials) trials_ms[trial] = ms;
     trial++;
   };
-  // 1. subsequence size x decode-kernel occupancy
+  // 1. subsequence size x decode-kernel occupancy (one size for every class)
+  for (int k = 0; k < CJ_SAMPLING_CLASSES; k++) b->sub_bits_class[k] = 0;
   for (int sb : subs)
     for (int c : ctas) {
       b->sub_bits = sb;
@@ -1795,9 +1830,38 @@ int cjBatchAutotune(CJBatch* b, int n, const unsigned char* blob, const int64_t*
         best_c = c;
       }
     }
-  // 2. pixel tile width at the best entropy configuration
+  // 1b. per sampling class holding at least 1/16 of the scan bytes: other
+  // sizes for that class alone, the others at their best so far
   b->sub_bits = best_s;
   b->decode_ctas = best_c;
+  b->tile_cap = 0;
+  int64_t cls_bytes[CJ_SAMPLING_CLASSES] = {0, 0, 0, 0, 0}, all_bytes = 0;
+  {
+    const CJImageHeader* hh = (const CJImageHeader*)b->h_hdr.p;  // the last stage's images
+    const CJImageDesc* dd = (const CJImageDesc*)b->h_desc.p;
+    for (int k = 0; k < b->n_dev; k++) {
+      cls_bytes[bt_sampling_class(hh[k])] += dd[k].raw_len;
+      all_bytes += dd[k].raw_len;
+    }
+  }
+  for (int c = 0; c < CJ_SAMPLING_CLASSES; c++) {
+    if (cls_bytes[c] * 16 < all_bytes) continue;
+    int best_c_bits = 0;
+    for (int sb : {1024, 2048, 4096, 8192, 16384}) {
+      if (sb == best_s) continue;
+      b->sub_bits_class[c] = sb;
+      float ms = 0.f;
+      int e = bt_time_config(b, n, blob, offsets, sizes, reps, &ms);
+      if (e) return e;
+      record(ms);
+      if (ms < best) {
+        best = ms;
+        best_c_bits = sb;
+      }
+    }
+    b->sub_bits_class[c] = best_c_bits;
+  }
+  // 2. pixel tile width at the best entropy configuration
   for (int cap : {8, 4, 2}) {
     b->tile_cap = cap;
     float ms = 0.f;
@@ -2056,7 +2120,7 @@ extern "C" int cjDecodeNoAlloc(const unsigned char* jpeg, size_t size, unsigned 
   if (per_dec < 1 || per_pix < 1) return UNSUPPORTED_ERROR;
   per_dec = std::min(per_dec, BT_DECODE_CTAS_DEFAULT);
 
-  CJBatchArgs a;
+  CJBatchArgs a{};
   a.hdr = (const CJImageHeader*)(base + o_hdr);
   a.desc = (const CJImageDesc*)(base + o_desc);
   a.prm = (CJScanParams*)(base + o_prm);

@@ -122,6 +122,22 @@ int cjBatchSetSubsequenceBits(CJBatch *b, int bits);
  * 128 pixels across). */
 int cjBatchSetTuning(CJBatch *b, int sub_bits, int decode_ctas_per_sm, int pixel_tile_cap);
 void cjBatchGetTuning(const CJBatch *b, int *sub_bits, int *decode_ctas_per_sm, int *pixel_tile_cap);
+/* Chroma sampling classes of a batch's images (by the sampling factors of
+ * SOF: Y 2x2 / 2x1 / 1x1 with 1x1 chroma, one component, anything else). */
+#define CJ_SAMPLING_420 0
+#define CJ_SAMPLING_422 1
+#define CJ_SAMPLING_444 2
+#define CJ_SAMPLING_GRAY 3
+#define CJ_SAMPLING_OTHER 4
+#define CJ_SAMPLING_CLASSES 5
+/* Bits per speculative subsequence for the images of one sampling class
+ * (staged from now on), overriding cjBatchSetSubsequenceBits for them: the
+ * distance a speculative decode runs before it falls into step differs by
+ * class (4:2:0 scans the longest), and so does the best size.  bits: as
+ * cjBatchSetSubsequenceBits, 0 = follow the batch-wide size.  The getter
+ * returns the size in force for the class. */
+int cjBatchSetSubsequenceBitsFor(CJBatch *b, int sampling_class, int bits);
+int cjBatchGetSubsequenceBitsFor(const CJBatch *b, int sampling_class);
 /* Output of a batch staged from now on.  format: CJ_OUTPUT_RGB (default:
  * interleaved RGB, grey as one plane -- the reference's output),
  * CJ_OUTPUT_PLANAR (the Y plane width*height, then the Cb and Cr planes at
@@ -154,8 +170,11 @@ void cjBatchGetOutput(const CJBatch *b, int *format, int *idct);
 int cjBatchSetWaitLimit(CJBatch *b, unsigned polls);
 /* Autotuner: times the given batch (device time, median of `reps` runs)
  * under every subsequence size in {512, 1024, 2048, 4096} x decode CTAs per
- * SM in {3, 4, 5}, then pixel tile caps {8, 4, 2} at the best of those, and
- * keeps the fastest tuning in `b`.  The batch is left staged under it.
+ * SM in {3, 4, 5}; then, one sampling class of the batch at a time (classes
+ * holding at least 1/16 of its scan bytes), the sizes {1024 .. 16384} other
+ * than the batch-wide best for that class alone; then pixel tile caps
+ * {8, 4, 2}; and keeps the fastest tuning in `b` (per-class sizes equal to
+ * the batch-wide one are stored as 0).  The batch is left staged under it.
  * trials_ms (may be NULL) receives up to max_trials timings in that order;
  * *best_ms (may be NULL) the best. */
 int cjBatchAutotune(CJBatch *b, int n, const unsigned char *blob, const int64_t *offsets,

@@ -160,10 +160,17 @@ def test_decode_steps_match_reference_lut(cj):
 def test_batch_tuning_validation_without_gpu(cj):
     """cjBatchSetTuning checks its arguments on the host (no device work)."""
     with cj.Batch() as b:
-        assert b.tuning() == {"sub_bits": 4096, "decode_ctas_per_sm": 4, "pixel_tile_cap": 0}
+        assert b.tuning() == {"sub_bits": 4096, "decode_ctas_per_sm": 4, "pixel_tile_cap": 0,
+                              "sub_bits_class": [4096] * 5}
         b.set_tuning(2048, 5, 4)
-        assert b.tuning() == {"sub_bits": 2048, "decode_ctas_per_sm": 5, "pixel_tile_cap": 4}
+        b.set_sub_bits_for(cj.SAMPLING_420, 8192)
+        assert b.tuning() == {"sub_bits": 2048, "decode_ctas_per_sm": 5, "pixel_tile_cap": 4,
+                              "sub_bits_class": [8192, 2048, 2048, 2048, 2048]}
         for bad in [(100, 4, 0), (1000, 4, 0), (1024, 7, 0), (1024, 2, 0), (1024, 4, 3), (1024, 4, -2)]:
             with pytest.raises(ValueError):
                 b.set_tuning(*bad)
+        for cls, bits in [(cj.SAMPLING_420, 96), (cj.SAMPLING_GRAY, 1000), (5, 1024), (-1, 1024)]:
+            with pytest.raises(ValueError):
+                b.set_sub_bits_for(cls, bits)
         assert b.tuning()["sub_bits"] == 2048  # a rejected call changes nothing
+        assert b.tuning()["sub_bits_class"][cj.SAMPLING_420] == 8192

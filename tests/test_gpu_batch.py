@@ -88,7 +88,30 @@ def test_tuning_variants_identical(cj, oracle_mod, sub_bits, ctas, cap):
     with cj.Batch() as b:
         b.set_tuning(sub_bits, ctas, cap)
         imgs, errs = b.decode(files)
-        assert b.tuning() == {"sub_bits": sub_bits, "decode_ctas_per_sm": ctas, "pixel_tile_cap": cap}
+        t = b.tuning()
+        assert (t["sub_bits"], t["decode_ctas_per_sm"], t["pixel_tile_cap"]) == (sub_bits, ctas, cap)
+        assert t["sub_bits_class"] == [sub_bits] * cj.SAMPLING_CLASSES
+    for k, data in enumerate(files):
+        ref = oracle_mod.decode(data)
+        assert errs[k] == ref.error, k
+        if ref.error == 0:
+            assert np.array_equal(imgs[k], ref.pixels), k
+
+
+def test_per_class_subsequence_sizes(cj, oracle_mod):
+    """A different subsequence size per sampling class in one batch (4:2:0
+    long, grey short, 4:4:4 and 4:2:2 in between): results unchanged."""
+    files = [s.data for s in W.mixed_batch(n=24, seed=14, max_side=900)]
+    with cj.Batch() as b:
+        for cls, bits in ((cj.SAMPLING_420, 16384), (cj.SAMPLING_GRAY, 256), (cj.SAMPLING_444, 8192),
+                          (cj.SAMPLING_422, 1024)):
+            b.set_sub_bits_for(cls, bits)
+        with pytest.raises(ValueError):
+            b.set_sub_bits_for(cj.SAMPLING_420, 100)
+        assert b.tuning()["sub_bits_class"] == [16384, 1024, 8192, 256, 4096]
+        imgs, errs = b.decode(files)
+        b.set_sub_bits_for(cj.SAMPLING_420, 0)
+        assert b.tuning()["sub_bits_class"][cj.SAMPLING_420] == 4096
     for k, data in enumerate(files):
         ref = oracle_mod.decode(data)
         assert errs[k] == ref.error, k
@@ -102,6 +125,7 @@ def test_autotune_keeps_results(cj, oracle_mod):
     with cj.Batch() as b:
         res = b.autotune(blob.ctypes.data, offsets, sizes, reps=1)
         assert res["sub_bits"] in (512, 1024, 2048, 4096)
+        assert all(x in (512, 1024, 2048, 4096, 8192, 16384) for x in res["sub_bits_class"])
         assert res["decode_ctas_per_sm"] in (3, 4, 5)
         assert res["best_ms"] > 0 and min(t for t in res["trials_ms"] if t > 0) == pytest.approx(res["best_ms"])
         b.run()
