@@ -1482,9 +1482,12 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
               CUDA_KERNEL_LAUNCH_ERROR);
   if (per_sm < 1) return UNSUPPORTED_ERROR;
   b->grid = std::min(per_sm, b->decode_ctas) * b->sm_count;
-  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                  &per_sm, (const void*)bt_pixel_kernel(b->idct, bt_pix_format(b)), CJ_PIX_THREADS, b->smem_pix),
-              CUDA_KERNEL_LAUNCH_ERROR);
+  const void* pk = (const void*)bt_pixel_kernel(b->idct, bt_pix_format(b));
+  if (b->idct == CJ_PIX_IDCT_TC)  // 64 tensor-memory columns per CTA
+    per_sm = cj_tc_ctas_per_sm(pk, CJ_PIX_THREADS, b->smem_pix, 64);
+  else
+    CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pk, CJ_PIX_THREADS, b->smem_pix),
+                CUDA_KERNEL_LAUNCH_ERROR);
   if (per_sm < 1) return UNSUPPORTED_ERROR;
   b->grid_pix = std::min(nptiles, per_sm * b->sm_count);
   return 0;

@@ -16,7 +16,38 @@
 // SBO (next 8-row group) = 1024 B.
 #pragma once
 #include <cuda_fp16.h>
+#include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
+
+// CTAs per SM of a kernel that allocates `tmem_cols` tensor-memory columns
+// per CTA, launched with `threads` threads and `dyn_smem` bytes of dynamic
+// shared memory.  The runtime's occupancy query answers 1 for every kernel
+// that contains tcgen05 instructions (it cannot know how many columns a CTA
+// takes), so the residency is worked out here from the kernel's registers
+// and static shared memory and the SM's limits: registers (allocated per
+// warp in units of 256), shared memory (plus the per-CTA reservation),
+// threads, CTA slots, and the 512 columns of tensor memory.  Returns 0 if
+// an attribute cannot be read.
+static inline int cj_tc_ctas_per_sm(const void* kernel, int threads, size_t dyn_smem, int tmem_cols) {
+  cudaFuncAttributes at;
+  int dev = 0, regs_sm = 0, smem_sm = 0, smem_rsv = 0, thr_sm = 0, blk_sm = 0;
+  if (cudaFuncGetAttributes(&at, kernel) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&blk_sm, cudaDevAttrMaxBlocksPerMultiprocessor, dev) != cudaSuccess)
+    return 0;
+  const int warps = (threads + 31) / 32;
+  const int regs_warp = ((at.numRegs * 32 + 255) / 256) * 256;
+  int n = std::min(thr_sm / (warps * 32), blk_sm);
+  if (regs_warp > 0) n = std::min(n, regs_sm / (regs_warp * warps));
+  n = std::min(n, (int)((size_t)smem_sm / (at.sharedSizeBytes + dyn_smem + (size_t)smem_rsv)));
+  if (tmem_cols > 0) n = std::min(n, 512 / tmem_cols);
+  return std::max(n, 0);
+}
 
 __device__ __forceinline__ uint32_t tc_core_off(int r, int k) {
   return (uint32_t)((((r >> 3) * 8 + (k >> 3)) * 128) + (r & 7) * 16 + (k & 7) * 2);

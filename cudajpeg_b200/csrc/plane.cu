@@ -347,14 +347,11 @@ static int cj_idct_tc_launch(const CJPlaneArgs& a, float* raw, bool is_raw, cuda
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int64_t ntiles = (a.nblocks + TC_M - 1) / TC_M;
-  // CTAs per SM: as many as shared memory and registers allow, at most 7 so
-  // that their tensor-memory columns (64 each) stay within the SM's 512
-  int per_sm = 0;
-  CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, is_raw ? (const void*)k_idct_tc<true>
-                                                                              : (const void*)k_idct_tc<false>,
-                                                            TC_THREADS, smem),
-              CUDA_KERNEL_LAUNCH_ERROR);
-  per_sm = std::max(1, std::min(per_sm, 7));
+  // CTAs per SM: as many as registers, shared memory and tensor memory (64
+  // columns each) allow
+  int per_sm = cj_tc_ctas_per_sm(is_raw ? (const void*)k_idct_tc<true> : (const void*)k_idct_tc<false>, TC_THREADS,
+                                 smem, 64);
+  if (per_sm < 1) return CUDA_KERNEL_LAUNCH_ERROR;
   unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)sms * per_sm);
   if (grid < 1) grid = 1;
   if (is_raw)
