@@ -550,9 +550,12 @@ def run_batch(args, wl, world, rank, local, dist):
                                                      / (total_ms / 1e3) / 1e6, 1),
                            passes=st["passes"], grid_ctas=st["grid"], warp_items=st["warp_items"],
                            pixel_ctas=st["pixel_grid"],
-                           tuning={k: tune[k] for k in ("sub_bits", "decode_ctas_per_sm", "pixel_tile_cap")},
+                           tuning={k: tune[k] for k in ("sub_bits", "decode_ctas_per_sm", "pixel_tile_cap",
+                                                        "sub_bits_class") if k in tune},
                            autotune=({"best_ms": tune["best_ms"], "trials_ms": tune["trials_ms"],
-                                      "order": "sub_bits {512,1024,2048,4096} x ctas {3,4,5}, "
+                                      "order": "sub_bits {512,1024,2048,4096} x ctas {3,4,5}, then per "
+                                               "sampling class (4:2:0, 4:2:2, 4:4:4, grey, other; classes "
+                                               "with >= 1/16 of the scan bytes) sub_bits {1024..16384}, "
                                                "then tile cap {8,4,2}"}
                                      if "best_ms" in tune else None)),
             "e2e": {"value": round(e2e_value, 2), "unit": "MPix/s",

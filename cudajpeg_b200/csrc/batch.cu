@@ -132,6 +132,7 @@ struct CJBatchArgs {
   CJWarpAgg* wagg;
   CJWarpAgg* carry;
   int16_t* coef;
+  const uint16_t* tc_basis;  // tensor-core form: the Kronecker basis (Khi, Klo) to stage per CTA
   uint8_t* out;
   uint8_t* rgb;   // fancy mode: the RGB output (out then holds planar samples)
   int64_t npix;   // fancy mode: pixels of the batch
@@ -872,7 +873,7 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
 // Kronecker basis, built by the CTA, in shared memory.
 template <int MODE, int OUT>
 __global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? 4 : 6) k_pixel_batch(CJBatchArgs a) {
-  extern __shared__ __align__(128) uint8_t smem[];
+  extern __shared__ __align__(1024) uint8_t smem[];  // the swizzled A tile needs 1024-byte alignment
   __shared__ uint64_t bar2[2];
   __shared__ CJPixSmemParams P;
   // a decode kernel whose grid barrier timed out left no settled
@@ -880,7 +881,6 @@ __global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? 4 : 6
   if (__ldcg(&a.ctl->timeout)) return;
   __shared__ uint64_t s_mma_bar;
   __shared__ uint32_t s_tmem;
-  __shared__ double s_b64[64];
   __shared__ float s_b32[64];
   if (threadIdx.x == 0) {
     cj_mbar_init(&bar2[0], 1);
@@ -889,10 +889,25 @@ __global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? 4 : 6
   }
   CJTcState tc;
   if (MODE == CJ_PIX_IDCT_TC) {
+    // the swizzled A tile must start on a 1024-byte boundary of the shared
+    // window; should the launch ever place it elsewhere, the run fails as a
+    // whole (reported like a barrier timeout) instead of computing garbage
+    if (cj_smem_addr(smem + BT_TC_A_OFF) & 1023u) {
+      if (threadIdx.x == 0) atomicExch(&a.ctl->timeout, 1);
+      return;
+    }
     // the A tile starts zeroed (rows past a tile's blocks are never written)
     for (int k = threadIdx.x; k < 16384 / 16; k += blockDim.x)
       reinterpret_cast<uint4*>(smem + BT_TC_A_OFF)[k] = make_uint4(0, 0, 0, 0);
-    tc_build_basis(reinterpret_cast<uint16_t*>(smem + BT_TC_B_OFF), s_b64, s_b32);
+    // the hi/lo Kronecker basis, built once per device, into the B operand
+    const uint4* gb = reinterpret_cast<const uint4*>(a.tc_basis);
+    for (int k = threadIdx.x; k < 16384 / 16; k += blockDim.x)
+      reinterpret_cast<uint4*>(smem + BT_TC_B_OFF)[k] = __ldg(gb + k);
+    // the 8x8 basis B[u][x] in FP32 for the range fallback
+    if (threadIdx.x < 64) {
+      const int u = threadIdx.x >> 3, x = threadIdx.x & 7;
+      s_b32[threadIdx.x] = (float)((u ? 0.5 : 0.5 * sqrt(0.5)) * cospi((double)((2 * x + 1) * u) / 16.0));
+    }
     if ((threadIdx.x >> 5) == 0) tc_alloc(&s_tmem, 64);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1483,6 +1498,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   if (per_sm < 1) return UNSUPPORTED_ERROR;
   b->grid = std::min(per_sm, b->decode_ctas) * b->sm_count;
   const void* pk = (const void*)bt_pixel_kernel(b->idct, bt_pix_format(b));
+  if (b->idct == CJ_PIX_IDCT_TC && !cj_tc_basis_device()) return CUDA_MEM_ERROR;
   if (b->idct == CJ_PIX_IDCT_TC)  // 64 tensor-memory columns per CTA
     per_sm = cj_tc_ctas_per_sm(pk, CJ_PIX_THREADS, b->smem_pix, 64);
   else
@@ -1513,6 +1529,7 @@ static CJBatchArgs bt_args(const CJBatch* b) {
   a.wagg = (CJWarpAgg*)b->wagg.p;
   a.carry = (CJWarpAgg*)b->carry.p;
   a.coef = (int16_t*)b->coef.p;
+  a.tc_basis = b->idct == CJ_PIX_IDCT_TC ? cj_tc_basis_device() : nullptr;
   const bool fancy = b->out_format == CJ_OUT_RGB_FANCY;
   a.out = (uint8_t*)(fancy ? b->fancy.p : b->out.p);
   a.rgb = fancy ? (uint8_t*)b->out.p : nullptr;

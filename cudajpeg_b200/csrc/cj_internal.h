@@ -119,6 +119,11 @@ extern "C" int cj_parse_to_scan(JPGReader* r, const unsigned char* buf, size_t s
 // Map a device status word to a format.h error code (0 = fine).
 int cj_status_error(const CJStatus* st);
 
+// Khi then Klo of the tensor-core iDCT's Kronecker basis (8192 FP16 values in
+// the B operand's core-matrix layout) on the current device, built on first
+// use; nullptr if it could not be allocated.
+const uint16_t* cj_tc_basis_device();
+
 #define CJ_CUDA_TRY(expr, code)                  \
   do {                                           \
     cudaError_t e_ = (expr);                     \

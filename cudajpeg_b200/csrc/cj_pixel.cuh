@@ -283,7 +283,8 @@ struct CJTcState {
 
 // Tensor-core iDCT of a tile's blocks (at most 64, rows of a 128-row A tile)
 // into the plane tiles.  A row kb = block kb's 64 coefficients dequantised in
-// FP16 (exact below 2048; a block row at or above it flags the block);
+// FP16 (exact below 2048; a block row at or above it flags the block), in
+// the 128-byte swizzled layout (conflict-free stores of a block's 8 rows);
 // thread 0 issues the 8 MMAs of D = A Khi + A Klo; the epilogue reads D row
 // kb (block kb) from tensor memory -- warps w and w + 4 share lanes
 // 32 (w & 3) .. +31 and take pixel rows 0-3 and 4-7 -- rounds,
@@ -312,12 +313,13 @@ __device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, c
       acc |= (p[j] & 0x7FFF7FFFu) + 0x18001800u;
     }
     big[t] = (acc & 0x80008000u) != 0;
-    *reinterpret_cast<uint4*>(sA + tc_core_off(kb, v * 8)) = make_uint4(p[0], p[1], p[2], p[3]);
+    // swizzled A rows: the 8 threads of a block row group store to 8 banks
+    *reinterpret_cast<uint4*>(sA + tc_sw128_off(kb, v)) = make_uint4(p[0], p[1], p[2], p[3]);
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncthreads();
   if (threadIdx.x == 0)
-    tc_idct_mmas(tc.tmem, cj_smem_addr(sA), cj_smem_addr(smem + g.b_off), cj_smem_addr(tc.bar));
+    tc_idct_mmas_asw(tc.tmem, cj_smem_addr(sA), cj_smem_addr(smem + g.b_off), cj_smem_addr(tc.bar));
   const bool ok = cj_mbar_wait(tc.bar, tc.parity);
   tc.parity ^= 1u;
   if (!__syncthreads_and(ok)) {
@@ -328,16 +330,21 @@ __device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, c
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kb = 32 * (w & 3) + lane, h = w >> 2;
-  float d[32];
-  tc_ld32(tc.tmem + ((uint32_t)(32 * (w & 3)) << 16) + 32u * h, d);
-  if (kb < nblk) {
-    const int ps = P.bc[kb] == 0 ? g.y_stride : g.c_stride;
-    uint8_t* dst = smem + P.boff[kb] + 4 * h * ps;
+  const bool live = kb < nblk;
+  const int ps = live && P.bc[kb] != 0 ? g.c_stride : g.y_stride;
+  uint8_t* dst = smem + (live ? P.boff[kb] : 0) + 4 * h * ps;
+  // two pixel rows per load (16 columns), to keep the live registers down
 #pragma unroll
-    for (int y = 0; y < 4; y++)
-      *reinterpret_cast<uint2*>(dst + y * ps) =
-          make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
-                     tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
+  for (int j = 0; j < 2; j++) {
+    float d[16];
+    tc_ld16(tc.tmem + ((uint32_t)(32 * (w & 3)) << 16) + 32u * h + 16u * j, d);
+    if (live) {
+#pragma unroll
+      for (int y = 0; y < 2; y++)
+        *reinterpret_cast<uint2*>(dst + (2 * j + y) * ps) =
+            make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
+                       tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   const bool flagged = kb < nblk && h == 0 && *reinterpret_cast<const uint64_t*>(big + kb * 8) != 0;

@@ -58,6 +58,20 @@ __device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr) {
          ((uint64_t)(1024 >> 4) << 32) | (1ull << 46);
 }
 
+// The same K-major operand with the 128-byte swizzle: rows of 128 bytes (the
+// whole K = 64 FP16 row) in 8-row atoms of 1024 bytes (SBO), the 16-byte
+// chunk c of row r stored at chunk c ^ (r & 7).  The atom must start on a
+// 1024-byte boundary; a K step of 16 inside the atom advances the start
+// address by 32 bytes (the swizzle is applied to the absolute address).
+__device__ __forceinline__ uint32_t tc_sw128_off(int r, int chunk) {
+  return (uint32_t)(r * 128 + ((chunk ^ (r & 7)) << 4));
+}
+
+__device__ __forceinline__ uint64_t tc_smem_desc_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+         (2ull << 61);
+}
+
 // kind::f16, D = F32, A = B = F16, both K-major, N = 64, M = 128
 #define TC_IDESC ((1u << 4) | (0u << 7) | (0u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24))
 
@@ -81,6 +95,32 @@ __device__ __forceinline__ void tc_idct_mmas(uint32_t tmem, uint32_t a_addr, uin
     tc_mma(tmem, tc_smem_desc(a_addr + kk * 256), tc_smem_desc(b_addr + 8192 + kk * 256), 1u);
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_addr)
                : "memory");
+}
+
+// tc_idct_mmas with A in the 128-byte swizzled layout (tc_sw128_off).
+__device__ __forceinline__ void tc_idct_mmas_asw(uint32_t tmem, uint32_t a_addr, uint32_t b_addr, uint32_t bar_addr) {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+  for (int kk = 0; kk < 4; kk++)
+    tc_mma(tmem, tc_smem_desc_sw128(a_addr + kk * 32), tc_smem_desc(b_addr + kk * 256), kk > 0);
+#pragma unroll
+  for (int kk = 0; kk < 4; kk++)
+    tc_mma(tmem, tc_smem_desc_sw128(a_addr + kk * 32), tc_smem_desc(b_addr + 8192 + kk * 256), 1u);
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_addr)
+               : "memory");
+}
+
+// 16 consecutive FP32 columns of this thread's tensor-memory lane.
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
 }
 
 __device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v) {
@@ -110,30 +150,6 @@ __device__ __forceinline__ void tc_alloc(uint32_t* slot, uint32_t cols) {
 }
 __device__ __forceinline__ void tc_dealloc(uint32_t tmem, uint32_t cols) {
   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols) : "memory");
-}
-
-// The 8x8 basis B[u][x] in float64 (`b64`) and float (`b32`), then Khi and
-// Klo of the Kronecker basis (row n = pixel 8y+x, column k = coefficient
-// 8v+u) in the B operand's core-matrix layout (`dst`, 8192 halves).  All
-// threads of the CTA; ends with a barrier.
-__device__ __forceinline__ void tc_build_basis(uint16_t* dst, double* b64, float* b32) {
-  for (int i = threadIdx.x; i < 64; i += blockDim.x) {
-    const int u = i >> 3, x = i & 7;
-    const double c = (u ? 0.5 : 0.5 * sqrt(0.5)) * cospi((double)((2 * x + 1) * u) / 16.0);
-    b64[i] = c;
-    b32[i] = (float)c;
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < 4096; e += blockDim.x) {
-    const int n = e >> 6, k = e & 63;
-    const double w = b64[(k >> 3) * 8 + (n >> 3)] * b64[(k & 7) * 8 + (n & 7)];
-    const __half hi = __double2half(w);
-    const __half lo = __double2half(w - (double)__half2float(hi));
-    const uint32_t off = tc_core_off(n, k) >> 1;
-    dst[off] = __half_as_ushort(hi);
-    dst[4096 + off] = __half_as_ushort(lo);
-  }
-  __syncthreads();
 }
 
 // Four iDCT outputs -> the bytes clip(round(v) + 128), v0 in the low byte:

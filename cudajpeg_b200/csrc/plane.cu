@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "../../include/pixelTransformGPU.h"
 #include "cj_internal.h"
@@ -133,16 +134,19 @@ k_idct_raw_f32(const int16_t* __restrict__ coef, const int16_t* __restrict__ qna
   }
 }
 
-static int cj_basis_ready = -1;
+// constant memory is per device: one upload on each
+static bool g_basis_ready[64];
 
 int cj_upload_basis() {
-  if (cj_basis_ready == 1) return 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CUDA_MEM_ERROR;
+  if (g_basis_ready[dev]) return 0;
   float b[64];
   for (int u = 0; u < 8; u++)
     for (int x = 0; x < 8; x++)
       b[u * 8 + x] = (float)((u ? 0.5 : 0.5 / sqrt(2.0)) * cos((2 * x + 1) * u * 3.14159265358979323846 / 16.0));
   CJ_CUDA_TRY(cudaMemcpyToSymbol(c_idct_basis, b, sizeof(b)), CUDA_MEM_ERROR);
-  cj_basis_ready = 1;
+  g_basis_ready[dev] = true;
   return 0;
 }
 
@@ -157,7 +161,10 @@ int cj_upload_basis() {
 #define TC_M 128
 #define TC_THREADS 128
 
-static uint16_t* g_tc_basis = nullptr;  // device: Khi then Klo, core-matrix layout
+// per device: Khi then Klo, core-matrix layout
+#define CJ_MAX_DEVICES 64
+static uint16_t* g_tc_basis_dev[CJ_MAX_DEVICES];
+static std::mutex g_tc_basis_mu;
 
 // One thread's block of a 128-block tile: its 8 coefficient rows as loaded
 // (quantised int16), where it lives and where its pixels go.
@@ -306,8 +313,11 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_idct_tc(CJPlaneArgs a, const 
 
 // Khi / Klo of the Kronecker basis in the K-major core-matrix layout of B
 // (row = pixel n = 8y+x, column = coefficient k = 8v+u).
-static int cj_tc_basis() {
-  if (g_tc_basis) return 0;
+static uint16_t* cj_tc_basis() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= CJ_MAX_DEVICES) return nullptr;
+  std::lock_guard<std::mutex> lock(g_tc_basis_mu);
+  if (g_tc_basis_dev[dev]) return g_tc_basis_dev[dev];
   static uint16_t h[2 * 64 * 64];
   double b[8][8];
   for (int u = 0; u < 8; u++)
@@ -323,28 +333,40 @@ static int cj_tc_basis() {
       h[off] = *reinterpret_cast<uint16_t*>(&hi);
       h[4096 + off] = *reinterpret_cast<uint16_t*>(&lo);
     }
-  CJ_CUDA_TRY(cudaMalloc(&g_tc_basis, sizeof(h)), CUDA_MEM_ERROR);
-  CJ_CUDA_TRY(cudaMemcpy(g_tc_basis, h, sizeof(h), cudaMemcpyHostToDevice), CUDA_MEM_ERROR);
-  return 0;
+  uint16_t* d = nullptr;
+  if (cudaMalloc(&d, sizeof(h)) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(d, h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  g_tc_basis_dev[dev] = d;
+  return d;
 }
 
-static int* g_tc_status = nullptr;
+const uint16_t* cj_tc_basis_device() { return cj_tc_basis(); }
+
+static int* g_tc_status_dev[CJ_MAX_DEVICES];  // per device: set when an MMA wait ran out
 
 static int cj_idct_tc_launch(const CJPlaneArgs& a, float* raw, bool is_raw, cudaStream_t s) {
-  if (cj_upload_basis() || cj_tc_basis()) return CUDA_MEM_ERROR;
-  if (!g_tc_status) {
-    CJ_CUDA_TRY(cudaMalloc(&g_tc_status, sizeof(int)), CUDA_MEM_ERROR);
-    CJ_CUDA_TRY(cudaMemset(g_tc_status, 0, sizeof(int)), CUDA_MEM_ERROR);
+  const uint16_t* basis = cj_tc_basis();
+  if (cj_upload_basis() || !basis) return CUDA_MEM_ERROR;
+  int dev = 0;
+  CJ_CUDA_TRY(cudaGetDevice(&dev), CUDA_MEM_ERROR);
+  int*& status = g_tc_status_dev[dev];  // dev < CJ_MAX_DEVICES: cj_tc_basis checked it
+  if (!status) {
+    CJ_CUDA_TRY(cudaMalloc(&status, sizeof(int)), CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaMemset(status, 0, sizeof(int)), CUDA_MEM_ERROR);
   }
-  static bool attr = false;
+  static bool attr[CJ_MAX_DEVICES];  // function attributes are set per device
   const int smem = 32768;
-  if (!attr) {
-    cudaFuncSetAttribute(k_idct_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_idct_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
+  if (!attr[dev]) {
+    CJ_CUDA_TRY(cudaFuncSetAttribute(k_idct_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                CUDA_KERNEL_LAUNCH_ERROR);
+    CJ_CUDA_TRY(cudaFuncSetAttribute(k_idct_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                CUDA_KERNEL_LAUNCH_ERROR);
+    attr[dev] = true;
   }
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
+  int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int64_t ntiles = (a.nblocks + TC_M - 1) / TC_M;
   // CTAs per SM: as many as registers, shared memory and tensor memory (64
@@ -355,9 +377,9 @@ static int cj_idct_tc_launch(const CJPlaneArgs& a, float* raw, bool is_raw, cuda
   unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)sms * per_sm);
   if (grid < 1) grid = 1;
   if (is_raw)
-    k_idct_tc<true><<<grid, TC_THREADS, smem, s>>>(a, g_tc_basis, raw, g_tc_status);
+    k_idct_tc<true><<<grid, TC_THREADS, smem, s>>>(a, basis, raw, status);
   else
-    k_idct_tc<false><<<grid, TC_THREADS, smem, s>>>(a, g_tc_basis, raw, g_tc_status);
+    k_idct_tc<false><<<grid, TC_THREADS, smem, s>>>(a, basis, raw, status);
   CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
   return 0;
 }
