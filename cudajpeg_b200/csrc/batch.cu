@@ -52,8 +52,6 @@
 #define BT_TILE_BAD (1 << 30)  // flag in a tile's marker count: malformed FF sequence
 // fixed shared-memory offsets of the tensor-core form's A tile and basis
 // (cj_pix_layout with two coefficient buffers)
-#define BT_TC_A_OFF 16384
-#define BT_TC_B_OFF 32768
 
 // ---------------------------------------------------------------- layouts
 
@@ -873,7 +871,7 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
 // Kronecker basis, built by the CTA, in shared memory.
 template <int MODE, int OUT>
 __global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? 4 : 6) k_pixel_batch(CJBatchArgs a) {
-  extern __shared__ __align__(1024) uint8_t smem[];  // the swizzled A tile needs 1024-byte alignment
+  extern __shared__ __align__(128) uint8_t smem[];
   __shared__ uint64_t bar2[2];
   __shared__ CJPixSmemParams P;
   // a decode kernel whose grid barrier timed out left no settled
@@ -889,20 +887,17 @@ __global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? 4 : 6
   }
   CJTcState tc;
   if (MODE == CJ_PIX_IDCT_TC) {
-    // the swizzled A tile must start on a 1024-byte boundary of the shared
-    // window; should the launch ever place it elsewhere, the run fails as a
-    // whole (reported like a barrier timeout) instead of computing garbage
-    if (cj_smem_addr(smem + BT_TC_A_OFF) & 1023u) {
-      if (threadIdx.x == 0) atomicExch(&a.ctl->timeout, 1);
-      return;
-    }
+    // the swizzled A tile starts on the first 1024-byte boundary of its
+    // region (the dynamic shared memory itself need not be so aligned)
+    uint8_t* a_region = smem + CJ_TC_A_OFF;
+    tc.a_tile = a_region + ((1024u - (cj_smem_addr(a_region) & 1023u)) & 1023u);
     // the A tile starts zeroed (rows past a tile's blocks are never written)
     for (int k = threadIdx.x; k < 16384 / 16; k += blockDim.x)
-      reinterpret_cast<uint4*>(smem + BT_TC_A_OFF)[k] = make_uint4(0, 0, 0, 0);
+      reinterpret_cast<uint4*>(tc.a_tile)[k] = make_uint4(0, 0, 0, 0);
     // the hi/lo Kronecker basis, built once per device, into the B operand
     const uint4* gb = reinterpret_cast<const uint4*>(a.tc_basis);
     for (int k = threadIdx.x; k < 16384 / 16; k += blockDim.x)
-      reinterpret_cast<uint4*>(smem + BT_TC_B_OFF)[k] = __ldg(gb + k);
+      reinterpret_cast<uint4*>(smem + CJ_TC_B_OFF)[k] = __ldg(gb + k);
     // the 8x8 basis B[u][x] in FP32 for the range fallback
     if (threadIdx.x < 64) {
       const int u = threadIdx.x >> 3, x = threadIdx.x & 7;

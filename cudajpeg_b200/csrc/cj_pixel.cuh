@@ -106,10 +106,15 @@ CJ_HD int cj_pix_check(const CJScanParams* hp) {
 // the two coefficient buffers sit at fixed offsets 0 and 8 KiB (a tile holds
 // at most 64 blocks), so tiles of different geometry -- consecutive tiles of
 // a batch CTA may come from different images -- never overlap the current
-// tile's working space.  The tensor-core form (tc) needs no row-pass buffer
-// but a 128-row FP16 A tile (16 KiB), the hi/lo Kronecker basis (16 KiB)
-// and one range flag per block row, at offsets that do not depend on the
-// geometry.
+// tile's working space.  The tensor-core form (tc, with nbuf = 2) needs no
+// row-pass buffer but a 128-row FP16 A tile (16 KiB, in the 128-byte swizzled
+// layout, which must start on a 1024-byte boundary: the region holds 1 KiB
+// of slack and the kernel aligns the tile inside it), the hi/lo Kronecker
+// basis (16 KiB) and one range flag per block row, at offsets that do not
+// depend on the geometry (CJ_TC_A_OFF, CJ_TC_B_OFF).
+#define CJ_TC_A_OFF 16384
+#define CJ_TC_A_BYTES (16384 + 1024)
+#define CJ_TC_B_OFF (CJ_TC_A_OFF + CJ_TC_A_BYTES)
 CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy, int nbuf = 1, bool tc = false) {
   g->y_stride = g->T * 8 * g->hmax;
   g->c_stride = g->nch == 3 ? g->T * 8 * csx : 0;
@@ -124,10 +129,9 @@ CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy, int nbuf = 1, bool tc
   }
   g->a_off = g->b_off = g->big_off = 0;
   if (tc) {
-    g->a_off = (int)off;
-    off += 16384;
-    g->b_off = (int)off;
-    off += 16384;
+    g->a_off = CJ_TC_A_OFF;
+    g->b_off = CJ_TC_B_OFF;
+    off = CJ_TC_B_OFF + 16384;
     g->big_off = (int)off;
     off += 64 * 8;
     g->tmp_off = g->a_off;  // unused
@@ -279,6 +283,7 @@ struct CJTcState {
   uint64_t* bar;
   uint32_t parity;
   const float* basis;
+  uint8_t* a_tile;  // the swizzled A tile: inside the A region, on a 1024-byte boundary
 };
 
 // Tensor-core iDCT of a tile's blocks (at most 64, rows of a 128-row A tile)
@@ -295,7 +300,7 @@ struct CJTcState {
 // (recorded).  Ends with a barrier.
 __device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, const int16_t* sc, uint8_t* smem,
                                                  const CJPixSmemParams& P, CJTcState& tc, CJStatus* st) {
-  uint8_t* sA = smem + g.a_off;
+  uint8_t* sA = tc.a_tile;
   uint8_t* big = smem + g.big_off;
   for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
     const int kb = t >> 3, v = t & 7;
@@ -330,21 +335,16 @@ __device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, c
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kb = 32 * (w & 3) + lane, h = w >> 2;
-  const bool live = kb < nblk;
-  const int ps = live && P.bc[kb] != 0 ? g.c_stride : g.y_stride;
-  uint8_t* dst = smem + (live ? P.boff[kb] : 0) + 4 * h * ps;
-  // two pixel rows per load (16 columns), to keep the live registers down
+  float d[32];
+  tc_ld32(tc.tmem + ((uint32_t)(32 * (w & 3)) << 16) + 32u * h, d);
+  if (kb < nblk) {
+    const int ps = P.bc[kb] == 0 ? g.y_stride : g.c_stride;
+    uint8_t* dst = smem + P.boff[kb] + 4 * h * ps;
 #pragma unroll
-  for (int j = 0; j < 2; j++) {
-    float d[16];
-    tc_ld16(tc.tmem + ((uint32_t)(32 * (w & 3)) << 16) + 32u * h + 16u * j, d);
-    if (live) {
-#pragma unroll
-      for (int y = 0; y < 2; y++)
-        *reinterpret_cast<uint2*>(dst + (2 * j + y) * ps) =
-            make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
-                       tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
-    }
+    for (int y = 0; y < 4; y++)
+      *reinterpret_cast<uint2*>(dst + y * ps) =
+          make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
+                     tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   const bool flagged = kb < nblk && h == 0 && *reinterpret_cast<const uint64_t*>(big + kb * 8) != 0;
