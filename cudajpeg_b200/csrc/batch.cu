@@ -881,6 +881,7 @@ __global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? 4 : 6
   __shared__ uint32_t s_tmem;
   __shared__ float s_b32[64];
   if (threadIdx.x == 0) {
+    cj_tile_fail = 0;
     cj_mbar_init(&bar2[0], 1);
     cj_mbar_init(&bar2[1], 1);
     if (MODE == CJ_PIX_IDCT_TC) cj_mbar_init(&s_mma_bar, 1);
@@ -979,6 +980,7 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
   CJPixGeom g = bt_pix_geom(a, img, TC);
   int gimg = img;
   cj_pixel_setup(a.prm[img], g, &P);
+  __syncthreads();  // the setup before any use (a tile has no barrier before its iDCT)
   // tile position in its image's grid, advanced tile by tile
   int gx = (g.mcux + g.T - 1) / g.T;
   int trow = (t0 - a.desc[img].ptile0) / gx, tcol = (t0 - a.desc[img].ptile0) % gx;
@@ -994,6 +996,7 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
       g = bt_pix_geom(a, img, TC);
       gimg = img;
       cj_pixel_setup(a.prm[img], g, &P);
+      __syncthreads();
       gx = (g.mcux + g.T - 1) / g.T;
       trow = tcol = 0;  // a new image starts at its first tile
     }

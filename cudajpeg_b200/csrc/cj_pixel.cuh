@@ -205,8 +205,8 @@ __device__ __forceinline__ void cj_rgb8(uint2 yv, const CJChromaTerms* d, int ds
   for (int w = 0; w < 6; w++) wds[w] = cj_pack_sat4(c[4 * w], c[4 * w + 1], c[4 * w + 2], c[4 * w + 3]);
 }
 
-// Per-image part of the tile setup (all threads; the tile's own barrier
-// after the coefficient copy orders it before use): dequantisation tables and,
+// Per-image part of the tile setup (all threads; the caller's barrier after
+// it orders it before use): dequantisation tables and,
 // for every block of a full tile, its destination in the plane tiles, its
 // component and its quantisation table.  A shorter last tile of an MCU row
 // uses a prefix of the same entries.
@@ -231,11 +231,23 @@ __device__ __forceinline__ void cj_pixel_setup(const CJScanParams& prmr, const C
   }
 }
 
+// A thread whose wait for the tile's coefficient copy (or, in the
+// tensor-core form, for its MMAs) ran out sets cj_tile_fail; the CTA reads it
+// after its next barrier and leaves together, with the image's error
+// recorded.  Every kernel that runs tiles clears it before its first barrier.
+static __shared__ int cj_tile_fail;
+
+__device__ __forceinline__ bool cj_pixel_failed(CJStatus* st) {
+  if (!cj_tile_fail) return false;
+  if (threadIdx.x == 0) atomicMax(&st->dec_err_key, ~((unsigned long long)CJ_DEV_CAPACITY));
+  return true;
+}
+
 // Integer iDCT of a tile's blocks (coefficients in `sc`) into the plane
 // tiles: row pass with dequantisation on load, then column pass with level
-// shift and clip.  Ends with a barrier.
-__device__ __forceinline__ void cj_pixel_idct_int(const CJPixGeom& g, int nblk, const int16_t* sc, uint8_t* smem,
-                                                  const CJPixSmemParams& P) {
+// shift and clip.  Ends with a barrier; false if a wait of the tile failed.
+__device__ __forceinline__ bool cj_pixel_idct_int(const CJPixGeom& g, int nblk, const int16_t* sc, uint8_t* smem,
+                                                  const CJPixSmemParams& P, CJStatus* st) {
   int* tmp = reinterpret_cast<int*>(smem + g.tmp_off);
   // Row pass: one thread per (block, row); dequantise on load.
   for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
@@ -252,6 +264,7 @@ __device__ __forceinline__ void cj_pixel_idct_int(const CJPixGeom& g, int nblk, 
     o[1] = make_int4(v[4], v[5], v[6], v[7]);
   }
   __syncthreads();
+  if (cj_pixel_failed(st)) return false;
 
   // Column pass: one thread per (block, column pair); the two columns' 8
   // samples go into the plane tile as one 16-bit store per row.
@@ -273,6 +286,7 @@ __device__ __forceinline__ void cj_pixel_idct_int(const CJPixGeom& g, int nblk, 
     for (int j = 0; j < 8; j++) *reinterpret_cast<uint16_t*>(dst + j * ps) = (uint16_t)cj_level2(o0[j], o1[j]);
   }
   __syncthreads();
+  return true;
 }
 
 // Tensor-memory state of a CTA running the tensor-core form: its 64-column
@@ -323,21 +337,20 @@ __device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, c
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncthreads();
+  if (cj_pixel_failed(st)) return false;  // the coefficient copy did not land
   if (threadIdx.x == 0)
     tc_idct_mmas_asw(tc.tmem, cj_smem_addr(sA), cj_smem_addr(smem + g.b_off), cj_smem_addr(tc.bar));
+  // no barrier after the wait: each thread reads only after its own wait
+  // succeeded, and a failed wait is agreed on at the barrier below
   const bool ok = cj_mbar_wait(tc.bar, tc.parity);
   tc.parity ^= 1u;
-  if (!__syncthreads_and(ok)) {
-    if (threadIdx.x == 0) atomicMax(&st->dec_err_key, ~((unsigned long long)CJ_DEV_CAPACITY));
-    cj_mbar_wait(tc.bar, tc.parity ^ 1u);  // a bounded second chance for MMAs still in flight
-    return false;
-  }
+  if (!ok) cj_tile_fail = 1;
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kb = 32 * (w & 3) + lane, h = w >> 2;
   float d[32];
   tc_ld32(tc.tmem + ((uint32_t)(32 * (w & 3)) << 16) + 32u * h, d);
-  if (kb < nblk) {
+  if (ok && kb < nblk) {
     const int ps = P.bc[kb] == 0 ? g.y_stride : g.c_stride;
     uint8_t* dst = smem + P.boff[kb] + 4 * h * ps;
 #pragma unroll
@@ -348,7 +361,11 @@ __device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, c
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   const bool flagged = kb < nblk && h == 0 && *reinterpret_cast<const uint64_t*>(big + kb * 8) != 0;
-  if (__syncthreads_or(flagged)) {  // rare: FP32 redo of the flagged blocks
+  if (__syncthreads_or(flagged || !ok)) {  // rare: a failed wait, or an FP32 redo of the flagged blocks
+    if (cj_pixel_failed(st)) {
+      cj_mbar_wait(tc.bar, tc.parity ^ 1u);  // a bounded second chance for MMAs still in flight
+      return false;
+    }
     for (int k = 0; k < nblk; k++) {
       if (!*reinterpret_cast<const uint64_t*>(big + k * 8)) continue;  // the same for every thread
       if (threadIdx.x < 64) {
@@ -494,15 +511,13 @@ __device__ __forceinline__ bool cj_pixel_tile(uint8_t* __restrict__ out, CJStatu
                                               uint32_t parity, CJPixSmemParams* Pp, CJTcState* tc) {
   const int nm = min(g.T, g.mcux - mc0);
   const int nblk = nm * g.bpm;
-  bool ok = cj_mbar_wait(barp, parity);
-  if (!__syncthreads_and(ok)) {
-    if (threadIdx.x == 0) atomicMax(&st->dec_err_key, ~((unsigned long long)CJ_DEV_CAPACITY));
-    return false;
-  }
+  // each thread reads the copied blocks only after its own wait; a wait that
+  // ran out is agreed on at the iDCT's first barrier (no barrier here)
+  if (!cj_mbar_wait(barp, parity)) cj_tile_fail = 1;
   if (MODE == CJ_PIX_IDCT_TC) {
     if (!cj_pixel_idct_tc(g, nblk, sc, smem, *Pp, *tc, st)) return false;
   } else {
-    cj_pixel_idct_int(g, nblk, sc, smem, *Pp);
+    if (!cj_pixel_idct_int(g, nblk, sc, smem, *Pp, st)) return false;
   }
   if (OUT == CJ_OUT_RGB) cj_pixel_emit_rgb(out, g, mrow, mc0, nm, smem);
   else cj_pixel_emit_planes<OUT>(out, g, mrow, mc0, nm, smem);

@@ -29,11 +29,13 @@ k_pixel(const CJScanParams* __restrict__ prm, const int16_t* __restrict__ coef,
   __shared__ uint64_t bar;
   __shared__ CJPixSmemParams P;
   if (threadIdx.x == 0) {
+    cj_tile_fail = 0;
     cj_mbar_init(&bar, 1);
     cj_pixel_issue(coef, g, blockIdx.y, blockIdx.x * g.T, reinterpret_cast<int16_t*>(smem), &bar);
   }
   __syncthreads();
   cj_pixel_setup(*prm, g, &P);
+  __syncthreads();
   cj_pixel_compute(out, st, g, blockIdx.y, blockIdx.x * g.T, reinterpret_cast<int16_t*>(smem), smem, &bar, 0, &P);
 }
 
