@@ -23,11 +23,14 @@ precision_8192 is the iDCT precision A/B (run_precision).
 * ``e2e``     the same metric through the public C API: per step the host
   parse, the host->device copy of the files from pinned memory, the decode,
   and the device->host copy of every decoded image into pinned memory.
-* ``roofline`` the dominant kernel (k_decode_batch): its algorithmic bytes
-  (compressed scans read, destuffed copy written and read twice, int16
-  coefficient blocks written) / its duration (in-kernel %globaltimer phase
-  stamps), against the measured HBM copy bandwidth in MEASURED_PEAKS.json;
-  ``roofline_pixel`` the same for k_pixel_batch (blocks read, pixels written).
+* ``roofline`` the dominant kernel (k_decode_batch): the path's algorithmic
+  bytes (compressed scans read + decoded pixels written) / its duration
+  (in-kernel %globaltimer phase stamps), against the measured HBM copy
+  bandwidth in MEASURED_PEAKS.json (else the fallback figure, said so);
+  ``kernel_min_bytes`` adds the kernel's own intermediates (destuffed copy
+  written and read twice, int16 coefficient blocks written);
+  ``roofline_pixel`` the same for k_pixel_batch (its algorithmic bytes are
+  the pixels it writes; ``kernel_min_bytes`` adds the blocks it reads).
 * ``plain_path`` (batch workload) the per-image path over the same images.
 * ``serving`` open-loop Poisson request streams through the continuous-
   batching server (cudajpeg_b200.serve): p50/p99/p99.9 latency, MPix/s.
@@ -533,7 +536,10 @@ def run_batch(args, wl, world, rank, local, dist):
     ach_decode = alg_path / (decode_ms / 1e3) / 1e9
     ach_step = alg_path / (mean_ms / 1e3) / 1e9
     tkey = traffic_key(args.workload, args.batch_size)
-    ach_pixel = min_pixel / (pixel_ms / 1e3) / 1e9
+    # the pixel kernel's share of the path's algorithmic bytes: the pixels it
+    # writes (its int16 block reads are an intermediate, kernel_min_bytes)
+    ach_pixel = st_run["output_bytes"] / (pixel_ms / 1e3) / 1e9
+    ach_pixel_min = min_pixel / (pixel_ms / 1e3) / 1e9
     tr_decode = read_traffic("k_decode_batch", tkey)
     tr_pixel = read_traffic("k_pixel_batch", tkey)
     tr_step = tr_decode + tr_pixel if tr_decode and tr_pixel else None
@@ -584,8 +590,11 @@ def run_batch(args, wl, world, rank, local, dist):
                                "peak": peaks["hbm_gbs"], "unit": "GB/s",
                                "frac": round(ach_pixel / peaks["hbm_gbs"], 4),
                                "traffic": tr_pixel,
+                               "algorithmic_bytes": int(st_run["output_bytes"]),
                                "kernel_min_bytes": int(min_pixel), "kernel_ms": round(pixel_ms, 4),
-                               "bytes": "int16 blocks read + decoded pixels written",
+                               "achieved_kernel_min": round(ach_pixel_min, 1),
+                               "bytes": "decoded pixels written (algorithmic); kernel_min_bytes adds the "
+                                        "int16 blocks it reads",
                                "peak_source": peaks["source"]},
             "phase_ms": pm, "gpu_launches": int(launches), "clocks": clocks.summary()}
     # the same batch with the tensor-core iDCT in the pixel kernel (the
