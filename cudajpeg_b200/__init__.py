@@ -60,7 +60,7 @@ EXPORTED = [
     "cjBatchSetSubsequenceBitsFor", "cjBatchGetSubsequenceBitsFor",
     "cjBatchGetOutput", "cjBatchChromaGeometry", "cjBatchDLPack", "cjServerDLPack", "cjDLPackFree",
     "decodeScanCPU", "upsampleAndColourTransformHybrid", "upsampleAndColourTransformGPU",
-    "upsampleAndColourTransformCPU",
+    "upsampleAndColourTransformCPU", "cjBatchSetParse", "cjDebugParseCompare",
 ]
 
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
@@ -153,6 +153,8 @@ def load(build_if_missing: bool = True):
     lib.cjBatchSetSubsequenceBitsFor.argtypes = [vp, C.c_int, C.c_int]
     lib.cjBatchGetSubsequenceBitsFor.argtypes = [vp, C.c_int]
     lib.cjBatchSetOutput.argtypes = [vp, C.c_int, C.c_int]
+    lib.cjBatchSetParse.argtypes = [vp, C.c_int]
+    lib.cjDebugParseCompare.argtypes = [vp, C.c_size_t, ip, ip]
     lib.cjBatchGetOutput.argtypes = [vp, ip, ip]
     lib.cjBatchChromaGeometry.argtypes = [vp, C.c_int, ip, ip]
     lib.cjBatchDLPack.restype = vp
@@ -487,6 +489,12 @@ class Batch:
         if self.lib.cjBatchSetSubsequenceBitsFor(self.ptr, sampling_class, bits):
             raise ValueError(f"bad subsequence size {bits} for class {sampling_class}")
 
+    def set_parse(self, on_device: bool = True):
+        """Parse the files' marker segments on the GPU or on the host (the
+        default), for batches staged from now on (cjBatchSetParse)."""
+        if self.lib.cjBatchSetParse(self.ptr, 1 if on_device else 0):
+            raise ValueError("cjBatchSetParse")
+
     def set_wait_limit(self, polls: int):
         """Bound each grid-barrier wait of the decode kernel (0 = default)."""
         if self.lib.cjBatchSetWaitLimit(self.ptr, polls):
@@ -644,6 +652,20 @@ def _image_view(p: int, w: int, h: int, c: int, fmt: int, chroma, copy: bool):
     if fmt == OUTPUT_NV12:
         return y, flat[w * h:].reshape(ch, cw, 2)
     return y, flat[w * h: w * h + cw * ch].reshape(ch, cw), flat[w * h + cw * ch:].reshape(ch, cw)
+
+
+def parse_compare(data: bytes) -> tuple:
+    """(mismatch mask, host error, device-parse error) of cjDebugParseCompare:
+    the batch decoder's marker parse (run on the host) against openJPGMem's
+    marker loop on the same file.  Needs no GPU."""
+    lib = load()
+    # 64 KiB of zeros after the file: a malformed segment length must not let
+    # a parser read beyond what it was given, and if one did, it stays in
+    # this buffer
+    buf = C.create_string_buffer(bytes(data) + bytes(65536), len(data) + 65536)
+    e1, e2 = C.c_int(0), C.c_int(0)
+    r = lib.cjDebugParseCompare(buf, len(data), C.byref(e1), C.byref(e2))
+    return r, e1.value, e2.value
 
 
 def build_info() -> dict:

@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <atomic>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <vector>
 
@@ -37,6 +38,7 @@
 #include "cj_entropy.cuh"
 #include "cj_idct.cuh"
 #include "cj_internal.h"
+#include "cj_parse.cuh"
 #include "cj_pixel.cuh"
 #include "cj_scan_util.cuh"
 #include "cj_tables.h"
@@ -54,17 +56,6 @@
 // (cj_pix_layout with two coefficient buffers)
 
 // ---------------------------------------------------------------- layouts
-
-// What the host parse of one image hands the device.
-struct CJImageHeader {
-  uint8_t counts[4][16];    // DHT BITS per table slot
-  uint8_t symbols[4][256];  // DHT HUFFVAL per table slot
-  uint16_t dq[4][64];       // DQT (8- or 16-bit values), zig-zag order
-  uint8_t comp_dc[3], comp_ac[3], comp_q[3], comp_sx[3], comp_sy[3];
-  uint8_t nch, huff_mask, xshift, yshift, pad[4];
-  int32_t mcux, mcuy, width, height, hmax, vmax, restart_interval, nseg_expected;
-  int64_t total_blocks;
-};
 
 // Where one image's data lives in the batch buffers (host-planned).
 struct CJImageDesc {
@@ -858,7 +849,10 @@ static cudaError_t bt_decode_attrs() {
 
 template <int MODE, int OUT>
 __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int t1, uint8_t* smem,
-                                               uint64_t* bar2, CJPixSmemParams* Pp, CJTcState* tc);
+                                               uint64_t* bar2, CJPixSmemParams* Pp);
+template <int OUT>
+__device__ __forceinline__ void bt_pixel_tiles_tc(const CJBatchArgs& a, int t0, int t1, uint8_t* smem,
+                                                  uint64_t* bar2, CJPixSmemParams* Pp, CJTcState* tc);
 
 // Phase 9 runs as its own kernel, launched right after k_decode_batch on the
 // same stream: the pixel work needs no grid barrier, and on its own it runs
@@ -870,7 +864,7 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
 // keeps a 64-column accumulator in tensor memory per CTA and the hi/lo
 // Kronecker basis, built by the CTA, in shared memory.
 template <int MODE, int OUT>
-__global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? 4 : 6) k_pixel_batch(CJBatchArgs a) {
+__global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? CJ_TC_MINB : 6) k_pixel_batch(CJBatchArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ uint64_t bar2[2];
   __shared__ CJPixSmemParams P;
@@ -922,7 +916,10 @@ __global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? 4 : 6
   // tile geometry is rebuilt only when it changes.
   const int per = (a.nptiles + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(t0 + per, a.nptiles);
-  if (t0 < t1) bt_pixel_tiles<MODE, OUT>(a, t0, t1, smem, bar2, &P, &tc);
+  if (t0 < t1) {
+    if constexpr (MODE == CJ_PIX_IDCT_TC) bt_pixel_tiles_tc<OUT>(a, t0, t1, smem, bar2, &P, &tc);
+    else bt_pixel_tiles<MODE, OUT>(a, t0, t1, smem, bar2, &P);
+  }
   __syncthreads();
   if (MODE == CJ_PIX_IDCT_TC && (threadIdx.x >> 5) == 0) tc_dealloc(s_tmem, 64);
   if (threadIdx.x == 0 && atomicAdd(&a.ctl->pix_done, 1) == gridDim.x - 1) bt_stamp_any(a.ctl, BT_NPHASE);
@@ -952,8 +949,8 @@ __device__ __forceinline__ CJPixGeom bt_pix_geom(const CJBatchArgs& a, int i, bo
 // Tiles [t0, t1) of one pixel-kernel CTA.
 template <int MODE, int OUT>
 __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int t1, uint8_t* smem,
-                                               uint64_t* bar2, CJPixSmemParams* Pp, CJTcState* tc) {
-  constexpr bool TC = MODE == CJ_PIX_IDCT_TC;
+                                               uint64_t* bar2, CJPixSmemParams* Pp) {
+  constexpr bool TC = false;
   CJPixSmemParams& P = *Pp;
   auto advance = [&](int tt, int i) {
     while (tt >= a.desc[i].ptile0 + a.desc[i].nptiles) i++;
@@ -1003,7 +1000,7 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
     const CJImageDesc& d = a.desc[img];
     const int16_t* sc = reinterpret_cast<const int16_t*>(smem + buf * g.sc1_off);
     if (!cj_pixel_tile<MODE, OUT>(a.out + d.out_off, &a.st[img], g, trow, tcol * g.T, sc, smem, &bar2[buf],
-                                  (par >> buf) & 1u, &P, tc)) {
+                                  (par >> buf) & 1u, &P)) {
       if (t + 1 < t1) cj_mbar_wait(&bar2[buf ^ 1], (par >> (buf ^ 1)) & 1u);  // the prefetch in flight
       break;
     }
@@ -1013,6 +1010,140 @@ __device__ __forceinline__ void bt_pixel_tiles(const CJBatchArgs& a, int t0, int
     }
     par ^= 1u << buf;
     buf ^= 1;
+  }
+}
+
+// Tiles [t0, t1) of one pixel-kernel CTA in the tensor-core form.  A tile
+// holds up to CJ_TC_MAXB blocks (cj_pix_tile_mcus_tc) and costs two
+// barrier-separated phases:
+//   1. thread 0 issues the tile's 8 MMAs (its A tile was built in the
+//      previous phase) and the bulk copy of the coefficients of the tile
+//      CJ_TC_NBUF ahead (into the buffer this tile's A was built from);
+//      every thread waits for the MMAs and runs the epilogue into the plane
+//      tiles -- barrier -- (rare: the FP32 redo of range-flagged blocks);
+//   2. the output of the tile from the plane tiles, then the A tile of the
+//      next tile from its copied coefficients -- barrier.
+// The output and the next A build share a phase, so no warp idles through
+// a phase of its own, and the MMAs' latency is covered by the other CTAs of
+// the SM.  An image change between two tiles adds two barriers (the new
+// image's tables and block destinations replace the old ones after the
+// output).
+template <int OUT>
+__device__ __forceinline__ void bt_pixel_tiles_tc(const CJBatchArgs& a, int t0, int t1, uint8_t* smem,
+                                                  uint64_t* bar2, CJPixSmemParams* Pp, CJTcState* tc) {
+  CJPixSmemParams& P = *Pp;
+  uint8_t* big = smem + CJ_TC_BIG_OFF;
+  auto advance = [&](int tt, int i) {
+    while (tt >= a.desc[i].ptile0 + a.desc[i].nptiles) i++;
+    return i;
+  };
+  // tile u's coefficient buffer, and the wait for its copy (each buffer's
+  // barrier completes one phase per tile it receives)
+  auto sc_of = [&](int u) {
+    return reinterpret_cast<int16_t*>(smem + CJ_TC_SC_OFF + ((u - t0) % CJ_TC_NBUF) * CJ_TC_COEF_BYTES);
+  };
+  auto wait_copy = [&](int u) {
+    return cj_mbar_wait(&bar2[(u - t0) % CJ_TC_NBUF], (uint32_t)(((u - t0) / CJ_TC_NBUF) & 1));
+  };
+  // thread 0 issues the copies in tile order and keeps the geometry of the
+  // image it issues from
+  __shared__ CJPixGeom s_pg;
+  __shared__ int s_pimg;
+  int nimg = 0;
+  auto issue = [&](int u) {
+    nimg = advance(u, nimg);
+    if (nimg != s_pimg) {
+      s_pg = bt_pix_geom(a, nimg, true);
+      s_pimg = nimg;
+    }
+    const int local = u - a.desc[nimg].ptile0, gx = (s_pg.mcux + s_pg.T - 1) / s_pg.T;
+    cj_pixel_issue(a.coef + a.desc[nimg].coef0 * 64, s_pg, local / gx, (local % gx) * s_pg.T, sc_of(u),
+                   &bar2[(u - t0) % CJ_TC_NBUF]);
+  };
+  int img = bt_find(a.n, t0, [&](int k) { return a.desc[k].ptile0; });
+  int issued_to = min(t0 + CJ_TC_NBUF, t1);  // copies of tiles [.., issued_to) are issued
+  int waited_to = t0;                         // and those of [.., waited_to) waited for
+  if (threadIdx.x == 0) {
+    s_pimg = -1;
+    nimg = img;
+    for (int u = t0; u < issued_to; u++) issue(u);
+  }
+  // on leaving early: a bounded wait for every copy still in flight
+  auto leave = [&]() {
+    for (int u = waited_to; u < issued_to; u++) wait_copy(u);
+  };
+  // the geometry of the current image lives in shared memory (written by
+  // thread 0), not in every thread's registers
+  __shared__ CJPixGeom s_g;
+  const CJPixGeom& g = s_g;
+  if (threadIdx.x == 0) s_g = bt_pix_geom(a, img, true);
+  __syncthreads();
+  cj_pixel_setup(a.prm[img], g, &P);
+  int gx = (g.mcux + g.T - 1) / g.T;
+  int trow = (t0 - a.desc[img].ptile0) / gx, tcol = (t0 - a.desc[img].ptile0) % gx;
+  int nblk = min(g.T, g.mcux - tcol * g.T) * g.bpm;
+  __syncthreads();  // the setup before the first A build
+  if (!wait_copy(t0)) cj_tile_fail = 1;
+  waited_to = t0 + 1;
+  cj_tc_build_a(nblk, sc_of(t0), tc->a_tile, big, P);
+  __syncthreads();
+  if (cj_pixel_failed(&a.st[img])) {
+    leave();
+    return;
+  }
+  for (int t = t0; t < t1; t++) {
+    // ---- phase 1: the tile's MMAs, the copy CJ_TC_NBUF tiles ahead, the epilogue
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (threadIdx.x == 0) {
+      tc_idct_mmas_asw(tc->tmem, cj_smem_addr(tc->a_tile), cj_smem_addr(smem + CJ_TC_B_OFF), cj_smem_addr(tc->bar));
+      if (t + CJ_TC_NBUF < t1) issue(t + CJ_TC_NBUF);
+    }
+    if (t + CJ_TC_NBUF < t1) issued_to = t + CJ_TC_NBUF + 1;
+    const bool ok = cj_mbar_wait(tc->bar, tc->parity);
+    tc->parity ^= 1u;
+    if (!ok) cj_tile_fail = 1;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool flagged = cj_tc_epilogue(g, nblk, smem, big, P, *tc, ok);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    const CJImageDesc& d = a.desc[img];
+    if (__syncthreads_or(flagged || !ok)) {  // rare: a failed wait, or an FP32 redo
+      if (cj_pixel_failed(&a.st[img])) {
+        cj_mbar_wait(tc->bar, tc->parity ^ 1u);  // a bounded second chance for MMAs still in flight
+        leave();
+        return;
+      }
+      cj_tc_fallback(g, nblk, a.coef + (d.coef0 + ((int64_t)trow * g.mcux + (int64_t)tcol * g.T) * g.bpm) * 64,
+                     smem, big, P, *tc);
+    }
+    // ---- phase 2: the tile's output, then the next tile's A
+    const int nm = min(g.T, g.mcux - tcol * g.T);
+    if (OUT == CJ_OUT_RGB) cj_pixel_emit_rgb(a.out + d.out_off, g, trow, tcol * g.T, nm, smem);
+    else cj_pixel_emit_planes<OUT>(a.out + d.out_off, g, trow, tcol * g.T, nm, smem);
+    if (t + 1 < t1) {
+      const int img1 = advance(t + 1, img);
+      if (img1 != img) {  // CTA-uniform
+        __syncthreads();  // the plane tiles, P and the geometry of the old image are read no more
+        img = img1;
+        if (threadIdx.x == 0) s_g = bt_pix_geom(a, img, true);
+        __syncthreads();
+        cj_pixel_setup(a.prm[img], g, &P);
+        gx = (g.mcux + g.T - 1) / g.T;
+        trow = tcol = 0;  // a new image starts at its first tile
+        __syncthreads();
+      } else if (++tcol == gx) {
+        tcol = 0;
+        trow++;
+      }
+      nblk = min(g.T, g.mcux - tcol * g.T) * g.bpm;
+      if (!wait_copy(t + 1)) cj_tile_fail = 1;
+      waited_to = t + 2;
+      cj_tc_build_a(nblk, sc_of(t + 1), tc->a_tile, big, P);
+    }
+    __syncthreads();  // the output is written, the next A tile is complete
+    if (cj_pixel_failed(&a.st[img])) {
+      leave();
+      return;
+    }
   }
 }
 
@@ -1090,6 +1221,24 @@ static int64_t bt_out_bytes(const CJImageHeader& h, int out) {
   return y + 2 * cw * ch;
 }
 
+// ---------------------------------------------------------------- device header parse
+
+// The batch's marker parse on the GPU: thread i walks file i's marker
+// segments (cj_parse_header) in the blob already copied to the device and
+// leaves its header and {error, scan offset, scan length}.
+__global__ void __launch_bounds__(128) k_parse_headers(const uint8_t* __restrict__ blob,
+                                                        const int64_t* __restrict__ offsets,
+                                                        const int64_t* __restrict__ sizes, int n,
+                                                        CJImageHeader* hdr, int64_t* meta) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t so = 0, sl = 0;
+  const int e = cj_parse_header(blob + offsets[i], sizes[i], &hdr[i], &so, &sl);
+  meta[3 * i] = e;
+  meta[3 * i + 1] = so;
+  meta[3 * i + 2] = sl;
+}
+
 // ---------------------------------------------------------------- host side
 
 struct CJBatch {
@@ -1106,11 +1255,13 @@ struct CJBatch {
   int idct = CJ_PIX_IDCT_INT;                // pixel-stage iDCT arithmetic
   int out_format = CJ_OUT_RGB;               // output format
   JPGReader* parser = nullptr;  // host marker parse, one image at a time
+  bool parse_on_device = false;  // marker parse on the GPU (k_parse_headers) or on the host
   // device buffers (grow-only)
   CJDevBuf hdr, desc, prm, st, blob, data, tile_keep, tile_mark, mpos, mcode, segs, recs, ckpt, snap,
       wagg, carry, coef, out, ctl, fancy;  // fancy: planar samples of the fancy mode
+  CJDevBuf p_size, p_hdr, p_meta;          // device parse: file offsets + sizes, headers, results
   // pinned host staging
-  CJHostBuf h_hdr, h_desc, h_out, h_st, h_ctl;
+  CJHostBuf h_hdr, h_desc, h_out, h_st, h_ctl, h_psize, h_phdr, h_pmeta;
   // plan of the staged batch
   int n_in = 0, n_dev = 0;
   std::vector<int> dev_of;     // device slot of each submitted image, -1 if rejected
@@ -1265,10 +1416,10 @@ void cjBatchDestroy(CJBatch* b) {
     CJDevBuf* bufs[] = {&b->hdr,  &b->desc, &b->prm,   &b->st,   &b->blob,  &b->data,
                         &b->tile_keep, &b->tile_mark, &b->mpos, &b->mcode, &b->segs,
                         &b->recs, &b->ckpt, &b->snap, &b->wagg, &b->carry, &b->coef, &b->out, &b->ctl,
-                        &b->fancy};
+                        &b->fancy, &b->p_size, &b->p_hdr, &b->p_meta};
     for (CJDevBuf* d : bufs)
       if (d->p) cudaFree(d->p);
-    CJHostBuf* hb[] = {&b->h_hdr, &b->h_desc, &b->h_out, &b->h_st, &b->h_ctl};
+    CJHostBuf* hb[] = {&b->h_hdr, &b->h_desc, &b->h_out, &b->h_st, &b->h_ctl, &b->h_psize, &b->h_phdr, &b->h_pmeta};
     for (CJHostBuf* h : hb)
       if (h->p) cudaFreeHost(h->p);
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
@@ -1342,6 +1493,51 @@ int cjBatchSetOutput(CJBatch* b, int format, int idct) {
   return 0;
 }
 
+int cjBatchSetParse(CJBatch* b, int on_device) {
+  if (!b) return PROGRAMMER_ERROR;
+  b->parse_on_device = on_device != 0;
+  return 0;
+}
+
+// Host check of the device header parse: cj_parse_header (the function
+// k_parse_headers runs, here on the host) against the host marker loop of
+// the drop-in path with a fresh reader (cj_parse_to_scan + bt_fill_header).
+int cjDebugParseCompare(const unsigned char* data, size_t size, int* err_host, int* err_parse) {
+  if (!data || !err_host || !err_parse) return PROGRAMMER_ERROR;
+  JPGReader* r = newJPGReader();
+  if (!r) return OOM_ERROR;
+  CJImageHeader* h1 = new (std::nothrow) CJImageHeader;
+  CJImageHeader* h2 = new (std::nothrow) CJImageHeader;
+  if (!h1 || !h2) {
+    delete h1;
+    delete h2;
+    delJPGReader(r);
+    return OOM_ERROR;
+  }
+  memset(h1, 0, sizeof(*h1));
+  int64_t so1 = 0, sl1 = 0, so2 = 0, sl2 = 0;
+  int e1 = cj_parse_to_scan(r, data, size);
+  if (!e1) {
+    e1 = bt_fill_header(r, h1);
+    so1 = (int64_t)(r->pos - data);
+    sl1 = (int64_t)(r->end - r->pos);
+  }
+  if (!e1 && (uint64_t)sl1 > CJ_MAX_SCAN_BYTES) e1 = UNSUPPORTED_ERROR;
+  const int e2 = cj_parse_header(data, (int64_t)size, h2, &so2, &sl2);
+  *err_host = e1;
+  *err_parse = e2;
+  int diff = 0;
+  if (e1 != e2) diff |= 1;
+  if (!e1 && !e2) {
+    if (so1 != so2 || sl1 != sl2) diff |= 2;
+    if (memcmp(h1, h2, sizeof(CJImageHeader))) diff |= 4;
+  }
+  delete h1;
+  delete h2;
+  delJPGReader(r);
+  return diff;
+}
+
 void cjBatchGetOutput(const CJBatch* b, int* format, int* idct) {
   if (format) *format = b->out_format;
   if (idct) *idct = b->idct;
@@ -1378,6 +1574,39 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
     return OOM_ERROR;
   CJImageHeader* hh = (CJImageHeader*)b->h_hdr.p;
   CJImageDesc* dd = (CJImageDesc*)b->h_desc.p;
+  // Marker parse on the GPU: the files go to the device first, one thread per
+  // file parses its segments there (k_parse_headers), and only the headers
+  // and scan ranges come back for the plan.  The same parse runs on the host
+  // with cjBatchSetParse(b, 0).
+  const bool dev_parse = b->parse_on_device && n > 0;
+  const CJImageHeader* ph = nullptr;
+  const int64_t* pmeta = nullptr;
+  if (dev_parse) {
+    const size_t nn = (size_t)n;
+    if (cj_host_ensure(b->h_psize, nn * 16) || cj_host_ensure(b->h_phdr, nn * sizeof(CJImageHeader)) ||
+        cj_host_ensure(b->h_pmeta, nn * 24))
+      return OOM_ERROR;
+    if (bt_ensure(b, b->blob, (size_t)blob_bytes + 64) || bt_ensure(b, b->p_size, nn * 16) ||
+        bt_ensure(b, b->p_hdr, nn * sizeof(CJImageHeader)) || bt_ensure(b, b->p_meta, nn * 24))
+      return CUDA_MEM_ERROR;
+    int64_t* hs = (int64_t*)b->h_psize.p;
+    memcpy(hs, offsets, nn * 8);
+    memcpy(hs + n, sizes, nn * 8);
+    cudaStream_t s = b->stream;
+    CJ_CUDA_TRY(cudaMemcpyAsync(b->blob.p, blob, (size_t)blob_bytes, cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaMemcpyAsync(b->p_size.p, hs, nn * 16, cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
+    const int64_t* d_off = (const int64_t*)b->p_size.p;
+    k_parse_headers<<<(n + 127) / 128, 128, 0, s>>>((const uint8_t*)b->blob.p, d_off, d_off + n, n,
+                                                   (CJImageHeader*)b->p_hdr.p, (int64_t*)b->p_meta.p);
+    CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
+    b->launches++;
+    CJ_CUDA_TRY(cudaMemcpyAsync(b->h_phdr.p, b->p_hdr.p, nn * sizeof(CJImageHeader), cudaMemcpyDeviceToHost, s),
+                CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaMemcpyAsync(b->h_pmeta.p, b->p_meta.p, nn * 24, cudaMemcpyDeviceToHost, s), CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaStreamSynchronize(s), CUDA_KERNEL_LAUNCH_ERROR);
+    ph = (const CJImageHeader*)b->h_phdr.p;
+    pmeta = (const int64_t*)b->h_pmeta.p;
+  }
   int nd = 0, ntiles = 0, nsubw = 0, nptiles = 0, nmark = 0, nseg = 0;
   int64_t data_bytes = 0, blocks = 0, out_total = 0, planar_total = 0, npix = 0;
   const bool fancy = b->out_format == CJ_OUT_RGB_FANCY;
@@ -1386,7 +1615,15 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   size_t smem = 0;
   for (int i = 0; i < n; i++) {
     int64_t so = 0, sl = 0;
-    int e = bt_parse(b, blob + offsets[i], (size_t)sizes[i], &hh[nd], &so, &sl);
+    int e;
+    if (dev_parse) {
+      e = (int)pmeta[3 * i];
+      so = pmeta[3 * i + 1];
+      sl = pmeta[3 * i + 2];
+      if (!e) memcpy(&hh[nd], &ph[i], sizeof(CJImageHeader));
+    } else {
+      e = bt_parse(b, blob + offsets[i], (size_t)sizes[i], &hh[nd], &so, &sl);
+    }
     if (!e && (uint64_t)sl > CJ_MAX_SCAN_BYTES) e = UNSUPPORTED_ERROR;
     if (e) {
       b->host_err[i] = e;
@@ -1416,7 +1653,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
     d.sub_cap = sub_cap;
     nsubw += sub_cap / 32;
     int bpm = (int)(h.total_blocks / ((int64_t)h.mcux * h.mcuy));
-    d.T = cj_pix_tile_mcus(h.hmax, bpm);
+    d.T = b->idct == CJ_PIX_IDCT_TC ? cj_pix_tile_mcus_tc(h.hmax, bpm) : cj_pix_tile_mcus(h.hmax, bpm);
     while (b->tile_cap > 0 && d.T > b->tile_cap && d.T > 1) d.T >>= 1;
     d.ptile0 = nptiles;
     d.nptiles = h.mcuy * ((h.mcux + d.T - 1) / d.T);
@@ -1487,8 +1724,9 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
               CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaMemcpyAsync(b->desc.p, dd, nd_ * sizeof(CJImageDesc), cudaMemcpyHostToDevice, s),
               CUDA_MEM_ERROR);
-  CJ_CUDA_TRY(cudaMemcpyAsync(b->blob.p, blob, (size_t)blob_bytes, cudaMemcpyHostToDevice, s),
-              CUDA_MEM_ERROR);
+  if (!dev_parse)  // (the device parse copied the files already)
+    CJ_CUDA_TRY(cudaMemcpyAsync(b->blob.p, blob, (size_t)blob_bytes, cudaMemcpyHostToDevice, s),
+                CUDA_MEM_ERROR);
   int per_sm = 0;
   CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)bt_decode_kernel(b->decode_ctas),
                                                             BT_THREADS, b->smem),

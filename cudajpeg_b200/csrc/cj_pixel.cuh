@@ -75,12 +75,29 @@ struct CJPixGeom {
 // that the column pass (lanes = 4 blocks x 8 columns) reads 32 distinct banks.
 #define CJ_TMP_STRIDE 72
 
+// Blocks of one tensor-core tile: the rows of its 128-row A operand.  The
+// CUDA-core forms keep at most 64 blocks per tile (cj_pix_tile_mcus).
+#ifndef CJ_TC_MAXB
+#define CJ_TC_MAXB 128
+#endif
+// Coefficient buffers of a tensor-core tile (TMA bulk copies in flight) and
+// the CTAs per SM its kernel is compiled for (its register cap).  Measured on
+// the 1024-image mix: one buffer at 3 CTAs/SM (60 KB of shared memory each)
+// runs the pixel stage in 1.04 ms, two buffers at 2 CTAs/SM in 1.24 ms, and
+// 64-block tiles at 4 CTAs/SM in 1.42-1.48 ms.
+#ifndef CJ_TC_NBUF
+#define CJ_TC_NBUF 1
+#endif
+#ifndef CJ_TC_MINB
+#define CJ_TC_MINB 3
+#endif
+
 struct alignas(16) CJPixSmemParams {
   int32_t q[4][64];       // dequantisation tables, natural order (int32: no unpacking per row)
   uint16_t qh[4][64];     // the same as FP16 bit patterns (tensor-core form)
-  uint16_t boff[64];      // per block of the tile: smem offset of its 8x8 destination
-  uint8_t bc[64];         // per block of the tile: component
-  uint8_t bq[64];         // per block of the tile: quantisation table
+  uint16_t boff[CJ_TC_MAXB];  // per block of the tile: smem offset of its 8x8 destination
+  uint8_t bc[CJ_TC_MAXB];     // per block of the tile: component
+  uint8_t bq[CJ_TC_MAXB];     // per block of the tile: quantisation table
 };
 
 // MCUs per tile: 128 output pixels across, at most 64 blocks of coefficients.
@@ -88,6 +105,16 @@ CJ_HD int cj_pix_tile_mcus(int hmax, int bpm) {
   int T = 16 / hmax;
   if (T < 1) T = 1;
   while (T > 1 && T * bpm > 64) T >>= 1;
+  return T;
+}
+
+// MCUs per tensor-core tile: as many as fill the A operand (at most
+// CJ_TC_MAXB blocks), at most 1024 output pixels across.  The tile's plane
+// samples (64 per block) then fit in 64 * CJ_TC_MAXB bytes.
+CJ_HD int cj_pix_tile_mcus_tc(int hmax, int bpm) {
+  int T = 128 / hmax;
+  if (T < 1) T = 1;
+  while (T > 1 && T * bpm > CJ_TC_MAXB) T >>= 1;
   return T;
 }
 
@@ -106,20 +133,37 @@ CJ_HD int cj_pix_check(const CJScanParams* hp) {
 // the two coefficient buffers sit at fixed offsets 0 and 8 KiB (a tile holds
 // at most 64 blocks), so tiles of different geometry -- consecutive tiles of
 // a batch CTA may come from different images -- never overlap the current
-// tile's working space.  The tensor-core form (tc, with nbuf = 2) needs no
-// row-pass buffer but a 128-row FP16 A tile (16 KiB, in the 128-byte swizzled
-// layout, which must start on a 1024-byte boundary: the region holds 1 KiB
-// of slack and the kernel aligns the tile inside it), the hi/lo Kronecker
-// basis (16 KiB) and one range flag per block row, at offsets that do not
-// depend on the geometry (CJ_TC_A_OFF, CJ_TC_B_OFF).
-#define CJ_TC_A_OFF 16384
+// tile's working space.  The tensor-core form (tc) has a layout of its own
+// whose regions do not depend on the geometry either: the plane tiles first
+// (64 bytes per block: at most CJ_TC_SC_OFF), then CJ_TC_NBUF coefficient
+// buffers of CJ_TC_MAXB blocks, the 128-row FP16 A tile (16 KiB, in the
+// 128-byte swizzled layout, which must start on a 1024-byte boundary: the
+// region holds 1 KiB of slack and the kernel aligns the tile inside it), the
+// hi/lo Kronecker basis (16 KiB) and one range flag per block row.
+#define CJ_TC_COEF_BYTES (CJ_TC_MAXB * 128)
+#define CJ_TC_SC_OFF (CJ_TC_MAXB * 64)
+#define CJ_TC_A_OFF (CJ_TC_SC_OFF + CJ_TC_NBUF * CJ_TC_COEF_BYTES)
 #define CJ_TC_A_BYTES (16384 + 1024)
 #define CJ_TC_B_OFF (CJ_TC_A_OFF + CJ_TC_A_BYTES)
+#define CJ_TC_BIG_OFF (CJ_TC_B_OFF + 16384)
+#define CJ_TC_SMEM_BYTES (CJ_TC_BIG_OFF + CJ_TC_MAXB * 8)
 CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy, int nbuf = 1, bool tc = false) {
   g->y_stride = g->T * 8 * g->hmax;
   g->c_stride = g->nch == 3 ? g->T * 8 * csx : 0;
   g->ipr_shift = 0;
   while ((1 << g->ipr_shift) < g->T * g->hmax) g->ipr_shift++;
+  const int csz_tc = g->nch == 3 ? g->c_stride * 8 * csy : 0;
+  if (tc) {  // plane tiles at 0 (64 bytes per block, multiples of 64 each)
+    g->y_off = 0;
+    g->cb_off = g->y_stride * 8 * g->vmax;
+    g->cr_off = g->cb_off + csz_tc;
+    g->sc1_off = CJ_TC_COEF_BYTES;  // from one coefficient buffer to the next
+    g->tmp_off = 0;                 // unused
+    g->a_off = CJ_TC_A_OFF;
+    g->b_off = CJ_TC_B_OFF;
+    g->big_off = CJ_TC_BIG_OFF;
+    return CJ_TC_SMEM_BYTES;
+  }
   const size_t coef_bytes = (size_t)g->T * g->bpm * 128;
   size_t off = coef_bytes;
   g->sc1_off = 0;
@@ -128,17 +172,8 @@ CJ_HD size_t cj_pix_layout(CJPixGeom* g, int csx, int csy, int nbuf = 1, bool tc
     off = 16384;
   }
   g->a_off = g->b_off = g->big_off = 0;
-  if (tc) {
-    g->a_off = CJ_TC_A_OFF;
-    g->b_off = CJ_TC_B_OFF;
-    off = CJ_TC_B_OFF + 16384;
-    g->big_off = (int)off;
-    off += 64 * 8;
-    g->tmp_off = g->a_off;  // unused
-  } else {
-    g->tmp_off = (int)off;
-    off += (size_t)g->T * g->bpm * CJ_TMP_STRIDE * 4;
-  }
+  g->tmp_off = (int)off;
+  off += (size_t)g->T * g->bpm * CJ_TMP_STRIDE * 4;
   g->y_off = (int)off;
   off += (size_t)g->y_stride * 8 * g->vmax;
   off = (off + 15) & ~(size_t)15;
@@ -300,22 +335,20 @@ struct CJTcState {
   uint8_t* a_tile;  // the swizzled A tile: inside the A region, on a 1024-byte boundary
 };
 
-// Tensor-core iDCT of a tile's blocks (at most 64, rows of a 128-row A tile)
-// into the plane tiles.  A row kb = block kb's 64 coefficients dequantised in
-// FP16 (exact below 2048; a block row at or above it flags the block), in
-// the 128-byte swizzled layout (conflict-free stores of a block's 8 rows);
-// thread 0 issues the 8 MMAs of D = A Khi + A Klo; the epilogue reads D row
-// kb (block kb) from tensor memory -- warps w and w + 4 share lanes
-// 32 (w & 3) .. +31 and take pixel rows 0-3 and 4-7 -- rounds,
-// level-shifts, clips and stores the bytes.  Flagged blocks are then redone
-// on CUDA cores in FP32 by the whole CTA (one thread per pixel), a branch
-// the CTA takes together, so the common path carries no call and no spills.
-// Returns false if the MMAs did not complete within the wait bound
-// (recorded).  Ends with a barrier.
-__device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, const int16_t* sc, uint8_t* smem,
-                                                 const CJPixSmemParams& P, CJTcState& tc, CJStatus* st) {
-  uint8_t* sA = tc.a_tile;
-  uint8_t* big = smem + g.big_off;
+// Tensor-core iDCT of a tile's blocks (at most CJ_TC_MAXB, rows of the
+// 128-row A tile), in three steps the tile loop (batch.cu) interleaves with
+// the neighbouring tiles' work:
+//
+// cj_tc_build_a: A row kb = block kb's 64 coefficients dequantised in FP16,
+// the DC biased by TC_DC_BIAS (exact below 2048; a block row at or above it
+// sets the row's range flag),
+// in the 128-byte swizzled layout (conflict-free stores of a block's 8 rows),
+// then the proxy fence that makes the rows visible to the MMAs.
+__device__ __forceinline__ void cj_tc_build_a(int nblk, const int16_t* sc, uint8_t* sA, uint8_t* big,
+                                              const CJPixSmemParams& P) {
+  // a thread always builds row v = threadIdx.x & 7 (blockDim.x is a multiple
+  // of 8); row 0's DC gets the rounding bias (TC_DC_BIAS)
+  const __half2 bias = __halves2half2(__float2half_rn((threadIdx.x & 7) ? 0.f : TC_DC_BIAS), __float2half_rn(0.f));
   for (int t = threadIdx.x; t < nblk * 8; t += blockDim.x) {
     const int kb = t >> 3, v = t & 7;
     const uint4 raw = *reinterpret_cast<const uint4*>(sc + kb * 64 + v * 8);
@@ -325,66 +358,74 @@ __device__ __forceinline__ bool cj_pixel_idct_tc(const CJPixGeom& g, int nblk, c
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       const __half2 c2 = __halves2half2(__short2half_rn((short)(rw[j] & 0xFFFFu)), __short2half_rn((short)(rw[j] >> 16)));
-      const __half2 pr = __hmul2(c2, *reinterpret_cast<const __half2*>(&qw[j]));
+      __half2 pr = __hmul2(c2, *reinterpret_cast<const __half2*>(&qw[j]));
+      if (j == 0) pr = __hadd2(pr, bias);
       p[j] = *reinterpret_cast<const uint32_t*>(&pr);
       // per half: |x| >= 2048 (0x6800, NaN and Inf above) sets bit 15 of
       // (bits & 0x7FFF) + 0x1800; no carry crosses into the upper half
       acc |= (p[j] & 0x7FFF7FFFu) + 0x18001800u;
     }
     big[t] = (acc & 0x80008000u) != 0;
-    // swizzled A rows: the 8 threads of a block row group store to 8 banks
     *reinterpret_cast<uint4*>(sA + tc_sw128_off(kb, v)) = make_uint4(p[0], p[1], p[2], p[3]);
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  __syncthreads();
-  if (cj_pixel_failed(st)) return false;  // the coefficient copy did not land
-  if (threadIdx.x == 0)
-    tc_idct_mmas_asw(tc.tmem, cj_smem_addr(sA), cj_smem_addr(smem + g.b_off), cj_smem_addr(tc.bar));
-  // no barrier after the wait: each thread reads only after its own wait
-  // succeeded, and a failed wait is agreed on at the barrier below
-  const bool ok = cj_mbar_wait(tc.bar, tc.parity);
-  tc.parity ^= 1u;
-  if (!ok) cj_tile_fail = 1;
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// cj_tc_epilogue (after the MMAs' barrier phase completed): D row kb = block
+// kb's 64 outputs, read from tensor memory 16 columns (two pixel rows) at a
+// time -- warps w and w + 4 share lanes 32 (w & 3) .. +31 and take pixel rows
+// 0-3 and 4-7; a warp whose lanes hold no block of the tile skips the reads
+// -- floored (the bias did the rounding), level-shifted, clipped and stored
+// into the plane tiles.
+// `ok` false (the MMAs did not complete): nothing is stored.  Returns true
+// for the thread of a block with a range flag set (FP32 redo needed).
+__device__ __forceinline__ bool cj_tc_epilogue(const CJPixGeom& g, int nblk, uint8_t* smem, const uint8_t* big,
+                                               const CJPixSmemParams& P, const CJTcState& tc, bool ok) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int kb = 32 * (w & 3) + lane, h = w >> 2;
-  float d[32];
-  tc_ld32(tc.tmem + ((uint32_t)(32 * (w & 3)) << 16) + 32u * h, d);
-  if (ok && kb < nblk) {
-    const int ps = P.bc[kb] == 0 ? g.y_stride : g.c_stride;
-    uint8_t* dst = smem + P.boff[kb] + 4 * h * ps;
+  const int quad = w & 3, h = w >> 2, kb = 32 * quad + lane;
+  if (32 * quad >= nblk) return false;  // warp-uniform
+  const uint32_t ta = tc.tmem + ((uint32_t)(32 * quad) << 16) + 32u * h;
+  const bool live = ok && kb < nblk;
+  const int ps = live && P.bc[kb] != 0 ? g.c_stride : g.y_stride;
+  uint8_t* dst = smem + (live ? P.boff[kb] : 0) + 4 * h * ps;
 #pragma unroll
-    for (int y = 0; y < 4; y++)
-      *reinterpret_cast<uint2*>(dst + y * ps) =
-          make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
-                     tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  const bool flagged = kb < nblk && h == 0 && *reinterpret_cast<const uint64_t*>(big + kb * 8) != 0;
-  if (__syncthreads_or(flagged || !ok)) {  // rare: a failed wait, or an FP32 redo of the flagged blocks
-    if (cj_pixel_failed(st)) {
-      cj_mbar_wait(tc.bar, tc.parity ^ 1u);  // a bounded second chance for MMAs still in flight
-      return false;
+  for (int j = 0; j < 2; j++) {
+    float d[16];
+    tc_ld16(ta + 16u * j, d);
+    if (live) {
+#pragma unroll
+      for (int y = 0; y < 2; y++)
+        *reinterpret_cast<uint2*>(dst + (2 * j + y) * ps) =
+            make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
+                       tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
     }
-    for (int k = 0; k < nblk; k++) {
-      if (!*reinterpret_cast<const uint64_t*>(big + k * 8)) continue;  // the same for every thread
-      if (threadIdx.x < 64) {
-        const int y = threadIdx.x >> 3, x = threadIdx.x & 7;
-        const int16_t* blk = sc + k * 64;
-        const int32_t* q = P.q[P.bq[k]];
-        float acc = 0.f;
-        for (int v = 0; v < 8; v++) {
-          float row = 0.f;
-          for (int u = 0; u < 8; u++) row = fmaf((float)(blk[8 * v + u] * q[8 * v + u]), tc.basis[u * 8 + x], row);
-          acc = fmaf(row, tc.basis[v * 8 + y], acc);
-        }
-        const int ps = P.bc[k] == 0 ? g.y_stride : g.c_stride;
-        smem[P.boff[k] + y * ps + x] = (uint8_t)cj_clip8(__float2int_rn(acc) + 128);
+  }
+  return kb < nblk && h == 0 && *reinterpret_cast<const uint64_t*>(big + kb * 8) != 0;
+}
+
+// cj_tc_fallback (rare; the whole CTA): blocks with a range flag redone on
+// CUDA cores in FP32, one thread per output sample, from their coefficients
+// in global memory (`blocks` = the tile's first block).  Ends with a barrier.
+__device__ __forceinline__ void cj_tc_fallback(const CJPixGeom& g, int nblk, const int16_t* __restrict__ blocks,
+                                               uint8_t* smem, const uint8_t* big, const CJPixSmemParams& P,
+                                               const CJTcState& tc) {
+  for (int k = 0; k < nblk; k++) {
+    if (!*reinterpret_cast<const uint64_t*>(big + k * 8)) continue;  // the same for every thread
+    if (threadIdx.x < 64) {
+      const int y = threadIdx.x >> 3, x = threadIdx.x & 7;
+      const int16_t* blk = blocks + (int64_t)k * 64;
+      const int32_t* q = P.q[P.bq[k]];
+      float acc = 0.f;
+      for (int v = 0; v < 8; v++) {
+        float row = 0.f;
+        for (int u = 0; u < 8; u++) row = fmaf((float)(blk[8 * v + u] * q[8 * v + u]), tc.basis[u * 8 + x], row);
+        acc = fmaf(row, tc.basis[v * 8 + y], acc);
       }
+      const int ps = P.bc[k] == 0 ? g.y_stride : g.c_stride;
+      smem[P.boff[k] + y * ps + x] = (uint8_t)cj_clip8(tc_round(acc) + 128);
     }
-    __syncthreads();
   }
-  return true;
+  __syncthreads();
 }
 
 // Nearest upsampling + YCbCr->RGB (or a grey copy) of a tile's plane tiles
@@ -501,24 +542,21 @@ __device__ __forceinline__ void cj_pixel_emit_planes(uint8_t* __restrict__ out, 
 
 // One tile (after cj_pixel_setup for its image), MCU row `mrow`, MCUs
 // [mc0, mc0 + T), whose coefficients arrive in `sc` on phase `parity` of
-// `bar`: the iDCT (MODE) into plane tiles, then the output (OUT) into `out`.
-// Returns false if the copy or the MMAs did not land within the wait bound
+// `bar`: the integer iDCT (MODE) into plane tiles, then the output (OUT) into
+// `out`.  Returns false if the copy did not land within the wait bound
 // (recorded).  Ends with a barrier, so `sc` and the plane tiles are free
 // afterwards.
 template <int MODE, int OUT>
 __device__ __forceinline__ bool cj_pixel_tile(uint8_t* __restrict__ out, CJStatus* st, const CJPixGeom& g, int mrow,
                                               int mc0, const int16_t* sc, uint8_t* smem, uint64_t* barp,
-                                              uint32_t parity, CJPixSmemParams* Pp, CJTcState* tc) {
+                                              uint32_t parity, CJPixSmemParams* Pp) {
   const int nm = min(g.T, g.mcux - mc0);
   const int nblk = nm * g.bpm;
   // each thread reads the copied blocks only after its own wait; a wait that
   // ran out is agreed on at the iDCT's first barrier (no barrier here)
   if (!cj_mbar_wait(barp, parity)) cj_tile_fail = 1;
-  if (MODE == CJ_PIX_IDCT_TC) {
-    if (!cj_pixel_idct_tc(g, nblk, sc, smem, *Pp, *tc, st)) return false;
-  } else {
-    if (!cj_pixel_idct_int(g, nblk, sc, smem, *Pp, st)) return false;
-  }
+  static_assert(MODE == CJ_PIX_IDCT_INT, "tensor-core tiles run in their own loop (bt_pixel_tiles_tc)");
+  if (!cj_pixel_idct_int(g, nblk, sc, smem, *Pp, st)) return false;
   if (OUT == CJ_OUT_RGB) cj_pixel_emit_rgb(out, g, mrow, mc0, nm, smem);
   else cj_pixel_emit_planes<OUT>(out, g, mrow, mc0, nm, smem);
   __syncthreads();
@@ -529,7 +567,7 @@ __device__ __forceinline__ bool cj_pixel_tile(uint8_t* __restrict__ out, CJStatu
 __device__ __forceinline__ bool cj_pixel_compute(uint8_t* __restrict__ out, CJStatus* st, const CJPixGeom& g,
                                                  int mrow, int mc0, const int16_t* sc, uint8_t* smem,
                                                  uint64_t* barp, uint32_t parity, CJPixSmemParams* Pp) {
-  return cj_pixel_tile<CJ_PIX_IDCT_INT, CJ_OUT_RGB>(out, st, g, mrow, mc0, sc, smem, barp, parity, Pp, nullptr);
+  return cj_pixel_tile<CJ_PIX_IDCT_INT, CJ_OUT_RGB>(out, st, g, mrow, mc0, sc, smem, barp, parity, Pp);
 }
 
 // Fancy (triangle) upsampling of a cw x ch chroma plane by 2^xs x 2^ys: the

@@ -283,6 +283,12 @@ static int cj_marker_loop(JPGReader* r, unsigned char* buf, size_t size, bool st
         else r->error = SYNTAX_ERROR;
     }
     if (r->error) break;
+    // a skipped segment that ran past the end: the next marker read fails
+    // (checked here, so the byte before pos is inside the file)
+    if (r->pos > r->end) {
+      r->error = SYNTAX_ERROR;
+      break;
+    }
     if (r->pos[-1] == 0xD9) {
       // EOI (or a segment that happens to end on byte 0xD9, which the
       // reference also takes as the end of the file, src/format.cu:204)

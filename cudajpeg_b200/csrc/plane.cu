@@ -7,6 +7,8 @@
 //   CJ_IDCT_TC   FP16 hi/lo Kronecker basis on tensor cores (k_idct_tc).
 // Input is the quantised int16 block buffer decodeScanGPU leaves on the
 // device; the component's blocks are gathered from the MCU-interleaved order.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_fp16.h>
 #include <math.h>
 #include <stdio.h>
@@ -154,161 +156,228 @@ int cj_upload_basis() {
 // ---------------------------------------------------------------- tensor cores
 //
 // The plane iDCT as one GEMM per 128-block tile (cj_tc.cuh): D = A * Khi +
-// A * Klo with A the dequantised coefficients in FP16 (exact: |value| <= 2048
+// A * Klo with A the dequantised coefficients in FP16 (exact: |value| < 2048
 // for every block a real encoder produces; larger blocks are redone on CUDA
 // cores in FP32), FP32 accumulation in tensor memory, a tcgen05.ld epilogue.
 
 #define TC_M 128
-#define TC_THREADS 128
+#define TC_THREADS 256
+#ifndef TC_STAGES
+#define TC_STAGES 2                 // coefficient tiles in flight per CTA (TMA ring)
+#endif
+#ifndef TC_ABUF
+#define TC_ABUF 1                   // A tiles (with one, a tile's A build waits for the previous MMAs)
+#endif
+#ifndef TC_MINB
+#define TC_MINB 3                   // CTAs per SM the kernel is compiled for
+#endif
+#define TC_TILE_BYTES 16384         // 128 blocks x 64 int16
+// dynamic shared memory: 1 KiB of alignment slack, the TMA ring, the
+// swizzled A tile(s), the hi/lo basis, three slots of per-row range flags
+#define TC_SMEM (1024 + TC_STAGES * TC_TILE_BYTES + TC_ABUF * 16384 + 16384 + 3 * 1024)
 
 // per device: Khi then Klo, core-matrix layout
 #define CJ_MAX_DEVICES 64
 static uint16_t* g_tc_basis_dev[CJ_MAX_DEVICES];
 static std::mutex g_tc_basis_mu;
 
-// One thread's block of a 128-block tile: its 8 coefficient rows as loaded
-// (quantised int16), where it lives and where its pixels go.
-struct TcRows {
-  uint4 r[8];
-  int64_t gb;  // block index in the coefficient buffer
-  int bx, by;  // block position in the plane
-  bool live;
-};
-
-template <bool RAW>
-__device__ __forceinline__ void tc_fetch(const CJPlaneArgs& a, int64_t t, TcRows& x) {
-  const int64_t kb = t * TC_M + threadIdx.x;
-  x.live = kb < a.nblocks;
-  x.bx = x.by = 0;
-  x.gb = 0;
-  if (x.live) x.gb = RAW ? kb : cj_plane_src(a, kb, &x.bx, &x.by);
-#pragma unroll
-  for (int k8 = 0; k8 < 8; k8++)
-    x.r[k8] = x.live ? __ldg(reinterpret_cast<const uint4*>(a.coef + x.gb * 64 + k8 * 8)) : make_uint4(0, 0, 0, 0);
+// Thread 0: the TMA copy of a 128-block tile of the component (3-D tensor
+// map: 64 coefficients x the component's blocks in an MCU x MCUs, box
+// {64, per, 128 / per}) into `dst`, completing on `bar`.  Coordinates past
+// the last MCU read zeros.
+__device__ __forceinline__ void tc_tile_load(void* dst, const CUtensorMap* map, int mcu0, uint64_t* bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(cj_smem_addr(bar)),
+               "r"((uint32_t)TC_TILE_BYTES)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(cj_smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(mcu0), "r"(cj_smem_addr(bar))
+      : "memory");
 }
 
 // RAW = true: write the FP32 values (before +128 / rounding / clip) of block
 // list entries to raw_out; RAW = false: write pixels into the plane.
 //
-// Per 128-block tile: each of the 128 threads dequantises its block into the
-// FP16 A tile (a block whose values FP16 cannot hold exactly is flagged),
-// thread 0 issues the 8 MMAs, and -- while they run and during the epilogue
-// -- every thread already has the loads of its block of the CTA's next tile
-// in flight (register prefetch).  The epilogue reads the block's row of D
-// from tensor memory in two halves of 32 values (pixel rows 0-3, 4-7).
-// Flagged blocks are listed in shared memory and redone afterwards by the
-// whole CTA on CUDA cores in FP32 (one thread per output pixel), a branch the
-// CTA takes together, so the common path carries no call and no spills.
+// A persistent CTA runs its tiles k = 0, 1, ... (tile blockIdx.x + k *
+// gridDim.x) through a software pipeline with one barrier per tile:
+//   - TC_STAGES - 1 tiles ahead, thread 0 has TMA copies in flight into a
+//     ring of shared-memory stages (mbarrier per stage);
+//   - iteration k: every thread dequantises 4 coefficient rows of tile k
+//     into the FP16 A tile (TC_ABUF of them, 128-byte swizzled; with one,
+//     after tile k-1's MMAs have read it; for pixels the DC is biased by
+//     TC_DC_BIAS; a row FP16 cannot hold exactly sets its range flag)
+//     -- barrier -- thread 0 issues tile k's 8 MMAs into one of two
+//     64-column accumulators and the next copy, while every thread runs tile
+//     k-1's epilogue: wait for its MMAs, read its block's half row of D (32
+//     values) with tcgen05.ld, floor (the bias did the rounding), level-
+//     shift and clip, store.  A thread whose block has a range flag computes
+//     its 32 outputs in FP32 from the coefficients in global memory instead.
+// Range flags keep three slots, so a thread still in tile k-1's epilogue
+// never sees tile k+1's flags.  A wait that runs out marks `status` and the
+// tile's output is not written; the pipeline keeps its barriers.
 template <bool RAW>
-__global__ void __launch_bounds__(TC_THREADS, 4) k_idct_tc(CJPlaneArgs a, const uint16_t* __restrict__ basis,
-                                                          float* raw_out, int* status) {
-  extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint64_t bar;
+__global__ void __launch_bounds__(TC_THREADS, TC_MINB) k_idct_tc(const __grid_constant__ CUtensorMap tmap, CJPlaneArgs a,
+                                                          const uint16_t* __restrict__ basis, float* raw_out,
+                                                          int* status) {
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ uint64_t full[TC_STAGES], mma_done[2];
   __shared__ uint32_t tmem_base;
-  __shared__ int16_t q[64];
   __shared__ int32_t q32[64];
   __shared__ float sbasis[64];
-  __shared__ int s_nbig, s_big[TC_M];
-  uint8_t* sA = smem;               // 128 x 64 fp16 = 16 KiB
-  uint8_t* sB = smem + 16384;       // Khi, Klo: 2 x 64 x 64 fp16 = 16 KiB
-  const int tid = threadIdx.x, warp = tid >> 5;
+  uint8_t* smem = smem_raw + ((1024u - (cj_smem_addr(smem_raw) & 1023u)) & 1023u);
+  uint8_t* stages = smem;
+  uint8_t* sA = smem + TC_STAGES * TC_TILE_BYTES;  // A tile(s), 1024-byte aligned
+  uint8_t* sB = sA + TC_ABUF * 16384;
+  uint8_t* flags = sB + 16384;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int k = tid; k < 16384 / 16; k += TC_THREADS)
     reinterpret_cast<uint4*>(sB)[k] = __ldg(reinterpret_cast<const uint4*>(basis) + k);
   if (tid < 64) {
-    q[tid] = a.qnat[tid];
     q32[tid] = a.qnat[tid];
     sbasis[tid] = c_idct_basis[tid];
   }
-  if (warp == 0) tc_alloc(&tmem_base, 64);
-  if (tid == 0) cj_mbar_init(&bar, 1);
+  if (warp == 0) tc_alloc(&tmem_base, 128);
+  if (tid == 0) {
+    for (int s = 0; s < TC_STAGES; s++) cj_mbar_init(&full[s], 1);
+    cj_mbar_init(&mma_done[0], 1);
+    cj_mbar_init(&mma_done[1], 1);
+  }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
-  const uint32_t aaddr = cj_smem_addr(sA), baddr = cj_smem_addr(sB);
-  if (tid == 0) s_nbig = 0;
   const int64_t ntiles = (a.nblocks + TC_M - 1) / TC_M;
-  uint32_t parity = 0;
-  TcRows nx;
-  if ((int64_t)blockIdx.x < ntiles) tc_fetch<RAW>(a, blockIdx.x, nx);
-  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    // ---- A tile: thread m owns block m; dequantise, check range, FP16
-    const TcRows cur = nx;
-    bool big = false;
+  const int64_t K = (int64_t)blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int per = a.sx * a.sy, per_shift = __ffs(per) - 1;  // a power of two
+  const int mcus_per_tile = TC_M / per;
+  auto issue = [&](int64_t k) {
+    const int64_t tile = blockIdx.x + k * gridDim.x;
+    const int s = (int)(k % TC_STAGES);
+    tc_tile_load(stages + s * TC_TILE_BYTES, &tmap, (int)(tile * mcus_per_tile), &full[s]);
+  };
+  if (tid == 0)
+    for (int64_t k = 0; k < K && k < TC_STAGES - 1; k++) issue(k);
+  // this thread always converts coefficient row v = tid & 7 of its blocks:
+  // the row's 8 quantisation steps as FP16 pairs, once
+  const int v = tid & 7;
+  uint32_t qh[4];
 #pragma unroll
-    for (int k8 = 0; k8 < 8; k8++) {
-      int v[8];
-      cj_unpack_dequant(cur.r[k8], q + k8 * 8, v);
-      uint32_t h[4];
+  for (int j = 0; j < 4; j++) {
+    const __half2 q2 = __floats2half2_rn((float)q32[8 * v + 2 * j], (float)q32[8 * v + 2 * j + 1]);
+    qh[j] = *reinterpret_cast<const uint32_t*>(&q2);
+  }
+  // row 0's DC carries the rounding bias (TC_DC_BIAS) for pixels; raw values
+  // are left unbiased
+  const __half2 bias = __floats2half2_rn(!RAW && v == 0 ? TC_DC_BIAS : 0.f, 0.f);
+  bool bad = false;
+  for (int64_t k = 0; k <= K; k++) {
+    if (k < K) {  // ---- A tile of local tile k
+      const int s = (int)(k % TC_STAGES);
+      if (!cj_mbar_wait(&full[s], (uint32_t)((k / TC_STAGES) & 1))) bad = true;
+      const uint8_t* st = stages + s * TC_TILE_BYTES;
+      uint8_t* a_k = sA + (k % TC_ABUF) * 16384;
+      // with one A tile, tile k - 1's MMAs must have read it (bounded wait;
+      // the epilogue below waits for the same phase)
+      if (TC_ABUF == 1 && k >= 1 && !cj_mbar_wait(&mma_done[(k - 1) & 1], (uint32_t)(((k - 1) >> 1) & 1)))
+        bad = true;
+      uint8_t* fl = flags + (k % 3) * 1024;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        big |= (v[2 * j] > 2048 || v[2 * j] < -2048 || v[2 * j + 1] > 2048 || v[2 * j + 1] < -2048);
-        __half2 p2 = __floats2half2_rn((float)v[2 * j], (float)v[2 * j + 1]);
-        h[j] = *reinterpret_cast<uint32_t*>(&p2);
-      }
-      *reinterpret_cast<uint4*>(sA + tc_core_off(tid, k8 * 8)) = make_uint4(h[0], h[1], h[2], h[3]);
-    }
-    if (big && cur.live) s_big[atomicAdd(&s_nbig, 1)] = tid;
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) tc_idct_mmas(tmem, aaddr, baddr, cj_smem_addr(&bar));
-    // ---- the next tile's loads fly while the MMAs run and the epilogue works
-    if (t + gridDim.x < ntiles) tc_fetch<RAW>(a, t + gridDim.x, nx);
-    const bool ok = cj_mbar_wait(&bar, parity);
-    parity ^= 1;
-    if (!__syncthreads_and(ok)) {
-      if (tid == 0) atomicExch(status, 1);
-      cj_mbar_wait(&bar, parity ^ 1);  // give an in-flight MMA a bounded chance to land
-      break;
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // ---- D row m = block m: two halves of 32 FP32 values (pixel rows 0-3, 4-7)
-#pragma unroll 1
-    for (int h = 0; h < 2; h++) {
-      float d[32];
-      tc_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 32u * h, d);
-      if (!cur.live) continue;
-      if (RAW) {
-        float4* o = reinterpret_cast<float4*>(raw_out + (cur.gb * 64 + 32 * h));
+        const int t = tid + TC_THREADS * j, kb = t >> 3;  // row (kb, v) sits at t * 16
+        const uint4 raw = *reinterpret_cast<const uint4*>(st + t * 16);
+        const uint32_t rw[4] = {raw.x, raw.y, raw.z, raw.w};
+        uint32_t p[4], acc = 0;
 #pragma unroll
-        for (int k = 0; k < 8; k++) o[k] = make_float4(d[4 * k], d[4 * k + 1], d[4 * k + 2], d[4 * k + 3]);
-      } else {
-#pragma unroll
-        for (int y = 0; y < 4; y++)
-          *reinterpret_cast<uint2*>(a.plane + (int64_t)(cur.by * 8 + 4 * h + y) * a.stride + cur.bx * 8) =
-              make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
-                         tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
+        for (int i = 0; i < 4; i++) {
+          const __half2 c2 = __halves2half2(__short2half_rn((short)(rw[i] & 0xFFFFu)),
+                                            __short2half_rn((short)(rw[i] >> 16)));
+          __half2 pr = __hmul2(c2, *reinterpret_cast<const __half2*>(&qh[i]));
+          if (i == 0) pr = __hadd2(pr, bias);
+          p[i] = *reinterpret_cast<const uint32_t*>(&pr);
+          // per half: |x| >= 2048 (0x6800, NaN and Inf above) sets bit 15 of
+          // (bits & 0x7FFF) + 0x1800; no carry crosses into the upper half
+          acc |= (p[i] & 0x7FFF7FFFu) + 0x18001800u;
+        }
+        fl[t] = (acc & 0x80008000u) != 0;
+        *reinterpret_cast<uint4*>(a_k + tc_sw128_off(kb, v)) = make_uint4(p[0], p[1], p[2], p[3]);
       }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();  // TMEM and the A tile are free for the next tile
-    const int nbig = s_nbig;
-    if (nbig) {  // CTA-uniform, rare: FP32 redo of the flagged blocks
-      for (int bi = 0; bi < nbig; bi++) {
-        const int64_t kb = t * TC_M + s_big[bi];
-        int bx = 0, by = 0;
-        const int64_t gb = RAW ? kb : cj_plane_src(a, kb, &bx, &by);
-        if (tid < 64) {
-          const int y = tid >> 3, x = tid & 7;
-          const int16_t* blk = a.coef + gb * 64;
-          float acc = 0.f;
-          for (int v = 0; v < 8; v++) {
-            float row = 0.f;
-            for (int u = 0; u < 8; u++) row = fmaf((float)(blk[8 * v + u] * q32[8 * v + u]), sbasis[u * 8 + x], row);
-            acc = fmaf(row, sbasis[v * 8 + y], acc);
-          }
-          if (RAW) raw_out[gb * 64 + tid] = acc;
-          else a.plane[(int64_t)(by * 8 + y) * a.stride + bx * 8 + x] = (uint8_t)cj_clip8(__float2int_rn(acc) + 128);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (k < K && tid == 0) {  // ---- tile k's MMAs, then the copy TC_STAGES - 1 tiles ahead
+      tc_idct_mmas_asw(tmem + (uint32_t)(k & 1) * 64u, cj_smem_addr(sA + (k % TC_ABUF) * 16384), cj_smem_addr(sB),
+                       cj_smem_addr(&mma_done[k & 1]));
+      if (k + TC_STAGES - 1 < K) issue(k + TC_STAGES - 1);
+    }
+    if (k >= 1) {  // ---- epilogue of local tile k - 1
+      const int64_t kk = k - 1;
+      const bool ok = cj_mbar_wait(&mma_done[kk & 1], (uint32_t)((kk >> 1) & 1));
+      if (!ok) bad = true;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int quad = warp & 3, h = warp >> 2, m = 32 * quad + lane;
+      const int64_t kb = (blockIdx.x + kk * gridDim.x) * TC_M + m;
+      const bool live = ok && kb < a.nblocks;
+      const bool flagged = live && *reinterpret_cast<const uint64_t*>(flags + (kk % 3) * 1024 + m * 8) != 0;
+      int bx = 0, by = 0;
+      int64_t gb = 0;
+      if (live && RAW) {
+        gb = kb;
+      } else if (live) {  // cj_plane_src in 32-bit arithmetic (the launcher bounds the MCU count below 2^31)
+        const uint32_t mcu = (uint32_t)kb >> per_shift, loc = (uint32_t)kb & (uint32_t)(per - 1);
+        const uint32_t mrow = mcu / (uint32_t)a.mcux, mcol = mcu - mrow * (uint32_t)a.mcux;
+        bx = (int)(mcol * a.sx + loc % (uint32_t)a.sx);
+        by = (int)(mrow * a.sy + loc / (uint32_t)a.sx);
+        gb = (int64_t)mcu * a.bpm + a.first + loc;
+      }
+      const uint32_t ta = tmem + (uint32_t)(kk & 1) * 64u + ((uint32_t)(32 * quad) << 16) + 32u * h;
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        float d[16];
+        tc_ld16(ta + 16u * j, d);
+        if (!live || flagged) continue;
+        if (RAW) {
+          float4* o = reinterpret_cast<float4*>(raw_out + (gb * 64 + 32 * h + 16 * j));
+#pragma unroll
+          for (int i = 0; i < 4; i++) o[i] = make_float4(d[4 * i], d[4 * i + 1], d[4 * i + 2], d[4 * i + 3]);
+        } else {
+#pragma unroll
+          for (int y = 0; y < 2; y++)
+            *reinterpret_cast<uint2*>(a.plane + (int64_t)(by * 8 + 4 * h + 2 * j + y) * a.stride + bx * 8) =
+                make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
+                           tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
         }
       }
-      __syncthreads();
-      if (tid == 0) s_nbig = 0;
-      __syncthreads();
+      if (flagged) {  // rare: this thread's 32 outputs (pixel rows 4h..4h+3) in FP32
+        const int16_t* blk = a.coef + gb * 64;
+#pragma unroll 1
+        for (int x = 0; x < 8; x++) {
+          float col[8];
+#pragma unroll 1
+          for (int vv = 0; vv < 8; vv++) {
+            float r = 0.f;
+            for (int u = 0; u < 8; u++) r = fmaf((float)(blk[8 * vv + u] * q32[8 * vv + u]), sbasis[u * 8 + x], r);
+            col[vv] = r;
+          }
+#pragma unroll 1
+          for (int y = 4 * h; y < 4 * h + 4; y++) {
+            float s = 0.f;
+            for (int vv = 0; vv < 8; vv++) s = fmaf(col[vv], sbasis[vv * 8 + y], s);
+            if (RAW) raw_out[gb * 64 + y * 8 + x] = s;
+            else a.plane[(int64_t)(by * 8 + y) * a.stride + bx * 8 + x] = (uint8_t)cj_clip8(tc_round(s) + 128);
+          }
+        }
+      }
     }
   }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) tc_dealloc(tmem, 64);
+  if (bad) atomicExch(status, 1);
+  if (warp == 0) tc_dealloc(tmem, 128);
 }
 
 // Khi / Klo of the Kronecker basis in the K-major core-matrix layout of B
@@ -347,6 +416,21 @@ const uint16_t* cj_tc_basis_device() { return cj_tc_basis(); }
 
 static int* g_tc_status_dev[CJ_MAX_DEVICES];  // per device: set when an MMA wait ran out
 
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link-time dependency on libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 cj_encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
 static int cj_idct_tc_launch(const CJPlaneArgs& a, float* raw, bool is_raw, cudaStream_t s) {
   const uint16_t* basis = cj_tc_basis();
   if (cj_upload_basis() || !basis) return CUDA_MEM_ERROR;
@@ -357,29 +441,49 @@ static int cj_idct_tc_launch(const CJPlaneArgs& a, float* raw, bool is_raw, cuda
     CJ_CUDA_TRY(cudaMalloc(&status, sizeof(int)), CUDA_MEM_ERROR);
     CJ_CUDA_TRY(cudaMemset(status, 0, sizeof(int)), CUDA_MEM_ERROR);
   }
+  const int per = a.sx * a.sy;
+  if (per < 1 || per > 16 || (per & (per - 1)) || a.bpm <= 0) return PROGRAMMER_ERROR;
+  const int64_t nmcu = a.nblocks / per;
+  // block indices stay in 32 bits (the epilogue's arithmetic)
+  if (nmcu < 1 || a.nblocks > ((int64_t)1 << 31) - TC_M) return PROGRAMMER_ERROR;
+  // the component's blocks as a 3-D tensor: 64 coefficients x `per` blocks
+  // in an MCU x MCUs, starting at its first block (16-byte aligned: 128 bytes
+  // per block); tiles are 128 / per MCUs
+  PFN_cuTensorMapEncodeTiled_v12000 encode = cj_encode_tiled();
+  if (!encode) return CUDA_KERNEL_LAUNCH_ERROR;
+  CUtensorMap map;
+  const cuuint64_t dims[3] = {64, (cuuint64_t)per, (cuuint64_t)nmcu};
+  const cuuint64_t strides[2] = {128, (cuuint64_t)a.bpm * 128};
+  const cuuint32_t box[3] = {64, (cuuint32_t)per, (cuuint32_t)(TC_M / per)};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  if (encode(&map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, (void*)(a.coef + (int64_t)a.first * 64), dims, strides, box,
+             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return PROGRAMMER_ERROR;
   static bool attr[CJ_MAX_DEVICES];  // function attributes are set per device
-  const int smem = 32768;
   if (!attr[dev]) {
-    CJ_CUDA_TRY(cudaFuncSetAttribute(k_idct_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+    CJ_CUDA_TRY(cudaFuncSetAttribute(k_idct_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM),
                 CUDA_KERNEL_LAUNCH_ERROR);
-    CJ_CUDA_TRY(cudaFuncSetAttribute(k_idct_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+    CJ_CUDA_TRY(cudaFuncSetAttribute(k_idct_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM),
                 CUDA_KERNEL_LAUNCH_ERROR);
     attr[dev] = true;
   }
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int64_t ntiles = (a.nblocks + TC_M - 1) / TC_M;
-  // CTAs per SM: as many as registers, shared memory and tensor memory (64
-  // columns each) allow
-  int per_sm = cj_tc_ctas_per_sm(is_raw ? (const void*)k_idct_tc<true> : (const void*)k_idct_tc<false>, TC_THREADS,
-                                 smem, 64);
+  const int64_t ntiles = (a.nblocks + TC_M - 1) / TC_M;
+  // persistent CTAs: as many per SM as registers, shared memory and tensor
+  // memory (128 columns each) allow.  L2 fills are promoted to 128 bytes
+  // (one block): a component's blocks are 128-byte runs at a stride of the
+  // MCU's blocks, and 256-byte promotion read 1.5x the bytes on 4:4:4.
+  const int per_sm = cj_tc_ctas_per_sm(is_raw ? (const void*)k_idct_tc<true> : (const void*)k_idct_tc<false>,
+                                       TC_THREADS, TC_SMEM, 128);
   if (per_sm < 1) return CUDA_KERNEL_LAUNCH_ERROR;
   unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)sms * per_sm);
   if (grid < 1) grid = 1;
   if (is_raw)
-    k_idct_tc<true><<<grid, TC_THREADS, smem, s>>>(a, basis, raw, status);
+    k_idct_tc<true><<<grid, TC_THREADS, TC_SMEM, s>>>(map, a, basis, raw, status);
   else
-    k_idct_tc<false><<<grid, TC_THREADS, smem, s>>>(a, basis, raw, status);
+    k_idct_tc<false><<<grid, TC_THREADS, TC_SMEM, s>>>(map, a, basis, raw, status);
   CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
   return 0;
 }
@@ -392,6 +496,7 @@ int cj_idct_tc_raw(const int16_t* coef, const int16_t* qnat, float* out, int64_t
   a.coef = coef;
   a.qnat = qnat;
   a.nblocks = nblocks;
+  a.bpm = a.sx = a.sy = a.mcux = 1;
   return cj_idct_tc_launch(a, out, true, s);
 }
 

@@ -91,6 +91,14 @@ int cjDebugHuffDecode(const unsigned char counts[16], const unsigned char *symbo
 int cjDebugStepTable(const unsigned char counts[16], const unsigned char *symbols, int ac,
                      unsigned short *out);
 
+/* Host check of the batch decoder's marker parse: the parse function the
+ * GPU runs per file (cjBatchSetParse), run here on the host, against the
+ * host marker loop of openJPGMem up to the scan (a fresh reader).  Stores
+ * both error codes; returns 0 when they agree and, on success, the scan
+ * range and every byte of the device header agree too (else a bit mask:
+ * 1 error code, 2 scan range, 4 header). */
+int cjDebugParseCompare(const unsigned char *data, size_t size, int *err_host, int *err_parse);
+
 /* Which device code the library was built with: archs[0..] receives the
  * compute capabilities compiled in (1000 = sm_100a), up to max_archs of
  * them, and the count is returned; *binary_version (may be NULL) receives
@@ -159,6 +167,15 @@ int cjBatchGetSubsequenceBitsFor(const CJBatch *b, int sampling_class);
 #define CJ_OUTPUT_NV12 2
 #define CJ_OUTPUT_RGB_FANCY 3
 int cjBatchSetOutput(CJBatch *b, int format, int idct);
+/* Where a batch staged from now on has its files' marker segments parsed:
+ * on the GPU (on_device != 0: the files are copied to the device first and
+ * one thread per file walks its segments there, the reference's
+ * marker loop src/format.cu:159-215 with the segment checks of
+ * src/format.cu:242-442 and the scan-header check of
+ * src/decodeScanGPU.cu:124-144) or on the host (on_device == 0, the default:
+ * the marker loop of openJPG, one file after another).  Both give the same
+ * headers and error codes. */
+int cjBatchSetParse(CJBatch *b, int on_device);
 void cjBatchGetOutput(const CJBatch *b, int *format, int *idct);
 /* Bound on each grid-barrier wait of the decode kernel, in polls of about
  * 128 ns (0 = the default, 2^24 polls: about 2 s).  A wait that runs out

@@ -14,9 +14,10 @@ ZZ = np.array([0, 1, 8, 16, 9, 2, 3, 10, 17, 24, 32, 25, 18, 11, 4, 5, 12, 19, 2
                23, 30, 37, 44, 51, 58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63])
 
 
-@pytest.mark.parametrize("mode", ["444", "422", "gray"])
-def test_plane_forms(cj, oracle_mod, mode):
-    s = W.small_case(61, 512, 384, mode, 95, 0, "noise")
+@pytest.mark.parametrize("mode,w,h", [("444", 512, 384), ("422", 512, 384), ("gray", 512, 384),
+                                      ("420", 520, 392), ("420", 72, 40)])
+def test_plane_forms(cj, oracle_mod, mode, w, h):
+    s = W.small_case(61, w, h, mode, 95, 0, "noise")
     ref = oracle_mod.decode(s.data)
     with cj.Reader() as r:
         r.open_bytes(s.data)
