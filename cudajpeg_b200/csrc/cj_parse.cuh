@@ -278,9 +278,10 @@ CJ_HD int cj_parse_header(const uint8_t* buf, int64_t size, CJImageHeader* h, in
         else e = SYNTAX_ERROR;
     }
     if (e) return e;
-    // a skipped segment that ran past the end: the next marker read fails
-    // (checked here, so the byte before pos is inside the file)
-    if (pos > end) return SYNTAX_ERROR;
+    // a skipped segment that ran past the file: the next marker read fails
+    // (checked here, so the byte before pos -- at most the EOI's last byte,
+    // end + 1 -- is inside the file)
+    if (pos > end + 2) return SYNTAX_ERROR;
     // EOI, or a segment that happens to end on byte 0xD9 (the reference
     // takes either as the end of the file, src/format.cu:204): before any
     // scan, a syntax error

@@ -283,9 +283,10 @@ static int cj_marker_loop(JPGReader* r, unsigned char* buf, size_t size, bool st
         else r->error = SYNTAX_ERROR;
     }
     if (r->error) break;
-    // a skipped segment that ran past the end: the next marker read fails
-    // (checked here, so the byte before pos is inside the file)
-    if (r->pos > r->end) {
+    // a skipped segment that ran past the file: the next marker read fails
+    // (checked here, so the byte before pos -- at most the EOI's last byte,
+    // end + 1 -- is inside the file)
+    if (r->pos > r->end + 2) {
       r->error = SYNTAX_ERROR;
       break;
     }
