@@ -490,8 +490,8 @@ class Batch:
             raise ValueError(f"bad subsequence size {bits} for class {sampling_class}")
 
     def set_parse(self, on_device: bool = True):
-        """Parse the files' marker segments on the GPU or on the host (the
-        default), for batches staged from now on (cjBatchSetParse)."""
+        """Parse the files' marker segments on the GPU (the default) or on the
+        host, for batches staged from now on (cjBatchSetParse)."""
         if self.lib.cjBatchSetParse(self.ptr, 1 if on_device else 0):
             raise ValueError("cjBatchSetParse")
 

@@ -1223,20 +1223,78 @@ static int64_t bt_out_bytes(const CJImageHeader& h, int out) {
 
 // ---------------------------------------------------------------- device header parse
 
+// What the host plan needs of a parsed file: everything of its header but
+// the tables (which stay on the device), its scan range and its error code.
+struct alignas(16) CJParseSummary {
+  int64_t scan_off, scan_len, total_blocks;
+  int32_t err, mcux, mcuy, width, height, hmax, vmax, restart_interval, nseg_expected;
+  uint8_t nch, huff_mask, xshift, yshift;
+  uint8_t comp_dc[3], comp_ac[3], comp_q[3], comp_sx[3], comp_sy[3], pad[1];
+};
+static_assert(sizeof(CJParseSummary) == 80, "summary size");
+static_assert(sizeof(CJImageHeader) % 16 == 0, "headers are copied in 16-byte words");
+
+#define BT_PARSE_THREADS 128
+
 // The batch's marker parse on the GPU: thread i walks file i's marker
 // segments (cj_parse_header) in the blob already copied to the device and
-// leaves its header and {error, scan offset, scan length}.
-__global__ void __launch_bounds__(128) k_parse_headers(const uint8_t* __restrict__ blob,
-                                                        const int64_t* __restrict__ offsets,
-                                                        const int64_t* __restrict__ sizes, int n,
-                                                        CJImageHeader* hdr, int64_t* meta) {
+// leaves its header in `hdr` (device memory).  The CTA's summaries are
+// written to `sum`, pinned host memory mapped into the device's address
+// space, as one contiguous run of 16-byte stores: they reach the host
+// without a device-to-host copy (which would queue behind any other copy in
+// that direction).
+__global__ void __launch_bounds__(BT_PARSE_THREADS) k_parse_headers(const uint8_t* __restrict__ blob,
+                                                                   const int64_t* __restrict__ offsets,
+                                                                   const int64_t* __restrict__ sizes, int n,
+                                                                   CJImageHeader* hdr, CJParseSummary* sum) {
+  __shared__ CJParseSummary s_sum[BT_PARSE_THREADS];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int64_t so = 0, sl = 0;
-  const int e = cj_parse_header(blob + offsets[i], sizes[i], &hdr[i], &so, &sl);
-  meta[3 * i] = e;
-  meta[3 * i + 1] = so;
-  meta[3 * i + 2] = sl;
+  if (i < n) {
+    int64_t so = 0, sl = 0;
+    CJImageHeader* h = &hdr[i];
+    const int e = cj_parse_header(blob + offsets[i], sizes[i], h, &so, &sl);
+    CJParseSummary& q = s_sum[threadIdx.x];
+    q.scan_off = so;
+    q.scan_len = sl;
+    q.total_blocks = h->total_blocks;
+    q.err = e;
+    q.mcux = h->mcux;
+    q.mcuy = h->mcuy;
+    q.width = h->width;
+    q.height = h->height;
+    q.hmax = h->hmax;
+    q.vmax = h->vmax;
+    q.restart_interval = h->restart_interval;
+    q.nseg_expected = h->nseg_expected;
+    q.nch = h->nch;
+    q.huff_mask = h->huff_mask;
+    q.xshift = h->xshift;
+    q.yshift = h->yshift;
+    for (int c = 0; c < 3; c++) {
+      q.comp_dc[c] = h->comp_dc[c];
+      q.comp_ac[c] = h->comp_ac[c];
+      q.comp_q[c] = h->comp_q[c];
+      q.comp_sx[c] = h->comp_sx[c];
+      q.comp_sy[c] = h->comp_sy[c];
+    }
+    q.pad[0] = 0;
+  }
+  __syncthreads();
+  const int first = blockIdx.x * blockDim.x, cnt = min((int)blockDim.x, n - first);
+  const uint4* src = reinterpret_cast<const uint4*>(s_sum);
+  uint4* dst = reinterpret_cast<uint4*>(sum + first);
+  const int words = cnt * (int)(sizeof(CJParseSummary) / 16);
+  for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = src[k];
+}
+
+// The headers of the planned images, compacted: hdr[d] = parsed[file_of[d]]
+// (one CTA per image, 16-byte copies).
+__global__ void __launch_bounds__(128) k_gather_headers(const CJImageHeader* __restrict__ parsed,
+                                                        const int32_t* __restrict__ file_of,
+                                                        CJImageHeader* hdr) {
+  const uint4* src = reinterpret_cast<const uint4*>(parsed + file_of[blockIdx.x]);
+  uint4* dst = reinterpret_cast<uint4*>(hdr + blockIdx.x);
+  for (int k = threadIdx.x; k < (int)(sizeof(CJImageHeader) / 16); k += blockDim.x) dst[k] = src[k];
 }
 
 // ---------------------------------------------------------------- host side
@@ -1255,16 +1313,21 @@ struct CJBatch {
   int idct = CJ_PIX_IDCT_INT;                // pixel-stage iDCT arithmetic
   int out_format = CJ_OUT_RGB;               // output format
   JPGReader* parser = nullptr;  // host marker parse, one image at a time
-  bool parse_on_device = false;  // marker parse on the GPU (k_parse_headers) or on the host
+  bool parse_on_device = true;   // marker parse on the GPU (k_parse_headers) or on the host
   // device buffers (grow-only)
   CJDevBuf hdr, desc, prm, st, blob, data, tile_keep, tile_mark, mpos, mcode, segs, recs, ckpt, snap,
       wagg, carry, coef, out, ctl, fancy;  // fancy: planar samples of the fancy mode
-  CJDevBuf p_size, p_hdr, p_meta;          // device parse: file offsets + sizes, headers, results
+  CJDevBuf p_size, p_hdr, p_map;           // device parse: file offsets + sizes, headers, image -> file
   // pinned host staging
-  CJHostBuf h_hdr, h_desc, h_out, h_st, h_ctl, h_psize, h_phdr, h_pmeta;
+  CJHostBuf h_hdr, h_desc, h_out, h_st, h_ctl, h_psize, h_pmap;
+  // device parse summaries: pinned host memory mapped into the device
+  CJParseSummary* h_psum = nullptr;
+  CJParseSummary* d_psum = nullptr;
+  size_t psum_cap = 0;
   // plan of the staged batch
   int n_in = 0, n_dev = 0;
   std::vector<int> dev_of;     // device slot of each submitted image, -1 if rejected
+  std::vector<int32_t> file_of;  // device parse: submitted image of each device slot
   std::vector<int> host_err;   // host-side (parse) error of each submitted image
   std::vector<int> dims;       // width, height, channels, chroma width, chroma height per device slot
   std::vector<int64_t> outoff; // output offset per device slot
@@ -1416,12 +1479,13 @@ void cjBatchDestroy(CJBatch* b) {
     CJDevBuf* bufs[] = {&b->hdr,  &b->desc, &b->prm,   &b->st,   &b->blob,  &b->data,
                         &b->tile_keep, &b->tile_mark, &b->mpos, &b->mcode, &b->segs,
                         &b->recs, &b->ckpt, &b->snap, &b->wagg, &b->carry, &b->coef, &b->out, &b->ctl,
-                        &b->fancy, &b->p_size, &b->p_hdr, &b->p_meta};
+                        &b->fancy, &b->p_size, &b->p_hdr, &b->p_map};
     for (CJDevBuf* d : bufs)
       if (d->p) cudaFree(d->p);
-    CJHostBuf* hb[] = {&b->h_hdr, &b->h_desc, &b->h_out, &b->h_st, &b->h_ctl, &b->h_psize, &b->h_phdr, &b->h_pmeta};
+    CJHostBuf* hb[] = {&b->h_hdr, &b->h_desc, &b->h_out, &b->h_st, &b->h_ctl, &b->h_psize, &b->h_pmap};
     for (CJHostBuf* h : hb)
       if (h->p) cudaFreeHost(h->p);
+    if (b->h_psum) cudaFreeHost(b->h_psum);
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
     cudaEventDestroy(b->ev0);
     cudaEventDestroy(b->ev1);
@@ -1575,19 +1639,37 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   CJImageHeader* hh = (CJImageHeader*)b->h_hdr.p;
   CJImageDesc* dd = (CJImageDesc*)b->h_desc.p;
   // Marker parse on the GPU: the files go to the device first, one thread per
-  // file parses its segments there (k_parse_headers), and only the headers
-  // and scan ranges come back for the plan.  The same parse runs on the host
-  // with cjBatchSetParse(b, 0).
+  // file parses its segments there (k_parse_headers); the headers stay on
+  // the device and only the summaries the plan needs come back, through
+  // mapped pinned memory.  The same parse runs on the host with
+  // cjBatchSetParse(b, 0).
   const bool dev_parse = b->parse_on_device && n > 0;
-  const CJImageHeader* ph = nullptr;
-  const int64_t* pmeta = nullptr;
+  const CJParseSummary* psum = nullptr;
   if (dev_parse) {
     const size_t nn = (size_t)n;
-    if (cj_host_ensure(b->h_psize, nn * 16) || cj_host_ensure(b->h_phdr, nn * sizeof(CJImageHeader)) ||
-        cj_host_ensure(b->h_pmeta, nn * 24))
-      return OOM_ERROR;
+    if (cj_host_ensure(b->h_psize, nn * 16)) return OOM_ERROR;
+    if (nn > b->psum_cap) {
+      if (b->h_psum) cudaFreeHost(b->h_psum);
+      b->h_psum = b->d_psum = nullptr;
+      b->psum_cap = 0;
+      const size_t cap = nn + nn / 2 + 64;
+      void* hp = nullptr;
+      if (cudaHostAlloc(&hp, cap * sizeof(CJParseSummary), cudaHostAllocMapped) != cudaSuccess) {
+        cudaGetLastError();
+        return OOM_ERROR;
+      }
+      void* dp = nullptr;
+      if (cudaHostGetDevicePointer(&dp, hp, 0) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeHost(hp);
+        return CUDA_MEM_ERROR;
+      }
+      b->h_psum = (CJParseSummary*)hp;
+      b->d_psum = (CJParseSummary*)dp;
+      b->psum_cap = cap;
+    }
     if (bt_ensure(b, b->blob, (size_t)blob_bytes + 64) || bt_ensure(b, b->p_size, nn * 16) ||
-        bt_ensure(b, b->p_hdr, nn * sizeof(CJImageHeader)) || bt_ensure(b, b->p_meta, nn * 24))
+        bt_ensure(b, b->p_hdr, nn * sizeof(CJImageHeader)))
       return CUDA_MEM_ERROR;
     int64_t* hs = (int64_t*)b->h_psize.p;
     memcpy(hs, offsets, nn * 8);
@@ -1596,17 +1678,15 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
     CJ_CUDA_TRY(cudaMemcpyAsync(b->blob.p, blob, (size_t)blob_bytes, cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
     CJ_CUDA_TRY(cudaMemcpyAsync(b->p_size.p, hs, nn * 16, cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
     const int64_t* d_off = (const int64_t*)b->p_size.p;
-    k_parse_headers<<<(n + 127) / 128, 128, 0, s>>>((const uint8_t*)b->blob.p, d_off, d_off + n, n,
-                                                   (CJImageHeader*)b->p_hdr.p, (int64_t*)b->p_meta.p);
+    k_parse_headers<<<(n + BT_PARSE_THREADS - 1) / BT_PARSE_THREADS, BT_PARSE_THREADS, 0, s>>>(
+        (const uint8_t*)b->blob.p, d_off, d_off + n, n, (CJImageHeader*)b->p_hdr.p, b->d_psum);
     CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
     b->launches++;
-    CJ_CUDA_TRY(cudaMemcpyAsync(b->h_phdr.p, b->p_hdr.p, nn * sizeof(CJImageHeader), cudaMemcpyDeviceToHost, s),
-                CUDA_MEM_ERROR);
-    CJ_CUDA_TRY(cudaMemcpyAsync(b->h_pmeta.p, b->p_meta.p, nn * 24, cudaMemcpyDeviceToHost, s), CUDA_MEM_ERROR);
     CJ_CUDA_TRY(cudaStreamSynchronize(s), CUDA_KERNEL_LAUNCH_ERROR);
-    ph = (const CJImageHeader*)b->h_phdr.p;
-    pmeta = (const int64_t*)b->h_pmeta.p;
+    psum = b->h_psum;
   }
+  std::vector<int32_t>& file_of = b->file_of;
+  file_of.clear();
   int nd = 0, ntiles = 0, nsubw = 0, nptiles = 0, nmark = 0, nseg = 0;
   int64_t data_bytes = 0, blocks = 0, out_total = 0, planar_total = 0, npix = 0;
   const bool fancy = b->out_format == CJ_OUT_RGB_FANCY;
@@ -1616,11 +1696,35 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   for (int i = 0; i < n; i++) {
     int64_t so = 0, sl = 0;
     int e;
-    if (dev_parse) {
-      e = (int)pmeta[3 * i];
-      so = pmeta[3 * i + 1];
-      sl = pmeta[3 * i + 2];
-      if (!e) memcpy(&hh[nd], &ph[i], sizeof(CJImageHeader));
+    if (dev_parse) {  // the header without its tables (they stay on the device)
+      const CJParseSummary& q = psum[i];
+      e = q.err;
+      so = q.scan_off;
+      sl = q.scan_len;
+      if (!e) {
+        CJImageHeader& h = hh[nd];
+        memset(&h, 0, sizeof(h));
+        h.total_blocks = q.total_blocks;
+        h.mcux = q.mcux;
+        h.mcuy = q.mcuy;
+        h.width = q.width;
+        h.height = q.height;
+        h.hmax = q.hmax;
+        h.vmax = q.vmax;
+        h.restart_interval = q.restart_interval;
+        h.nseg_expected = q.nseg_expected;
+        h.nch = q.nch;
+        h.huff_mask = q.huff_mask;
+        h.xshift = q.xshift;
+        h.yshift = q.yshift;
+        for (int c = 0; c < 3; c++) {
+          h.comp_dc[c] = q.comp_dc[c];
+          h.comp_ac[c] = q.comp_ac[c];
+          h.comp_q[c] = q.comp_q[c];
+          h.comp_sx[c] = q.comp_sx[c];
+          h.comp_sy[c] = q.comp_sy[c];
+        }
+      }
     } else {
       e = bt_parse(b, blob + offsets[i], (size_t)sizes[i], &hh[nd], &so, &sl);
     }
@@ -1680,6 +1784,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
     g.T = d.T;
     smem = std::max(smem, cj_pix_layout(&g, h.comp_sx[1], h.comp_sy[1], 2, b->idct == CJ_PIX_IDCT_TC));
     b->dev_of[i] = nd;
+    if (dev_parse) file_of.push_back(i);
     b->dims.push_back(h.width);
     b->dims.push_back(h.height);
     b->dims.push_back(ch);
@@ -1720,8 +1825,18 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   if (cj_host_ensure(b->h_st, nd_ * sizeof(CJStatus)) || cj_host_ensure(b->h_ctl, sizeof(CJBatchCtl)))
     return OOM_ERROR;
   cudaStream_t s = b->stream;
-  CJ_CUDA_TRY(cudaMemcpyAsync(b->hdr.p, hh, nd_ * sizeof(CJImageHeader), cudaMemcpyHostToDevice, s),
-              CUDA_MEM_ERROR);
+  if (dev_parse) {  // the parsed headers, compacted to the planned images on the device
+    if (cj_host_ensure(b->h_pmap, nd_ * 4) || bt_ensure(b, b->p_map, nd_ * 4)) return CUDA_MEM_ERROR;
+    memcpy(b->h_pmap.p, file_of.data(), nd_ * 4);
+    CJ_CUDA_TRY(cudaMemcpyAsync(b->p_map.p, b->h_pmap.p, nd_ * 4, cudaMemcpyHostToDevice, s), CUDA_MEM_ERROR);
+    k_gather_headers<<<nd, 128, 0, s>>>((const CJImageHeader*)b->p_hdr.p, (const int32_t*)b->p_map.p,
+                                        (CJImageHeader*)b->hdr.p);
+    CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
+    b->launches++;
+  } else {
+    CJ_CUDA_TRY(cudaMemcpyAsync(b->hdr.p, hh, nd_ * sizeof(CJImageHeader), cudaMemcpyHostToDevice, s),
+                CUDA_MEM_ERROR);
+  }
   CJ_CUDA_TRY(cudaMemcpyAsync(b->desc.p, dd, nd_ * sizeof(CJImageDesc), cudaMemcpyHostToDevice, s),
               CUDA_MEM_ERROR);
   if (!dev_parse)  // (the device parse copied the files already)

@@ -168,13 +168,14 @@ int cjBatchGetSubsequenceBitsFor(const CJBatch *b, int sampling_class);
 #define CJ_OUTPUT_RGB_FANCY 3
 int cjBatchSetOutput(CJBatch *b, int format, int idct);
 /* Where a batch staged from now on has its files' marker segments parsed:
- * on the GPU (on_device != 0: the files are copied to the device first and
- * one thread per file walks its segments there, the reference's
+ * on the GPU (on_device != 0, the default: the files are copied to the
+ * device first and one thread per file walks its segments there, the reference's
  * marker loop src/format.cu:159-215 with the segment checks of
  * src/format.cu:242-442 and the scan-header check of
- * src/decodeScanGPU.cu:124-144) or on the host (on_device == 0, the default:
- * the marker loop of openJPG, one file after another).  Both give the same
- * headers and error codes. */
+ * src/decodeScanGPU.cu:124-144) or on the host (on_device == 0: the marker
+ * loop of openJPG, one file after another).  Both give the same headers and
+ * error codes.  With the GPU parse, cjBatchStage waits for the files' copy
+ * and the parse before it plans the batch. */
 int cjBatchSetParse(CJBatch *b, int on_device);
 void cjBatchGetOutput(const CJBatch *b, int *format, int *idct);
 /* Bound on each grid-barrier wait of the decode kernel, in polls of about
