@@ -60,7 +60,7 @@ EXPORTED = [
     "cjBatchSetSubsequenceBitsFor", "cjBatchGetSubsequenceBitsFor",
     "cjBatchGetOutput", "cjBatchChromaGeometry", "cjBatchDLPack", "cjServerDLPack", "cjDLPackFree",
     "decodeScanCPU", "upsampleAndColourTransformHybrid", "upsampleAndColourTransformGPU",
-    "upsampleAndColourTransformCPU", "cjBatchSetParse", "cjDebugParseCompare",
+    "upsampleAndColourTransformCPU", "cjBatchSetParse", "cjDebugParseCompare", "cjBatchSetHypotheses",
 ]
 
 BATCH_PHASES = ["tables", "destuff_count", "tile_scan", "destuff_scatter", "segments", "sync",
@@ -154,6 +154,7 @@ def load(build_if_missing: bool = True):
     lib.cjBatchGetSubsequenceBitsFor.argtypes = [vp, C.c_int]
     lib.cjBatchSetOutput.argtypes = [vp, C.c_int, C.c_int]
     lib.cjBatchSetParse.argtypes = [vp, C.c_int]
+    lib.cjBatchSetHypotheses.argtypes = [vp, C.c_int]
     lib.cjDebugParseCompare.argtypes = [vp, C.c_size_t, ip, ip]
     lib.cjBatchGetOutput.argtypes = [vp, ip, ip]
     lib.cjBatchChromaGeometry.argtypes = [vp, C.c_int, ip, ip]
@@ -494,6 +495,12 @@ class Batch:
         host, for batches staged from now on (cjBatchSetParse)."""
         if self.lib.cjBatchSetParse(self.ptr, 1 if on_device else 0):
             raise ValueError("cjBatchSetParse")
+
+    def set_hypotheses(self, on: bool = True):
+        """MCU-phase hypotheses in the entropy decode of latency-bound batches
+        (cjBatchSetHypotheses; results identical either way)."""
+        if self.lib.cjBatchSetHypotheses(self.ptr, 1 if on else 0):
+            raise ValueError("cjBatchSetHypotheses")
 
     def set_wait_limit(self, polls: int):
         """Bound each grid-barrier wait of the decode kernel (0 = default)."""

@@ -50,6 +50,9 @@
 // single-image paths keep CJ_SUB_BITS_DEFAULT (more lanes per image).
 #define BT_SUB_BITS_DEFAULT 4096
 #define BT_WARPS (BT_THREADS / 32)
+// MCU-phase hypotheses per subsequence at most (the standard's largest MCU
+// has 10 blocks)
+#define BT_MAX_HYP 10
 #define BT_TILE_BYTES 4096  // destuff tile: 256 threads x 16 bytes
 #define BT_TILE_BAD (1 << 30)  // flag in a tile's marker count: malformed FF sequence
 // fixed shared-memory offsets of the tensor-core form's A tile and basis
@@ -82,7 +85,7 @@ struct CJBatchCtl {
   int pad;
   int next_sync, next_write, next_fix[3];  // dynamic work counters
   unsigned pix_done;                      // pixel-kernel CTAs finished
-  int pad2[2];
+  int next_hyp, pad2;                     // work counter of the phase-hypothesis decodes
   // %globaltimer (ns) at each phase start (CTA 0); t[BT_NPHASE] = end of the
   // pixel kernel (its last CTA)
   unsigned long long t[BT_NPHASE + 1];
@@ -128,6 +131,13 @@ struct CJBatchArgs {
   CJBatchCtl* ctl;
   int n, ntiles, nwarps, nptiles, max_passes;
   unsigned wait_limit;  // grid-barrier polls before a timeout (0 = default)
+  // MCU-phase hypotheses (0 or 1: none): subsequences not at a segment start
+  // are also decoded from their first bit under MCU phases 1 .. nhyp - 1
+  // (below each image's blocks per MCU) before the settle; per global
+  // subsequence, nhyp - 1 records and checkpoint sets
+  int nhyp;
+  CJSubRec* hrecs;
+  CJCkpt* hckpt;
 };
 
 // ---------------------------------------------------------------- device helpers
@@ -380,8 +390,10 @@ __device__ __forceinline__ uint32_t bt_smem_addr(const void* p) {
 }
 
 // MINB = CTAs per SM the register allocation is sized for (64 registers at
-// 4); the autotuner picks among the compiled variants.
-template <int MINB>
+// 4); the autotuner picks among the compiled variants.  HYP: the variant
+// with MCU-phase hypotheses (phase 5a), launched only for latency-bound
+// decodes (a.nhyp > 1), so the throughput variants carry none of its code.
+template <int MINB, bool HYP = false>
 __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ int2 sm2[33];
@@ -585,9 +597,50 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
   if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
 
   bt_stamp(a.ctl, 5);
+  CJSteps* tab = reinterpret_cast<CJSteps*>(smem);
+  // ---- phase 5a (latency-bound decodes only): MCU-phase hypotheses.  A
+  // subsequence's guessed start (its first bit, MCU phase 0) lines up with
+  // the true decode only after hundreds to thousands of bits for
+  // multi-component scans, while one of the decodes from its first bit
+  // under the other phases usually does within a few blocks; the settle
+  // below may join any of them at a checkpoint.  Items: (hypothesis, group
+  // of BT_WARPS warps), each hypothesis's warps padded to whole groups.
+  const int nh = HYP && a.nhyp > 1 ? a.nhyp - 1 : 0;
+  if (HYP && nh) {
+    const int nw8 = (a.nwarps + BT_WARPS - 1) / BT_WARPS * BT_WARPS;
+    for (;;) {
+      const int g0 = bt_next_group(&a.ctl->next_hyp, &s_grp);
+      if (g0 >= nh * nw8) break;
+      const int hp = g0 / nw8, wg = g0 - hp * nw8;
+      if (wg >= a.nwarps) continue;  // CTA-uniform
+      const BTStaged sg = bt_stage(a, wg, min(wg + BT_WARPS, a.nwarps) - 1, tab);
+      const int w = wg + (int)(threadIdx.x >> 5);
+      if (w >= a.nwarps) continue;  // warp-uniform
+      const int i = bt_image_of_warp(a, w);
+      const CJImageDesc& d = a.desc[i];
+      const int nsub = __ldcg(&a.st[i].nsub), nseg = __ldcg(&a.st[i].nseg);
+      const int j0 = w * 32 - d.sub0;
+      if (j0 >= nsub) continue;  // warp-uniform
+      const CJScanParams& sp = a.prm[i];
+      const int h = hp + 1;
+      if (h >= sp.bpm) continue;  // warp-uniform: no such phase in this image
+      CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
+      if (ln.active && !ln.head) {  // a segment's first subsequence starts exactly
+        const int64_t hi = (int64_t)(d.sub0 + j0 + lane) * nh + hp;
+        CJSubRec r;
+        r.start = cj_state(ln.begin, (uint32_t)h);
+        r.exit = r.start;
+        r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
+        r = cj_spec_decode<false>(sp, bt_steps_of(a, sg, tab, i),
+                                  reinterpret_cast<const uint32_t*>(a.data + d.data_off), ln, r.start,
+                                  cj_lane_ckpts(a.hckpt, hi), r, cj_ckpt_step(d.sub_bits));
+        a.hrecs[hi] = r;
+      }
+    }
+    if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
+  }
   // ---- phase 5: speculative decode + warp settle, in groups of BT_WARPS
   // consecutive warps per CTA (handed out dynamically) with staged tables
-  CJSteps* tab = reinterpret_cast<CJSteps*>(smem);
   for (;;) {
     const int g0 = bt_next_group(&a.ctl->next_sync, &s_grp);
     if (g0 >= a.nwarps) break;
@@ -610,7 +663,13 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
     CJCkpt* ck = cj_lane_ckpts(a.ckpt, d.sub0 + j0 + lane);
     const uint32_t cs = cj_ckpt_step(d.sub_bits);
     if (ln.active) r = cj_spec_decode<false>(sp, T, words, ln, r.start, ck, r, cs);
-    cj_warp_settle(sp, T, words, ln, r, r.start, ck, cs);
+    if constexpr (HYP) {
+      const int64_t hi = (int64_t)(d.sub0 + j0 + lane) * nh;
+      cj_warp_settle<true>(sp, T, words, ln, r, r.start, ck, cs, nh ? cj_lane_ckpts(a.hckpt, hi) : nullptr,
+                           nh ? a.hrecs + hi : nullptr, nh ? min(nh, sp.bpm - 1) : 0);
+    } else {
+      cj_warp_settle(sp, T, words, ln, r, r.start, ck, cs);
+    }
     if (ln.active) a.recs[d.sub0 + j0 + lane] = r;
     unsigned act = __ballot_sync(CJ_FULL, ln.active);
     if (lane == 31 - __clz(act)) a.snap0[w] = r.exit;
@@ -670,8 +729,18 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       if (!work) continue;
       const CJScanParams& sp = a.prm[i];
       const uint32_t* words = reinterpret_cast<const uint32_t*>(a.data + d.data_off);
-      if (cj_warp_settle(sp, bt_steps_of(a, sg, tab, i), words, ln, r, in0, cj_lane_ckpts(a.ckpt, d.sub0 + j0 + lane),
-                         cj_ckpt_step(d.sub_bits)) && ln.active)
+      const CJSteps& T = bt_steps_of(a, sg, tab, i);
+      CJCkpt* ck = cj_lane_ckpts(a.ckpt, d.sub0 + j0 + lane);
+      const uint32_t cs = cj_ckpt_step(d.sub_bits);
+      bool moved;
+      if constexpr (HYP) {
+        const int64_t hi = (int64_t)(d.sub0 + j0 + lane) * nh;
+        moved = cj_warp_settle<true>(sp, T, words, ln, r, in0, ck, cs, nh ? cj_lane_ckpts(a.hckpt, hi) : nullptr,
+                                     nh ? a.hrecs + hi : nullptr, nh ? min(nh, sp.bpm - 1) : 0);
+      } else {
+        moved = cj_warp_settle(sp, T, words, ln, r, in0, ck, cs);
+      }
+      if (moved && ln.active)
         a.recs[d.sub0 + j0 + lane] = r;
       unsigned act = __ballot_sync(CJ_FULL, ln.active);
       if (lane == 31 - __clz(act)) {
@@ -827,11 +896,11 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
 
 typedef void (*bt_decode_fn)(CJBatchArgs);
 #define BT_DECODE_CTAS_DEFAULT 4
-static bt_decode_fn bt_decode_kernel(int ctas_per_sm) {
+static bt_decode_fn bt_decode_kernel(int ctas_per_sm, bool hyp = false) {
   switch (ctas_per_sm) {
-    case 3: return k_decode_batch<3>;
-    case 5: return k_decode_batch<5>;
-    default: return k_decode_batch<4>;
+    case 3: return hyp ? k_decode_batch<3, true> : k_decode_batch<3>;
+    case 5: return hyp ? k_decode_batch<5, true> : k_decode_batch<5>;
+    default: return hyp ? k_decode_batch<4, true> : k_decode_batch<4>;
   }
 }
 
@@ -839,11 +908,11 @@ static bt_decode_fn bt_decode_kernel(int ctas_per_sm) {
 // without opting in.
 static cudaError_t bt_decode_attrs() {
   const int bytes = (int)BT_DECODE_SMEM;
-  cudaError_t e = cudaFuncSetAttribute(k_decode_batch<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_decode_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_decode_batch<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = cudaSuccess;
+  for (int c = 3; c <= 5 && e == cudaSuccess; c++)
+    for (int h = 0; h < 2 && e == cudaSuccess; h++)
+      e = cudaFuncSetAttribute((const void*)bt_decode_kernel(c, h != 0), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               bytes);
   return e;
 }
 
@@ -1315,6 +1384,9 @@ struct CJBatch {
   JPGReader* parser = nullptr;  // host marker parse, one image at a time
   bool parse_on_device = true;   // marker parse on the GPU (k_parse_headers) or on the host
   // device buffers (grow-only)
+  CJDevBuf hrecs, hckpt;  // MCU-phase hypotheses of a latency-bound batch
+  int nhyp = 1;
+  bool hyp_enabled = true;  // cjBatchSetHypotheses
   CJDevBuf hdr, desc, prm, st, blob, data, tile_keep, tile_mark, mpos, mcode, segs, recs, ckpt, snap,
       wagg, carry, coef, out, ctl, fancy;  // fancy: planar samples of the fancy mode
   CJDevBuf p_size, p_hdr, p_map;           // device parse: file offsets + sizes, headers, image -> file
@@ -1479,7 +1551,7 @@ void cjBatchDestroy(CJBatch* b) {
     CJDevBuf* bufs[] = {&b->hdr,  &b->desc, &b->prm,   &b->st,   &b->blob,  &b->data,
                         &b->tile_keep, &b->tile_mark, &b->mpos, &b->mcode, &b->segs,
                         &b->recs, &b->ckpt, &b->snap, &b->wagg, &b->carry, &b->coef, &b->out, &b->ctl,
-                        &b->fancy, &b->p_size, &b->p_hdr, &b->p_map};
+                        &b->fancy, &b->p_size, &b->p_hdr, &b->p_map, &b->hrecs, &b->hckpt};
     for (CJDevBuf* d : bufs)
       if (d->p) cudaFree(d->p);
     CJHostBuf* hb[] = {&b->h_hdr, &b->h_desc, &b->h_out, &b->h_st, &b->h_ctl, &b->h_psize, &b->h_pmap};
@@ -1554,6 +1626,12 @@ int cjBatchSetOutput(CJBatch* b, int format, int idct) {
   if (idct != CJ_PIX_IDCT_INT && idct != CJ_PIX_IDCT_TC) return PROGRAMMER_ERROR;
   b->out_format = format;
   b->idct = idct;
+  return 0;
+}
+
+int cjBatchSetHypotheses(CJBatch* b, int on) {
+  if (!b) return PROGRAMMER_ERROR;
+  b->hyp_enabled = on != 0;
   return 0;
 }
 
@@ -1848,6 +1926,29 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
               CUDA_KERNEL_LAUNCH_ERROR);
   if (per_sm < 1) return UNSUPPORTED_ERROR;
   b->grid = std::min(per_sm, b->decode_ctas) * b->sm_count;
+  // MCU-phase hypotheses only where their decodes fit beside the batch's own
+  // warps in one round of the grid: a batch of a few images leaves most of
+  // the GPU idle while its settle chains run, a full batch has no room
+  b->nhyp = 1;
+  if (b->hyp_enabled) {
+    int maxbpm = 1;
+    for (int k = 0; k < nd; k++) {
+      int bpm = 0;
+      for (int c = 0; c < hh[k].nch; c++) bpm += hh[k].comp_sx[c] * hh[k].comp_sy[c];
+      maxbpm = std::max(maxbpm, bpm);
+    }
+    const int nh = std::min(maxbpm, BT_MAX_HYP);
+    int per_sm_hyp = 0;  // the hypothesis variant must fit the same cooperative grid
+    CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &per_sm_hyp, (const void*)bt_decode_kernel(b->decode_ctas, true), BT_THREADS, b->smem),
+                CUDA_KERNEL_LAUNCH_ERROR);
+    if (nh > 1 && per_sm_hyp * b->sm_count >= b->grid && (int64_t)nsubw * nh <= (int64_t)b->grid * BT_WARPS) {
+      const size_t nsub = (size_t)nsubw * 32 * (nh - 1);
+      if (bt_ensure(b, b->hrecs, nsub * sizeof(CJSubRec)) || bt_ensure(b, b->hckpt, nsub * CJ_CKPTS * sizeof(CJCkpt)))
+        return CUDA_MEM_ERROR;
+      b->nhyp = nh;
+    }
+  }
   const void* pk = (const void*)bt_pixel_kernel(b->idct, bt_pix_format(b));
   if (b->idct == CJ_PIX_IDCT_TC && !cj_tc_basis_device()) return CUDA_MEM_ERROR;
   if (b->idct == CJ_PIX_IDCT_TC)  // 64 tensor-memory columns per CTA
@@ -1892,6 +1993,9 @@ static CJBatchArgs bt_args(const CJBatch* b) {
   a.nptiles = b->nptiles;
   a.max_passes = b->nwarps + 2;
   a.wait_limit = b->wait_limit;
+  a.nhyp = b->nhyp;
+  a.hrecs = (CJSubRec*)b->hrecs.p;
+  a.hckpt = (CJCkpt*)b->hckpt.p;
   return a;
 }
 
@@ -1928,7 +2032,7 @@ static bool bt_build_graph(CJBatch* b) {
   void* args[] = {&a1};
   cudaKernelNodeParams kp;
   memset(&kp, 0, sizeof(kp));
-  kp.func = (void*)bt_decode_kernel(b->decode_ctas);
+  kp.func = (void*)bt_decode_kernel(b->decode_ctas, b->nhyp > 1);
   kp.gridDim = dim3(b->grid);
   kp.blockDim = dim3(BT_THREADS);
   kp.sharedMemBytes = (unsigned)b->smem;
@@ -1995,7 +2099,7 @@ int cjBatchRun(CJBatch* b) {
   CJ_CUDA_TRY(cudaMemsetAsync(b->ctl.p, 0, sizeof(CJBatchCtl), s), CUDA_MEM_ERROR);
   CJ_CUDA_TRY(cudaEventRecord(b->ev0, s), CUDA_KERNEL_LAUNCH_ERROR);
   void* args[] = {&a};
-  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bt_decode_kernel(b->decode_ctas), dim3(b->grid),
+  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bt_decode_kernel(b->decode_ctas, b->nhyp > 1), dim3(b->grid),
                                           dim3(BT_THREADS), args, b->smem, s),
               CUDA_KERNEL_LAUNCH_ERROR);
   b->launches++;
@@ -2296,8 +2400,27 @@ int cj_reader_decode(JPGReader* jpg, bool stage) {
                     &per_sm, (const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT), BT_THREADS, BT_DECODE_SMEM),
                 CUDA_KERNEL_LAUNCH_ERROR);
     if (per_sm < 1) return UNSUPPORTED_ERROR;
-    const int work = std::max(desc.ntiles, (nwarps + BT_WARPS - 1) / BT_WARPS);
-    d->b_grid = std::max(1, std::min(std::min(per_sm, BT_DECODE_CTAS_DEFAULT) * sms, work));
+    const int cap = std::min(per_sm, BT_DECODE_CTAS_DEFAULT) * sms;
+    // MCU-phase hypotheses when their decodes fit in one round of the grid
+    // (one image leaves most of the GPU idle while its settle chains run)
+    int bpm = 0;
+    for (int c = 0; c < h.nch; c++) bpm += h.comp_sx[c] * h.comp_sy[c];
+    const int nh = std::min(bpm, BT_MAX_HYP);
+    d->b_nhyp = 1;
+    int per_sm_hyp = 0;  // the hypothesis variant must fit the same cooperative grid
+    CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &per_sm_hyp, (const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT, true), BT_THREADS,
+                    BT_DECODE_SMEM),
+                CUDA_KERNEL_LAUNCH_ERROR);
+    if (nh > 1 && per_sm_hyp * sms >= cap && (int64_t)nwarps * nh <= (int64_t)cap * BT_WARPS) {
+      const size_t nsub = (size_t)desc.sub_cap * (nh - 1);
+      if (cj_dev_ensure(d->hrecs, nsub * sizeof(CJSubRec)) || cj_dev_ensure(d->hckpt, nsub * CJ_CKPTS * sizeof(CJCkpt)))
+        return CUDA_MEM_ERROR;
+      d->b_nhyp = nh;
+    }
+    const int groups = (nwarps + BT_WARPS - 1) / BT_WARPS;
+    const int work = std::max(desc.ntiles, groups * d->b_nhyp);
+    d->b_grid = std::max(1, std::min(cap, work));
     d->b_ntiles = desc.ntiles;
     d->b_nwarps = nwarps;
     d->b_nptiles = desc.nptiles;
@@ -2339,10 +2462,14 @@ int cj_reader_decode(JPGReader* jpg, bool stage) {
   a.nwarps = d->b_nwarps;
   a.nptiles = d->b_nptiles;
   a.max_passes = d->b_nwarps + 2;
+  a.nhyp = d->b_nhyp;
+  a.hrecs = (CJSubRec*)d->hrecs.p;
+  a.hckpt = (CJCkpt*)d->hckpt.p;
   cj_profile_begin(d);
   CJ_CUDA_TRY(cudaMemsetAsync(d->bctl.p, 0, sizeof(CJBatchCtl), s), CUDA_MEM_ERROR);
   void* args[] = {&a};
-  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT), dim3(d->b_grid),
+  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT, d->b_nhyp > 1),
+                                          dim3(d->b_grid),
                                           dim3(BT_THREADS), args, BT_DECODE_SMEM, s),
               CUDA_KERNEL_LAUNCH_ERROR);
   cj_after_launch(d, CJ_K_DECODE_BATCH);

@@ -227,11 +227,13 @@ struct CJCkpt {
 // previous totals shifted by the difference in blocks and DC sums before that
 // point (shifting the later checkpoints too).  The result equals a full
 // decode from `start`.
-template <bool RESUME>
+template <bool RESUME, bool HYP = false>
 __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const CJSteps& T,
                                                    const uint32_t* words, const CJLane& ln, uint64_t start,
                                                    CJCkpt* __restrict__ ck,
-                                                   const CJSubRec& old, uint32_t cstep) {
+                                                   const CJSubRec& old, uint32_t cstep,
+                                                   const CJCkpt* hck = nullptr, const CJSubRec* hrec = nullptr,
+                                                   int nh = 0) {
   CJFBits br;
   br.init(words, ln.end_byte, cj_state_bit(start));
   uint32_t m = cj_state_phase(start);
@@ -269,6 +271,25 @@ __device__ __forceinline__ CJSubRec cj_spec_decode(const CJScanParams& sp, const
           r.dc[0] = old.dc[0] + e0;
           r.dc[1] = old.dc[1] + e1;
           r.dc[2] = old.dc[2] + e2;
+          return true;
+        }
+        // the same test against the decodes of the subsequence from its
+        // first bit under the other MCU phases (hypotheses): equal position
+        // and phase at a block boundary mean the two decodes coincide from
+        // there on, so this decode takes that path's totals and checkpoints
+        for (int h = 0; HYP && h < nh; h++) {
+          const CJCkpt* hc = hck + h * CJ_CKPTS;
+          if (__ldcg(&hc[j].pp) != pp) continue;
+          const int dn = nb - __ldcg(&hc[j].nb), e0 = d0 - __ldcg(&hc[j].d0), e1 = d1 - __ldcg(&hc[j].d1),
+                    e2 = d2 - __ldcg(&hc[j].d2);
+          for (uint32_t q = j; q < CJ_CKPTS; q++)
+            ck[q] = CJCkpt{__ldcg(&hc[q].pp), __ldcg(&hc[q].nb) + dn, __ldcg(&hc[q].d0) + e0,
+                           __ldcg(&hc[q].d1) + e1, __ldcg(&hc[q].d2) + e2};
+          r.exit = __ldcg(&hrec[h].exit);
+          r.nblocks = __ldcg(&hrec[h].nblocks) + dn;
+          r.dc[0] = __ldcg(&hrec[h].dc[0]) + e0;
+          r.dc[1] = __ldcg(&hrec[h].dc[1]) + e1;
+          r.dc[2] = __ldcg(&hrec[h].dc[2]) + e2;
           return true;
         }
       }
@@ -326,9 +347,12 @@ __device__ __forceinline__ uint32_t cj_ckpt_step(int sub_bits) { return (uint32_
 // Re-decode lanes whose input state (lane 0: `lane0_in`; others: the exit of
 // the previous lane) differs from the state they last decoded from, until no
 // lane changes.  Lane l settles after at most l+1 re-decodes.
+// HYP: hck / hrec / nh are the lane's hypothesis decodes (cj_spec_decode).
+template <bool HYP = false>
 __device__ __forceinline__ bool cj_warp_settle(const CJScanParams& sp, const CJSteps& T, const uint32_t* words,
                                                const CJLane& ln, CJSubRec& r, uint64_t lane0_in,
-                                               CJCkpt* ck, uint32_t cstep) {
+                                               CJCkpt* ck, uint32_t cstep, const CJCkpt* hck = nullptr,
+                                               const CJSubRec* hrec = nullptr, int nh = 0) {
   int lane = threadIdx.x & 31;
   bool dirty = false;
   for (int it = 0; it < 34; it++) {
@@ -337,7 +361,7 @@ __device__ __forceinline__ bool cj_warp_settle(const CJScanParams& sp, const CJS
     bool change = ln.active && want != r.start;
     if (!__any_sync(CJ_FULL, change)) break;
     if (change) {
-      r = cj_spec_decode<true>(sp, T, words, ln, want, ck, r, cstep);
+      r = cj_spec_decode<true, HYP>(sp, T, words, ln, want, ck, r, cstep, hck, hrec, nh);
       dirty = true;
     }
   }

@@ -177,6 +177,13 @@ int cjBatchSetOutput(CJBatch *b, int format, int idct);
  * error codes.  With the GPU parse, cjBatchStage waits for the files' copy
  * and the parse before it plans the batch. */
 int cjBatchSetParse(CJBatch *b, int on_device);
+/* MCU-phase hypotheses of the entropy decode (on != 0, the default): when a
+ * staged batch's speculative decodes leave most of the GPU idle (a few
+ * images), each subsequence of a multi-component scan is also decoded from
+ * its first bit under every other MCU phase, and the settle may continue
+ * from whichever of those decodes the true one meets first.  Results are
+ * identical either way; only the time to settle changes. */
+int cjBatchSetHypotheses(CJBatch *b, int on);
 void cjBatchGetOutput(const CJBatch *b, int *format, int *idct);
 /* Bound on each grid-barrier wait of the decode kernel, in polls of about
  * 128 ns (0 = the default, 2^24 polls: about 2 s).  A wait that runs out
