@@ -610,8 +610,8 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
     const int nw8 = (a.nwarps + BT_WARPS - 1) / BT_WARPS * BT_WARPS;
     for (;;) {
       const int g0 = bt_next_group(&a.ctl->next_hyp, &s_grp);
-      if (g0 >= nh * nw8) break;
-      const int hp = g0 / nw8, wg = g0 - hp * nw8;
+      if (g0 >= (nh + 1) * nw8) break;
+      const int h = g0 / nw8, wg = g0 - h * nw8;  // hypothesis h = 0 .. nh (0: the usual guess)
       if (wg >= a.nwarps) continue;  // CTA-uniform
       const BTStaged sg = bt_stage(a, wg, min(wg + BT_WARPS, a.nwarps) - 1, tab);
       const int w = wg + (int)(threadIdx.x >> 5);
@@ -622,19 +622,21 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       const int j0 = w * 32 - d.sub0;
       if (j0 >= nsub) continue;  // warp-uniform
       const CJScanParams& sp = a.prm[i];
-      const int h = hp + 1;
-      if (h >= sp.bpm) continue;  // warp-uniform: no such phase in this image
+      if (h && h >= sp.bpm) continue;  // warp-uniform: no such phase in this image
       CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
-      if (ln.active && !ln.head) {  // a segment's first subsequence starts exactly
-        const int64_t hi = (int64_t)(d.sub0 + j0 + lane) * nh + hp;
+      // a segment's first subsequence starts exactly: phase 0 only
+      if (ln.active && (h == 0 || !ln.head)) {
+        const int64_t gs = d.sub0 + j0 + lane, hi = gs * nh + (h - 1);
         CJSubRec r;
         r.start = cj_state(ln.begin, (uint32_t)h);
         r.exit = r.start;
         r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
         r = cj_spec_decode<false>(sp, bt_steps_of(a, sg, tab, i),
                                   reinterpret_cast<const uint32_t*>(a.data + d.data_off), ln, r.start,
-                                  cj_lane_ckpts(a.hckpt, hi), r, cj_ckpt_step(d.sub_bits));
-        a.hrecs[hi] = r;
+                                  h ? cj_lane_ckpts(a.hckpt, hi) : cj_lane_ckpts(a.ckpt, gs), r,
+                                  cj_ckpt_step(d.sub_bits));
+        if (h) a.hrecs[hi] = r;
+        else a.recs[gs] = r;
       }
     }
     if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
@@ -662,12 +664,44 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
     r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
     CJCkpt* ck = cj_lane_ckpts(a.ckpt, d.sub0 + j0 + lane);
     const uint32_t cs = cj_ckpt_step(d.sub_bits);
-    if (ln.active) r = cj_spec_decode<false>(sp, T, words, ln, r.start, ck, r, cs);
     if constexpr (HYP) {
-      const int64_t hi = (int64_t)(d.sub0 + j0 + lane) * nh;
-      cj_warp_settle<true>(sp, T, words, ln, r, r.start, ck, cs, nh ? cj_lane_ckpts(a.hckpt, hi) : nullptr,
-                           nh ? a.hrecs + hi : nullptr, nh ? min(nh, sp.bpm - 1) : 0);
+      // The decodes of phase 5a; the lane starts the settle from the path
+      // most of them ended on (decodes that have met the true one share its
+      // exit), keeping the others joinable.  The settle's fixed point, and
+      // so the result, does not depend on this choice.
+      const int64_t gs = d.sub0 + j0 + lane, hi = gs * nh;
+      const int nhi = nh ? min(nh, sp.bpm - 1) : 0;
+      CJCkpt* hck = nh ? cj_lane_ckpts(a.hckpt, hi) : nullptr;
+      CJSubRec* hrec = nh ? a.hrecs + hi : nullptr;
+      if (ln.active) r = nh ? bt_load_rec(&a.recs[gs]) : cj_spec_decode<false>(sp, T, words, ln, r.start, ck, r, cs);
+      if (ln.active && !ln.head && nhi) {
+        int best = 0, best_n = 0;
+        for (int x = 0; x <= nhi; x++) {
+          const uint64_t ex = x ? __ldcg(&hrec[x - 1].exit) : r.exit;
+          int cnt = 0;
+          for (int y = 0; y <= nhi; y++) cnt += (y ? __ldcg(&hrec[y - 1].exit) : r.exit) == ex;
+          if (cnt > best_n) {
+            best = x;
+            best_n = cnt;
+          }
+        }
+        if (best) {  // swap the chosen decode in (records and checkpoints)
+          const CJSubRec hb = bt_load_rec(&hrec[best - 1]);
+          hrec[best - 1] = r;
+          r = hb;
+          CJCkpt* hc = hck + (best - 1) * CJ_CKPTS;
+          for (int q = 0; q < CJ_CKPTS; q++) {
+            const CJCkpt t = CJCkpt{__ldcg(&hc[q].pp), __ldcg(&hc[q].nb), __ldcg(&hc[q].d0), __ldcg(&hc[q].d1),
+                                    __ldcg(&hc[q].d2)};
+            hc[q] = CJCkpt{__ldcg(&ck[q].pp), __ldcg(&ck[q].nb), __ldcg(&ck[q].d0), __ldcg(&ck[q].d1),
+                           __ldcg(&ck[q].d2)};
+            ck[q] = t;
+          }
+        }
+      }
+      cj_warp_settle<true>(sp, T, words, ln, r, r.start, ck, cs, hck, hrec, nhi);
     } else {
+      if (ln.active) r = cj_spec_decode<false>(sp, T, words, ln, r.start, ck, r, cs);
       cj_warp_settle(sp, T, words, ln, r, r.start, ck, cs);
     }
     if (ln.active) a.recs[d.sub0 + j0 + lane] = r;
