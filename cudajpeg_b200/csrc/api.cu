@@ -32,9 +32,11 @@ const unsigned char* cjReaderPixels(const JPGReader* r) { return r->pixels; }
 void cjReaderSetFlags(JPGReader* r, int flags) { r->flags = flags; }
 
 int cjReaderSetSubsequenceBits(JPGReader* r, int bits) {
+  const bool autosel = bits == 0;
   if (bits == 0) bits = CJ_SUB_BITS_DEFAULT;
   if (bits < 128 || bits > 65536 || (bits & 31)) return PROGRAMMER_ERROR;
   r->dev->sub_bits = bits;
+  r->dev->sub_bits_auto = autosel;
   return 0;
 }
 

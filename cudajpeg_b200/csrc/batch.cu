@@ -2406,8 +2406,31 @@ int cj_reader_decode(JPGReader* jpg, bool stage) {
     int e = bt_fill_header(jpg, &h);
     if (e) return e;
     const int64_t n = (int64_t)(jpg->end - jpg->pos);
+    static bool attrs = false;  // per process: the attribute is per function, not per device
+    if (!attrs) {
+      CJ_CUDA_TRY(bt_decode_attrs(), CUDA_MEM_ERROR);
+      attrs = true;
+    }
+    int sms = 0, per_sm = 0;
+    CJ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device), CUDA_MEM_ERROR);
+    CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &per_sm, (const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT), BT_THREADS, BT_DECODE_SMEM),
+                CUDA_KERNEL_LAUNCH_ERROR);
+    if (per_sm < 1) return UNSUPPORTED_ERROR;
+    const int cap = std::min(per_sm, BT_DECODE_CTAS_DEFAULT) * sms;
+    int bpm = 0;
+    for (int c = 0; c < h.nch; c++) bpm += h.comp_sx[c] * h.comp_sy[c];
+    const int nh = std::min(bpm, BT_MAX_HYP);
     CJImageDesc desc;
-    bt_plan_one(h, n, d->sub_bits, &desc);
+    // the default size: 512-bit subsequences (more, shorter speculative
+    // decodes: the lowest latency) when their hypothesis decodes still fit
+    // in one round of the grid, else 1024 bits
+    int sub = d->sub_bits;
+    if (d->sub_bits_auto) {
+      bt_plan_one(h, n, 512, &desc);
+      sub = (int64_t)(desc.sub_cap / 32) * std::max(nh, 1) <= (int64_t)cap * BT_WARPS ? 512 : CJ_SUB_BITS_DEFAULT;
+    }
+    bt_plan_one(h, n, sub, &desc);
     const int nwarps = desc.sub_cap / 32;
     if (cj_dev_ensure(d->bhdr, sizeof(CJImageHeader)) || cj_dev_ensure(d->bdesc, sizeof(CJImageDesc)) ||
         cj_dev_ensure(d->params, sizeof(CJScanParams)) || cj_dev_ensure(d->status, sizeof(CJStatus)) ||
@@ -2423,23 +2446,8 @@ int cj_reader_decode(JPGReader* jpg, bool stage) {
         cj_dev_ensure(d->coef, (size_t)h.total_blocks * 128 + 128) || cj_dev_ensure(d->bctl, sizeof(CJBatchCtl)))
       return CUDA_MEM_ERROR;
     if (cj_host_ensure(d->h_bctl, sizeof(CJBatchCtl))) return OOM_ERROR;
-    static bool attrs = false;  // per process: the attribute is per function, not per device
-    if (!attrs) {
-      CJ_CUDA_TRY(bt_decode_attrs(), CUDA_MEM_ERROR);
-      attrs = true;
-    }
-    int sms = 0, per_sm = 0;
-    CJ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device), CUDA_MEM_ERROR);
-    CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                    &per_sm, (const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT), BT_THREADS, BT_DECODE_SMEM),
-                CUDA_KERNEL_LAUNCH_ERROR);
-    if (per_sm < 1) return UNSUPPORTED_ERROR;
-    const int cap = std::min(per_sm, BT_DECODE_CTAS_DEFAULT) * sms;
     // MCU-phase hypotheses when their decodes fit in one round of the grid
     // (one image leaves most of the GPU idle while its settle chains run)
-    int bpm = 0;
-    for (int c = 0; c < h.nch; c++) bpm += h.comp_sx[c] * h.comp_sy[c];
-    const int nh = std::min(bpm, BT_MAX_HYP);
     d->b_nhyp = 1;
     int per_sm_hyp = 0;  // the hypothesis variant must fit the same cooperative grid
     CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(

@@ -45,6 +45,7 @@ struct CJReaderDevice {
   CJHostBuf h_params, h_status, h_pixels, h_file, h_bctl;
   // per-scan bookkeeping
   int sub_bits = CJ_SUB_BITS_DEFAULT;
+  bool sub_bits_auto = true;  // no size set: the decode picks 512 or 1024 bits per image
   size_t raw_len = 0;
   int64_t total_blocks = 0;
   int nsub_cap = 0, nwarp_cap = 0, nseg_exp = 0, mark_cap = 0;

@@ -30,7 +30,10 @@ const unsigned char *cjReaderPixels(const JPGReader *r);
 void cjReaderSetFlags(JPGReader *r, int flags);
 
 /* Bits per speculative subsequence of the parallel Huffman decode
- * (multiple of 32, 128..65536); 0 restores the default. */
+ * (multiple of 32, 128..65536); 0 restores the default, which picks per
+ * image: 512 bits where the MCU-phase hypothesis decodes of so many
+ * subsequences still fit in one round of the GPU (small images, the lowest
+ * latency), else 1024. */
 int cjReaderSetSubsequenceBits(JPGReader *r, int bits);
 
 /* Device time of the last decode split by stage, in milliseconds:
