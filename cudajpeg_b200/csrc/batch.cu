@@ -967,7 +967,8 @@ __device__ __forceinline__ void bt_pixel_tiles_tc(const CJBatchArgs& a, int t0, 
 // keeps a 64-column accumulator in tensor memory per CTA and the hi/lo
 // Kronecker basis, built by the CTA, in shared memory.
 template <int MODE, int OUT>
-__global__ void __launch_bounds__(CJ_PIX_THREADS, MODE == CJ_PIX_IDCT_TC ? CJ_TC_MINB : 6) k_pixel_batch(CJBatchArgs a) {
+__global__ void __launch_bounds__(MODE == CJ_PIX_IDCT_TC ? CJ_TC_THREADS : CJ_PIX_THREADS,
+                                  MODE == CJ_PIX_IDCT_TC ? CJ_TC_MINB : 6) k_pixel_batch(CJBatchArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ uint64_t bar2[2];
   __shared__ CJPixSmemParams P;
@@ -1986,7 +1987,7 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
   const void* pk = (const void*)bt_pixel_kernel(b->idct, bt_pix_format(b));
   if (b->idct == CJ_PIX_IDCT_TC && !cj_tc_basis_device()) return CUDA_MEM_ERROR;
   if (b->idct == CJ_PIX_IDCT_TC)  // 64 tensor-memory columns per CTA
-    per_sm = cj_tc_ctas_per_sm(pk, CJ_PIX_THREADS, b->smem_pix, 64);
+    per_sm = cj_tc_ctas_per_sm(pk, CJ_TC_THREADS, b->smem_pix, 64);
   else
     CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pk, CJ_PIX_THREADS, b->smem_pix),
                 CUDA_KERNEL_LAUNCH_ERROR);
@@ -2082,7 +2083,7 @@ static bool bt_build_graph(CJBatch* b) {
     cudaKernelNodeParams pp = kp;
     pp.func = (void*)bt_pixel_kernel(b->idct, bt_pix_format(b));
     pp.gridDim = dim3(b->grid_pix);
-    pp.blockDim = dim3(CJ_PIX_THREADS);
+    pp.blockDim = dim3(b->idct == CJ_PIX_IDCT_TC ? CJ_TC_THREADS : CJ_PIX_THREADS);
     pp.sharedMemBytes = (unsigned)b->smem_pix;
     ok = cudaGraphAddKernelNode(&n_pix, g, &n_dec, 1, &pp) == cudaSuccess;
   }
@@ -2138,7 +2139,8 @@ int cjBatchRun(CJBatch* b) {
               CUDA_KERNEL_LAUNCH_ERROR);
   b->launches++;
   if (b->grid_pix > 0) {
-    bt_pixel_kernel(b->idct, bt_pix_format(b))<<<b->grid_pix, CJ_PIX_THREADS, b->smem_pix, s>>>(a);
+    bt_pixel_kernel(b->idct, bt_pix_format(b))<<<b->grid_pix, b->idct == CJ_PIX_IDCT_TC ? CJ_TC_THREADS : CJ_PIX_THREADS,
+                                                 b->smem_pix, s>>>(a);
     CJ_CUDA_TRY(cudaGetLastError(), CUDA_KERNEL_LAUNCH_ERROR);
     b->launches++;
     if (b->out_format == CJ_OUT_RGB_FANCY && b->npix > 0) {

@@ -91,6 +91,15 @@ struct CJPixGeom {
 #ifndef CJ_TC_MINB
 #define CJ_TC_MINB 3
 #endif
+// Threads of a tensor-core pixel CTA: the epilogue splits each block's 64
+// outputs over CJ_TC_THREADS / 128 threads (warps w, w + 4, ... share TMEM
+// lanes 32 (w mod 4) .. +31), CJ_TC_COLS columns = CJ_TC_ROWS pixel rows each.
+#ifndef CJ_TC_THREADS
+#define CJ_TC_THREADS 256
+#endif
+#define CJ_TC_COLS (64 / (CJ_TC_THREADS / 128))
+#define CJ_TC_ROWS (8 / (CJ_TC_THREADS / 128))
+static_assert(CJ_TC_THREADS == 256 || CJ_TC_THREADS == 512, "two or four epilogue threads per block");
 
 struct alignas(16) CJPixSmemParams {
   int32_t q[4][64];       // dequantisation tables, natural order (int32: no unpacking per row)
@@ -384,12 +393,12 @@ __device__ __forceinline__ bool cj_tc_epilogue(const CJPixGeom& g, int nblk, uin
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int quad = w & 3, h = w >> 2, kb = 32 * quad + lane;
   if (32 * quad >= nblk) return false;  // warp-uniform
-  const uint32_t ta = tc.tmem + ((uint32_t)(32 * quad) << 16) + 32u * h;
+  const uint32_t ta = tc.tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(CJ_TC_COLS * h);
   const bool live = ok && kb < nblk;
   const int ps = live && P.bc[kb] != 0 ? g.c_stride : g.y_stride;
-  uint8_t* dst = smem + (live ? P.boff[kb] : 0) + 4 * h * ps;
+  uint8_t* dst = smem + (live ? P.boff[kb] : 0) + CJ_TC_ROWS * h * ps;
 #pragma unroll
-  for (int j = 0; j < 2; j++) {
+  for (int j = 0; j < CJ_TC_COLS / 16; j++) {
     float d[16];
     tc_ld16(ta + 16u * j, d);
     if (live) {

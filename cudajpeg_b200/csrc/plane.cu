@@ -161,7 +161,16 @@ int cj_upload_basis() {
 // cores in FP32), FP32 accumulation in tensor memory, a tcgen05.ld epilogue.
 
 #define TC_M 128
+#ifndef TC_THREADS
 #define TC_THREADS 256
+#endif
+// The epilogue splits each block's 64 outputs over TC_THREADS / 128 threads
+// (warps w, w + 4, ... share TMEM lanes 32 (w mod 4) .. +31): TC_COLS columns
+// (TC_ROWS pixel rows) each.
+#define TC_GROUPS (TC_THREADS / 128)
+#define TC_COLS (64 / TC_GROUPS)
+#define TC_ROWS (8 / TC_GROUPS)
+static_assert(TC_THREADS == 256 || TC_THREADS == 512, "two or four threads per block in the epilogue");
 #ifndef TC_STAGES
 #define TC_STAGES 2                 // coefficient tiles in flight per CTA (TMA ring)
 #endif
@@ -285,7 +294,7 @@ __global__ void __launch_bounds__(TC_THREADS, TC_MINB) k_idct_tc(const __grid_co
         bad = true;
       uint8_t* fl = flags + (k % 3) * 1024;
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
+      for (int j = 0; j < 1024 / TC_THREADS; j++) {
         const int t = tid + TC_THREADS * j, kb = t >> 3;  // row (kb, v) sits at t * 16
         const uint4 raw = *reinterpret_cast<const uint4*>(st + t * 16);
         const uint32_t rw[4] = {raw.x, raw.y, raw.z, raw.w};
@@ -334,25 +343,25 @@ __global__ void __launch_bounds__(TC_THREADS, TC_MINB) k_idct_tc(const __grid_co
         by = (int)(mrow * a.sy + loc / (uint32_t)a.sx);
         gb = (int64_t)mcu * a.bpm + a.first + loc;
       }
-      const uint32_t ta = tmem + (uint32_t)(kk & 1) * 64u + ((uint32_t)(32 * quad) << 16) + 32u * h;
+      const uint32_t ta = tmem + (uint32_t)(kk & 1) * 64u + ((uint32_t)(32 * quad) << 16) + (uint32_t)(TC_COLS * h);
 #pragma unroll
-      for (int j = 0; j < 2; j++) {
+      for (int j = 0; j < TC_COLS / 16; j++) {
         float d[16];
         tc_ld16(ta + 16u * j, d);
         if (!live || flagged) continue;
         if (RAW) {
-          float4* o = reinterpret_cast<float4*>(raw_out + (gb * 64 + 32 * h + 16 * j));
+          float4* o = reinterpret_cast<float4*>(raw_out + (gb * 64 + TC_COLS * h + 16 * j));
 #pragma unroll
           for (int i = 0; i < 4; i++) o[i] = make_float4(d[4 * i], d[4 * i + 1], d[4 * i + 2], d[4 * i + 3]);
         } else {
 #pragma unroll
           for (int y = 0; y < 2; y++)
-            *reinterpret_cast<uint2*>(a.plane + (int64_t)(by * 8 + 4 * h + 2 * j + y) * a.stride + bx * 8) =
+            *reinterpret_cast<uint2*>(a.plane + (int64_t)(by * 8 + TC_ROWS * h + 2 * j + y) * a.stride + bx * 8) =
                 make_uint2(tc_level4(d[8 * y], d[8 * y + 1], d[8 * y + 2], d[8 * y + 3]),
                            tc_level4(d[8 * y + 4], d[8 * y + 5], d[8 * y + 6], d[8 * y + 7]));
         }
       }
-      if (flagged) {  // rare: this thread's 32 outputs (pixel rows 4h..4h+3) in FP32
+      if (flagged) {  // rare: this thread's TC_COLS outputs (its TC_ROWS pixel rows) in FP32
         const int16_t* blk = a.coef + gb * 64;
 #pragma unroll 1
         for (int x = 0; x < 8; x++) {
@@ -364,7 +373,7 @@ __global__ void __launch_bounds__(TC_THREADS, TC_MINB) k_idct_tc(const __grid_co
             col[vv] = r;
           }
 #pragma unroll 1
-          for (int y = 4 * h; y < 4 * h + 4; y++) {
+          for (int y = TC_ROWS * h; y < TC_ROWS * (h + 1); y++) {
             float s = 0.f;
             for (int vv = 0; vv < 8; vv++) s = fmaf(col[vv], sbasis[vv * 8 + y], s);
             if (RAW) raw_out[gb * 64 + y * 8 + x] = s;
