@@ -532,7 +532,7 @@ def run_batch(args, wl, world, rank, local, dist):
     decode_ms = sum(pm[k] for k in cj.BATCH_PHASES[:9])
     pixel_ms = pm["pixel"]
     coef_bytes = st_run["blocks"] * 128
-    # the path's algorithmic bytes are the compressed scans read
+    # The path's algorithmic bytes are the compressed scans read
     # plus the decoded pixels written; intermediates are not counted.  The
     # dominant kernel is k_decode_batch, so the roofline is those bytes over
     # its time; the same bytes over the whole step, and each kernel's own
@@ -694,7 +694,7 @@ def run_single(args, wl, world, rank, local, dist):
     means = {k: statistics.mean(v) for k, v in kern_ms.items()}
     dom = max(means, key=means.get)
     peaks = read_peaks()
-    # SURVEY 8(d) bytes of the path (compressed scan read + pixels written)
+    # The path's algorithmic bytes (compressed scan read + pixels written)
     # over the dominant kernel's time; the kernel's own minimum bytes beside
     alg = geom["B"] + geom["P"]
     achieved = alg / (means[dom] / 1e3) / 1e9

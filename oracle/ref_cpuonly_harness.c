@@ -3,7 +3,7 @@
  * (CPUonly/src/{format,decodeScanCPU,pixelTransformCPU,main}.c, built with
  * main renamed) into oracle/_ref/libref_cpuonly.so and exposes a small C
  * surface for ctypes: decode a file, read its geometry and pixels, and time
- * it on N host threads.  TEST / BASELINE INFRASTRUCTURE ONLY.
+ * it on N host threads.  TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.
  *
  * The CPUonly decoder keeps no mutable globals (each JPG is self-contained),
  * so one image per thread is safe.
