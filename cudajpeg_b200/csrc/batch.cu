@@ -85,7 +85,7 @@ struct CJBatchCtl {
   int pad;
   int next_sync, next_write, next_fix[3];  // dynamic work counters
   unsigned pix_done;                      // pixel-kernel CTAs finished
-  int next_hyp, pad2;                     // work counter of the phase-hypothesis decodes
+  int next_hyp, next_probe;               // work counters of the phase-hypothesis decodes and probes
   // %globaltimer (ns) at each phase start (CTA 0); t[BT_NPHASE] = end of the
   // pixel kernel (its last CTA)
   unsigned long long t[BT_NPHASE + 1];
@@ -132,12 +132,17 @@ struct CJBatchArgs {
   int n, ntiles, nwarps, nptiles, max_passes;
   unsigned wait_limit;  // grid-barrier polls before a timeout (0 = default)
   // MCU-phase hypotheses (0 or 1: none): subsequences not at a segment start
-  // are also decoded from their first bit under MCU phases 1 .. nhyp - 1
-  // (below each image's blocks per MCU) before the settle; per global
-  // subsequence, nhyp - 1 records and checkpoint sets
+  // are also decoded from their first bit under MCU phases 0 .. nhyp - 1
+  // (below each image's blocks per MCU) before the settle, and then from
+  // each of their predecessor's hypothesis exits (probes).  Per global
+  // subsequence gs: records and checkpoint sets gs * 2 * nhyp + k for
+  // hypothesis k and gs * 2 * nhyp + nhyp + p for the probe from the
+  // predecessor's hypothesis p; hmap[gs * 16 + p] = the hypothesis whose exit
+  // that probe ends on (15: none)
   int nhyp;
   CJSubRec* hrecs;
   CJCkpt* hckpt;
+  uint8_t* hmap;
 };
 
 // ---------------------------------------------------------------- device helpers
@@ -207,6 +212,95 @@ __device__ __forceinline__ CJWarpAgg bt_load_agg(const CJWarpAgg* p) {
   *reinterpret_cast<int4*>(&r) = __ldcg(q);
   *(reinterpret_cast<int4*>(&r) + 1) = __ldcg(q + 1);
   return r;
+}
+
+// ---- hypothesis maps.  A lane's map sends the index p of a predecessor
+// hypothesis to the index of its own hypothesis whose exit the decode from
+// the predecessor's hypothesis-p exit ends on (15: none of them), packed as
+// 16 nibbles; a map of constant value c is c in every nibble.
+#define BT_MAP_NONE 0xFFFFFFFFFFFFFFFFull
+#define BT_MAP_ID 0xFEDCBA9876543210ull
+__device__ __forceinline__ uint32_t bt_map_at(uint64_t f, uint32_t i) {
+  return i >= 15 ? 15u : (uint32_t)(f >> (4 * i)) & 15u;
+}
+__device__ __forceinline__ uint64_t bt_map_const(uint32_t c) { return c >= 15 ? BT_MAP_NONE : 0x1111111111111111ull * c; }
+// f after g, on the first n entries (the rest: none)
+__device__ __forceinline__ uint64_t bt_map_compose(uint64_t f, uint64_t g, int n) {
+  uint64_t o = BT_MAP_NONE;
+  for (int i = 0; i < n; i++) o &= ~((uint64_t)(15u ^ bt_map_at(f, bt_map_at(g, (uint32_t)i))) << (4 * i));
+  return o;
+}
+
+// The settle of the hypothesis variant: cj_warp_settle's loop and fixed
+// point, with the probe decodes as shortcuts.  Each round the first lane u
+// whose input moved has a final input (every lane before it is consistent).
+// If that input is one of its predecessor's hypothesis exits, the lanes from
+// u on follow the maps (a warp-wide prefix composition) to the hypothesis
+// each predecessor ends on, and every lane with a known predecessor
+// hypothesis takes the probe decode from that hypothesis's exit (record and
+// checkpoints) without decoding; the other moved lanes re-decode as in
+// cj_warp_settle.  Lane u is final after the round, so the loop ends within
+// 33 rounds; with the maps defined it ends after one.
+__device__ __forceinline__ bool bt_settle_map(const CJBatchArgs& a, const CJScanParams& sp, const CJSteps& T,
+                                           const uint32_t* words, const CJLane& ln, bool pred_head, CJSubRec& r,
+                                           uint64_t lane0_in, CJCkpt* ck, uint32_t cs, int64_t gs, int nhi) {
+  const int lane = threadIdx.x & 31;
+  const int NH = a.nhyp;
+  const int64_t hb = gs * 2 * NH;
+  const CJCkpt* hck = cj_lane_ckpts(a.hckpt, hb);
+  const CJSubRec* hrec = a.hrecs + hb;
+  uint64_t M = BT_MAP_NONE;
+  if (ln.active && ln.head) {
+    M = 0;  // a segment's first subsequence starts exactly: its hypothesis 0
+  } else if (ln.active) {
+    const uint4 mb = __ldcg(reinterpret_cast<const uint4*>(a.hmap + gs * 16));
+    const uint32_t wv[4] = {mb.x, mb.y, mb.z, mb.w};
+#pragma unroll
+    for (int p = 0; p < 16; p++)
+      if (p < NH) M &= ~((uint64_t)(15u ^ ((wv[p >> 2] >> (8 * (p & 3))) & 15u)) << (4 * p));
+  }
+  bool dirty = false;
+  for (int it = 0; it < 34; it++) {
+    const uint64_t pred = __shfl_up_sync(CJ_FULL, r.exit, 1);
+    const uint64_t want = ln.head ? r.start : (lane == 0 ? lane0_in : pred);
+    const bool change = ln.active && want != r.start;
+    const unsigned cb = __ballot_sync(CJ_FULL, change);
+    if (!cb) break;
+    const int u = __ffs(cb) - 1;
+    uint32_t q = 15;  // lane u: its input as a predecessor hypothesis
+    if (lane == u) {
+      const CJSubRec* ph = a.hrecs + (gs - 1) * 2 * NH;
+      const int pmax = pred_head ? 0 : nhi;
+      for (int p = 0; p <= pmax; p++)
+        if (__ldcg(&ph[p].exit) == want) {
+          q = (uint32_t)p;
+          break;
+        }
+    }
+    uint64_t v = lane < u ? BT_MAP_ID : (lane == u ? bt_map_const(bt_map_at(M, q)) : M);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint64_t g = __shfl_up_sync(CJ_FULL, v, d);
+      if (lane >= d) v = bt_map_compose(v, g, NH);
+    }
+    uint32_t pidx = __shfl_up_sync(CJ_FULL, (uint32_t)v & 15u, 1);
+    if (lane == u) pidx = q;
+    if (ln.active && !ln.head && lane >= u && pidx < 15) {
+      const CJSubRec* pr = hrec + NH + pidx;
+      if (__ldcg(&pr->start) != r.start) {
+        r = bt_load_rec(pr);
+        const CJCkpt* pc = cj_lane_ckpts(a.hckpt, hb + NH + pidx);
+        for (int k = 0; k < CJ_CKPTS; k++)
+          ck[k] = CJCkpt{__ldcg(&pc[k].pp), __ldcg(&pc[k].nb), __ldcg(&pc[k].d0), __ldcg(&pc[k].d1),
+                         __ldcg(&pc[k].d2)};
+        dirty = true;
+      }
+    } else if (change) {
+      r = cj_spec_decode<true, true>(sp, T, words, ln, want, ck, r, cs, hck, hrec, nhi + 1);
+      dirty = true;
+    }
+  }
+  return dirty;
 }
 
 // Next warp item from a work counter (lane 0 takes it, the warp shares it).
@@ -624,20 +718,69 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       const CJScanParams& sp = a.prm[i];
       if (h && h >= sp.bpm) continue;  // warp-uniform: no such phase in this image
       CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
-      // a segment's first subsequence starts exactly: phase 0 only
+      // a segment's first subsequence starts exactly: phase 0 only.
+      // Hypothesis 0 is also the settle's starting record.
       if (ln.active && (h == 0 || !ln.head)) {
-        const int64_t gs = d.sub0 + j0 + lane, hi = gs * nh + (h - 1);
+        const int64_t gs = d.sub0 + j0 + lane, hs = gs * 2 * (nh + 1) + h;
         CJSubRec r;
         r.start = cj_state(ln.begin, (uint32_t)h);
         r.exit = r.start;
         r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
+        CJCkpt* hc = cj_lane_ckpts(a.hckpt, hs);
         r = cj_spec_decode<false>(sp, bt_steps_of(a, sg, tab, i),
-                                  reinterpret_cast<const uint32_t*>(a.data + d.data_off), ln, r.start,
-                                  h ? cj_lane_ckpts(a.hckpt, hi) : cj_lane_ckpts(a.ckpt, gs), r,
+                                  reinterpret_cast<const uint32_t*>(a.data + d.data_off), ln, r.start, hc, r,
                                   cj_ckpt_step(d.sub_bits));
-        if (h) a.hrecs[hi] = r;
-        else a.recs[gs] = r;
+        a.hrecs[hs] = r;
+        if (h == 0) {
+          a.recs[gs] = r;
+          CJCkpt* ck = cj_lane_ckpts(a.ckpt, gs);
+          for (int k = 0; k < CJ_CKPTS; k++) ck[k] = hc[k];
+        }
       }
+    }
+    if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
+    // ---- phase 5b: probes.  Each subsequence decoded from each of its
+    // predecessor's hypothesis exits (joining its own hypotheses at a
+    // checkpoint, usually the first): the decode it takes once its
+    // predecessor is known to end on that hypothesis, and the map entry
+    // naming the hypothesis it ends on.  Items: (predecessor hypothesis,
+    // group of BT_WARPS warps), as in phase 5a.
+    for (;;) {
+      const int g0 = bt_next_group(&a.ctl->next_probe, &s_grp);
+      if (g0 >= (nh + 1) * nw8) break;
+      const int p = g0 / nw8, wg = g0 - p * nw8;
+      if (wg >= a.nwarps) continue;  // CTA-uniform
+      const BTStaged sg = bt_stage(a, wg, min(wg + BT_WARPS, a.nwarps) - 1, tab);
+      const int w = wg + (int)(threadIdx.x >> 5);
+      if (w >= a.nwarps) continue;  // warp-uniform
+      const int i = bt_image_of_warp(a, w);
+      const CJImageDesc& d = a.desc[i];
+      const int nsub = __ldcg(&a.st[i].nsub), nseg = __ldcg(&a.st[i].nseg);
+      const int j0 = w * 32 - d.sub0;
+      if (j0 >= nsub) continue;  // warp-uniform
+      const CJScanParams& sp = a.prm[i];
+      const int nhi = min(nh, sp.bpm - 1);
+      CJLane ln = cj_lane(a.segs + d.seg0, nseg, nsub, j0 + lane, d.sub_bits);
+      const int64_t gs = d.sub0 + j0 + lane, hb = gs * 2 * (nh + 1);
+      uint8_t mk = 15;
+      const bool pred_head = ln.active && !ln.head && j0 + lane - 1 == a.segs[d.seg0 + ln.seg].first_sub;
+      if (ln.active && !ln.head && p <= (pred_head ? 0 : nhi)) {
+        CJCkpt* pc = cj_lane_ckpts(a.hckpt, hb + (nh + 1) + p);
+        for (int k = 0; k < CJ_CKPTS; k++) pc[k].pp = 0xFFFFFFFFu;  // matches no decode state
+        CJSubRec r;
+        r.start = r.exit = __ldcg(&a.hrecs[(gs - 1) * 2 * (nh + 1) + p].exit);
+        r.nblocks = r.dc[0] = r.dc[1] = r.dc[2] = 0;
+        r = cj_spec_decode<true, true>(sp, bt_steps_of(a, sg, tab, i),
+                                       reinterpret_cast<const uint32_t*>(a.data + d.data_off), ln, r.start, pc, r,
+                                       cj_ckpt_step(d.sub_bits), cj_lane_ckpts(a.hckpt, hb), a.hrecs + hb, nhi + 1);
+        a.hrecs[hb + (nh + 1) + p] = r;
+        for (int k = 0; k <= nhi; k++)
+          if (__ldcg(&a.hrecs[hb + k].exit) == r.exit) {
+            mk = (uint8_t)k;
+            break;
+          }
+      }
+      if (ln.active) a.hmap[gs * 16 + p] = mk;
     }
     if (!bt_grid_sync(a.ctl, gen, a.wait_limit, &s_ok)) return;
   }
@@ -665,41 +808,17 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
     CJCkpt* ck = cj_lane_ckpts(a.ckpt, d.sub0 + j0 + lane);
     const uint32_t cs = cj_ckpt_step(d.sub_bits);
     if constexpr (HYP) {
-      // The decodes of phase 5a; the lane starts the settle from the path
-      // most of them ended on (decodes that have met the true one share its
-      // exit), keeping the others joinable.  The settle's fixed point, and
-      // so the result, does not depend on this choice.
-      const int64_t gs = d.sub0 + j0 + lane, hi = gs * nh;
-      const int nhi = nh ? min(nh, sp.bpm - 1) : 0;
-      CJCkpt* hck = nh ? cj_lane_ckpts(a.hckpt, hi) : nullptr;
-      CJSubRec* hrec = nh ? a.hrecs + hi : nullptr;
-      if (ln.active) r = nh ? bt_load_rec(&a.recs[gs]) : cj_spec_decode<false>(sp, T, words, ln, r.start, ck, r, cs);
-      if (ln.active && !ln.head && nhi) {
-        int best = 0, best_n = 0;
-        for (int x = 0; x <= nhi; x++) {
-          const uint64_t ex = x ? __ldcg(&hrec[x - 1].exit) : r.exit;
-          int cnt = 0;
-          for (int y = 0; y <= nhi; y++) cnt += (y ? __ldcg(&hrec[y - 1].exit) : r.exit) == ex;
-          if (cnt > best_n) {
-            best = x;
-            best_n = cnt;
-          }
-        }
-        if (best) {  // swap the chosen decode in (records and checkpoints)
-          const CJSubRec hb = bt_load_rec(&hrec[best - 1]);
-          hrec[best - 1] = r;
-          r = hb;
-          CJCkpt* hc = hck + (best - 1) * CJ_CKPTS;
-          for (int q = 0; q < CJ_CKPTS; q++) {
-            const CJCkpt t = CJCkpt{__ldcg(&hc[q].pp), __ldcg(&hc[q].nb), __ldcg(&hc[q].d0), __ldcg(&hc[q].d1),
-                                    __ldcg(&hc[q].d2)};
-            hc[q] = CJCkpt{__ldcg(&ck[q].pp), __ldcg(&ck[q].nb), __ldcg(&ck[q].d0), __ldcg(&ck[q].d1),
-                           __ldcg(&ck[q].d2)};
-            ck[q] = t;
-          }
-        }
+      // The phase-0 decodes of phase 5a, settled with the probes of phase 5b
+      // (lane 0 keeps its guess until the fix-up passes)
+      if (nh) {
+        const int64_t gs = d.sub0 + j0 + lane;
+        const bool pred_head = ln.active && !ln.head && j0 + lane - 1 == a.segs[d.seg0 + ln.seg].first_sub;
+        if (ln.active) r = bt_load_rec(&a.recs[gs]);
+        bt_settle_map(a, sp, T, words, ln, pred_head, r, r.start, ck, cs, gs, min(nh, sp.bpm - 1));
+      } else {
+        if (ln.active) r = cj_spec_decode<false>(sp, T, words, ln, r.start, ck, r, cs);
+        cj_warp_settle(sp, T, words, ln, r, r.start, ck, cs);
       }
-      cj_warp_settle<true>(sp, T, words, ln, r, r.start, ck, cs, hck, hrec, nhi);
     } else {
       if (ln.active) r = cj_spec_decode<false>(sp, T, words, ln, r.start, ck, r, cs);
       cj_warp_settle(sp, T, words, ln, r, r.start, ck, cs);
@@ -768,9 +887,13 @@ __global__ void __launch_bounds__(BT_THREADS, MINB) k_decode_batch(CJBatchArgs a
       const uint32_t cs = cj_ckpt_step(d.sub_bits);
       bool moved;
       if constexpr (HYP) {
-        const int64_t hi = (int64_t)(d.sub0 + j0 + lane) * nh;
-        moved = cj_warp_settle<true>(sp, T, words, ln, r, in0, ck, cs, nh ? cj_lane_ckpts(a.hckpt, hi) : nullptr,
-                                     nh ? a.hrecs + hi : nullptr, nh ? min(nh, sp.bpm - 1) : 0);
+        if (nh) {
+          const bool pred_head = ln.active && !ln.head && j0 + lane - 1 == a.segs[d.seg0 + ln.seg].first_sub;
+          moved = bt_settle_map(a, sp, T, words, ln, pred_head, r, in0, ck, cs, (int64_t)(d.sub0 + j0 + lane),
+                                min(nh, sp.bpm - 1));
+        } else {
+          moved = cj_warp_settle(sp, T, words, ln, r, in0, ck, cs);
+        }
       } else {
         moved = cj_warp_settle(sp, T, words, ln, r, in0, ck, cs);
       }
@@ -1419,7 +1542,7 @@ struct CJBatch {
   JPGReader* parser = nullptr;  // host marker parse, one image at a time
   bool parse_on_device = true;   // marker parse on the GPU (k_parse_headers) or on the host
   // device buffers (grow-only)
-  CJDevBuf hrecs, hckpt;  // MCU-phase hypotheses of a latency-bound batch
+  CJDevBuf hrecs, hckpt, hmap;  // MCU-phase hypotheses and probes of a latency-bound batch
   int nhyp = 1;
   bool hyp_enabled = true;  // cjBatchSetHypotheses
   CJDevBuf hdr, desc, prm, st, blob, data, tile_keep, tile_mark, mpos, mcode, segs, recs, ckpt, snap,
@@ -1586,7 +1709,7 @@ void cjBatchDestroy(CJBatch* b) {
     CJDevBuf* bufs[] = {&b->hdr,  &b->desc, &b->prm,   &b->st,   &b->blob,  &b->data,
                         &b->tile_keep, &b->tile_mark, &b->mpos, &b->mcode, &b->segs,
                         &b->recs, &b->ckpt, &b->snap, &b->wagg, &b->carry, &b->coef, &b->out, &b->ctl,
-                        &b->fancy, &b->p_size, &b->p_hdr, &b->p_map, &b->hrecs, &b->hckpt};
+                        &b->fancy, &b->p_size, &b->p_hdr, &b->p_map, &b->hrecs, &b->hckpt, &b->hmap};
     for (CJDevBuf* d : bufs)
       if (d->p) cudaFree(d->p);
     CJHostBuf* hb[] = {&b->h_hdr, &b->h_desc, &b->h_out, &b->h_st, &b->h_ctl, &b->h_psize, &b->h_pmap};
@@ -1978,8 +2101,9 @@ int cjBatchStage(CJBatch* b, int n, const unsigned char* blob, const int64_t* of
                     &per_sm_hyp, (const void*)bt_decode_kernel(b->decode_ctas, true), BT_THREADS, b->smem),
                 CUDA_KERNEL_LAUNCH_ERROR);
     if (nh > 1 && per_sm_hyp * b->sm_count >= b->grid && (int64_t)nsubw * nh <= (int64_t)b->grid * BT_WARPS) {
-      const size_t nsub = (size_t)nsubw * 32 * (nh - 1);
-      if (bt_ensure(b, b->hrecs, nsub * sizeof(CJSubRec)) || bt_ensure(b, b->hckpt, nsub * CJ_CKPTS * sizeof(CJCkpt)))
+      const size_t nsub = (size_t)nsubw * 32, nrec = nsub * 2 * nh;  // hypotheses and probes
+      if (bt_ensure(b, b->hrecs, nrec * sizeof(CJSubRec)) || bt_ensure(b, b->hckpt, nrec * CJ_CKPTS * sizeof(CJCkpt)) ||
+          bt_ensure(b, b->hmap, nsub * 16))
         return CUDA_MEM_ERROR;
       b->nhyp = nh;
     }
@@ -2031,6 +2155,7 @@ static CJBatchArgs bt_args(const CJBatch* b) {
   a.nhyp = b->nhyp;
   a.hrecs = (CJSubRec*)b->hrecs.p;
   a.hckpt = (CJCkpt*)b->hckpt.p;
+  a.hmap = (uint8_t*)b->hmap.p;
   return a;
 }
 
@@ -2451,18 +2576,29 @@ int cj_reader_decode(JPGReader* jpg, bool stage) {
     // MCU-phase hypotheses when their decodes fit in one round of the grid
     // (one image leaves most of the GPU idle while its settle chains run)
     d->b_nhyp = 1;
-    int per_sm_hyp = 0;  // the hypothesis variant must fit the same cooperative grid
-    CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                    &per_sm_hyp, (const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT, true), BT_THREADS,
-                    BT_DECODE_SMEM),
-                CUDA_KERNEL_LAUNCH_ERROR);
-    if (nh > 1 && per_sm_hyp * sms >= cap && (int64_t)nwarps * nh <= (int64_t)cap * BT_WARPS) {
-      const size_t nsub = (size_t)desc.sub_cap * (nh - 1);
-      if (cj_dev_ensure(d->hrecs, nsub * sizeof(CJSubRec)) || cj_dev_ensure(d->hckpt, nsub * CJ_CKPTS * sizeof(CJCkpt)))
-        return CUDA_MEM_ERROR;
-      d->b_nhyp = nh;
-    }
+    d->b_ctas = BT_DECODE_CTAS_DEFAULT;
     const int groups = (nwarps + BT_WARPS - 1) / BT_WARPS;
+    if (nh > 1 && (int64_t)nwarps * nh <= (int64_t)cap * BT_WARPS) {
+      // the hypothesis variant must fit the cooperative grid: its 3-CTA
+      // build (no register spills) when the grid allows, else the 4-CTA one
+      const int grid_h = std::max(1, std::min(cap, std::max(desc.ntiles, groups * nh)));
+      int per3 = 0, per4 = 0;
+      CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per3, (const void*)bt_decode_kernel(3, true),
+                                                                BT_THREADS, BT_DECODE_SMEM),
+                  CUDA_KERNEL_LAUNCH_ERROR);
+      CJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                      &per4, (const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT, true), BT_THREADS, BT_DECODE_SMEM),
+                  CUDA_KERNEL_LAUNCH_ERROR);
+      const int ctas = per3 * sms >= grid_h ? 3 : (per4 * sms >= grid_h ? BT_DECODE_CTAS_DEFAULT : 0);
+      if (ctas) {
+        const size_t nsub = (size_t)desc.sub_cap, nrec = nsub * 2 * nh;  // hypotheses and probes
+        if (cj_dev_ensure(d->hrecs, nrec * sizeof(CJSubRec)) ||
+            cj_dev_ensure(d->hckpt, nrec * CJ_CKPTS * sizeof(CJCkpt)) || cj_dev_ensure(d->hmap, nsub * 16))
+          return CUDA_MEM_ERROR;
+        d->b_nhyp = nh;
+        d->b_ctas = ctas;
+      }
+    }
     const int work = std::max(desc.ntiles, groups * d->b_nhyp);
     d->b_grid = std::max(1, std::min(cap, work));
     d->b_ntiles = desc.ntiles;
@@ -2509,10 +2645,11 @@ int cj_reader_decode(JPGReader* jpg, bool stage) {
   a.nhyp = d->b_nhyp;
   a.hrecs = (CJSubRec*)d->hrecs.p;
   a.hckpt = (CJCkpt*)d->hckpt.p;
+  a.hmap = (uint8_t*)d->hmap.p;
   cj_profile_begin(d);
   CJ_CUDA_TRY(cudaMemsetAsync(d->bctl.p, 0, sizeof(CJBatchCtl), s), CUDA_MEM_ERROR);
   void* args[] = {&a};
-  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bt_decode_kernel(BT_DECODE_CTAS_DEFAULT, d->b_nhyp > 1),
+  CJ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bt_decode_kernel(d->b_ctas, d->b_nhyp > 1),
                                           dim3(d->b_grid),
                                           dim3(BT_THREADS), args, BT_DECODE_SMEM, s),
               CUDA_KERNEL_LAUNCH_ERROR);

@@ -41,7 +41,7 @@ struct CJReaderDevice {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_begin = nullptr, ev_scan = nullptr, ev_end = nullptr;
   CJDevBuf raw, data, tile_keep, tile_mark, mpos, mcode, segs, recs, ckpt, snap, wagg, carry, coef,
-      pix, params, status, wcoef, bhdr, bdesc, bctl, pscan, hrecs, hckpt;
+      pix, params, status, wcoef, bhdr, bdesc, bctl, pscan, hrecs, hckpt, hmap;
   CJHostBuf h_params, h_status, h_pixels, h_file, h_bctl;
   // per-scan bookkeeping
   int sub_bits = CJ_SUB_BITS_DEFAULT;
@@ -52,7 +52,7 @@ struct CJReaderDevice {
   int scan_pending = 0;   // a scan was launched and its status is not yet checked
   int comp_first[3];      // first block of each component inside an MCU
   // the scan as one image of the batch decode kernel (cj_reader_decode)
-  int b_grid = 0, b_ntiles = 0, b_nwarps = 0, b_nptiles = 0, b_nhyp = 1;
+  int b_grid = 0, b_ntiles = 0, b_nwarps = 0, b_nptiles = 0, b_nhyp = 1, b_ctas = 4;
   size_t param_bytes = 0;  // header + plan bytes copied to the device per scan
   // kernel accounting: launches since reader creation, and (when profiling)
   // one event after each kernel of the last decode

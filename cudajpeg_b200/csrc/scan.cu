@@ -87,7 +87,7 @@ void cj_dev_release(CJReaderDevice* d) {
   CJDevBuf* bufs[] = {&d->raw,  &d->data, &d->tile_keep, &d->tile_mark, &d->mpos,
                       &d->mcode, &d->segs, &d->recs, &d->ckpt,     &d->snap,      &d->wagg,
                       &d->carry, &d->coef, &d->pix,      &d->params,    &d->status,
-                      &d->wcoef, &d->bhdr, &d->bdesc, &d->bctl, &d->pscan, &d->hrecs, &d->hckpt};
+                      &d->wcoef, &d->bhdr, &d->bdesc, &d->bctl, &d->pscan, &d->hrecs, &d->hckpt, &d->hmap};
   for (CJDevBuf* b : bufs)
     if (b->p) cudaFree(b->p);
   CJHostBuf* hb[] = {&d->h_params, &d->h_status, &d->h_pixels, &d->h_file, &d->h_bctl};

@@ -2,7 +2,8 @@
 drop-in path): the settle may continue from a decode that started under
 another MCU phase, which changes only how long it takes.  The same batch
 decoded with and without them gives identical coefficients and pixels, and
-the single-image path (which uses them) matches the oracle."""
+the single-image path (which uses them, with the probe decodes from each
+predecessor hypothesis that settle a warp in one step) matches the oracle."""
 import numpy as np
 import pytest
 
@@ -34,10 +35,13 @@ def test_hypotheses_do_not_change_results(cj, oracle_mod):
             assert np.array_equal(i1[k], ref.pixels), k
 
 
-@pytest.mark.parametrize("case", [("420", 1024, 768, 75), ("422", 900, 700, 85), ("444", 640, 480, 95)])
+# restart intervals put segment starts inside warps: a subsequence whose
+# predecessor starts a segment has one predecessor hypothesis only
+@pytest.mark.parametrize("case", [("420", 1024, 768, 75, 0), ("422", 900, 700, 85, 0), ("444", 640, 480, 95, 0),
+                                  ("420", 1024, 768, 75, 3), ("420", 800, 600, 60, 17), ("422", 640, 480, 90, 40)])
 def test_single_image_path_with_hypotheses(cj, oracle_mod, case):
-    mode, w, h, q = case
-    s = W.small_case(95, w, h, mode, q, 0, "texture")
+    mode, w, h, q, restart = case
+    s = W.small_case(95, w, h, mode, q, restart, "texture")
     ref = oracle_mod.decode(s.data)
     with cj.Reader(host_coefficients=True) as r:
         r.open_bytes(s.data)
