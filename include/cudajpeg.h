@@ -183,9 +183,11 @@ int cjBatchSetParse(CJBatch *b, int on_device);
 /* MCU-phase hypotheses of the entropy decode (on != 0, the default): when a
  * staged batch's speculative decodes leave most of the GPU idle (a few
  * images), each subsequence of a multi-component scan is also decoded from
- * its first bit under every other MCU phase, and the settle may continue
- * from whichever of those decodes the true one meets first.  Results are
- * identical either way; only the time to settle changes. */
+ * its first bit under every other MCU phase and then from each of its
+ * predecessor's hypothesis exits; the settle takes those decodes instead of
+ * re-decoding lane after lane.  Results are identical either way; only the
+ * time to settle changes (device memory: two records and checkpoint sets
+ * per subsequence and hypothesis). */
 int cjBatchSetHypotheses(CJBatch *b, int on);
 void cjBatchGetOutput(const CJBatch *b, int *format, int *idct);
 /* Bound on each grid-barrier wait of the decode kernel, in polls of about
